@@ -1,0 +1,386 @@
+"""Benchmark of the graph-diffusion hot path on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Workload (one "step" = one full diffusion of the dense block):
+  500,000 cells from the seeded 10-component 50-D mixture, k=30 kNN (FP32 on
+  the device; a harness input, not timed), Gaussian adaptive-sigma weights,
+  (W+W^T)/2, row-normalised CSR; X0 500,000 x 64 FP32 ~ N(0,1); 16 diffusion
+  steps. Inputs are resident in HBM when the timed region starts and the L2 is
+  flushed (256 MiB write) before every timed step.
+
+Reported (one JSON line on rank 0):
+  value      algorithmic HBM GB/s of the FP32 plain diffusion, whole job
+             (B_step = nnz*(4+4) + (n+1)*4 + 2*n*F*4 bytes per SpMM step)
+  forms      BF16 / FP16 storage forms (GB/s, speed-up vs FP32, error vs FP64)
+  e2e        the same metric through scl_diffusion_diffuse_matrix with host
+             buffers (pinned), including all host<->device copies
+  roofline   dominant kernel (SpMM) vs the measured HBM copy bandwidth
+  cpu_baseline  scl-core's own CPU diffuse_matrix (oracle/_ref) on the host
+
+--impl reference times scl-core's CPU implementation of the same workload on
+the host cores and prints the same line with "impl": "reference".
+Multi-GPU (torchrun): every rank runs an independent replica (weak scaling).
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+sys.path.insert(0, str(ROOT / "scl-core_b200"))
+
+N_CELLS, K_NN, N_FEAT, N_STEPS = 500_000, 30, 64, 16
+METRIC = "diffusion HBM GB/s & fwd+bwd ms (500k cells,k=30,64 cols) BF16 vs FP32 plain"
+
+
+def step_bytes(n, nnz, F, s_idx=4, s_val=4, s_x=4):
+    return nnz * (s_idx + s_val) + (n + 1) * 4 + 2 * n * F * s_x
+
+
+def load_peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+# ---- clocks sampling -----------------------------------------------------------
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.samples = []
+        self._stop = threading.Event()
+        self._t = None
+
+    def _run(self):
+        while not self._stop.is_set():
+            try:
+                out = subprocess.run(["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}",
+                                      "--format=csv,noheader,nounits"], capture_output=True, text=True, timeout=5)
+                if out.returncode == 0 and out.stdout.strip():
+                    self.samples.append([x.strip() for x in out.stdout.strip().split(",")])
+            except Exception:
+                pass
+            self._stop.wait(0.2)
+
+    def __enter__(self):
+        self._t = threading.Thread(target=self._run, daemon=True)
+        self._t.start()
+        return self
+
+    def __exit__(self, *a):
+        self._stop.set()
+        if self._t:
+            self._t.join(timeout=10)
+
+    def summary(self):
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit()]
+        mx = [float(s[2]) for s in self.samples if s[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for s in self.samples for i in range(4) if "Active" in s[5 + i]})
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.samples)}
+
+
+# ---- inputs ------------------------------------------------------------------------
+def build_inputs(torch, device):
+    import scl
+
+    t0 = time.time()
+    pts = scl.synthetic.mixture(N_CELLS, seed=0)
+    ki, kd = scl.synthetic.knn_device(pts, K_NN, device=device, block=2048)
+    del pts
+    torch.cuda.synchronize()
+    t_knn = time.time() - t0
+    return ki, kd, t_knn
+
+
+def flush_l2(torch, buf):
+    buf.add_(1.0)
+
+
+def timed_calls(torch, fn, steps, warmup, flush_buf, stream):
+    for _ in range(warmup):
+        fn()
+    torch.cuda.synchronize()
+    times = []
+    for _ in range(steps):
+        flush_l2(torch, flush_buf)
+        a = torch.cuda.Event(enable_timing=True)
+        b = torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        fn()
+        b.record(stream)
+        b.synchronize()
+        times.append(a.elapsed_time(b))
+    return times
+
+
+# ---- CPU baseline (scl-core's own implementation) ---------------------------------------
+def cpu_reference_diffusion(ip, ind, P, n, F, target_s=12.0, max_steps=N_STEPS):
+    """Times oracle/_ref f32_i32 diffuse_matrix on a bounded number of steps of
+    the full graph; returns (GB/s, steps_run, seconds, cores)."""
+    from oracle import ref
+
+    R = ref.RefLib("f32_i32")
+    X0 = np.random.default_rng(1).standard_normal((n, F)).astype(np.float32)
+    t0 = time.time()
+    R.diffuse_matrix(ip, ind, P, X0, 1)
+    t1 = time.time() - t0
+    steps = int(max(1, min(max_steps, target_s // max(t1, 1e-3))))
+    t0 = time.time()
+    R.diffuse_matrix(ip, ind, P, X0, steps)
+    dt = time.time() - t0
+    nnz = int(ind.size)
+    gbs = step_bytes(n, nnz, F) * steps / dt / 1e9
+    cores = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1))
+    return gbs, steps, dt, cores, R.path.name
+
+
+def cpu_model():
+    try:
+        for line in open("/proc/cpuinfo"):
+            if line.startswith("model name"):
+                return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    args = ap.parse_args()
+    warmup = max(3, args.warmup)
+
+    import torch
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    device = f"cuda:{local}"
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600), device_id=torch.device(device))
+
+    import scl
+
+    os.environ.setdefault("OMP_NUM_THREADS", str(os.cpu_count() or 1))
+    ki, kd, t_knn = build_inputs(torch, device)
+    stream = torch.cuda.current_stream()
+
+    if args.impl == "reference":
+        # scl-core's CPU path on the host cores; rank 0 only.
+        if rank == 0:
+            g = scl.gpu.GpuGraph.from_knn(ki, kd)
+            ip, ind, W = g.export()
+            del g
+            from oracle import ref
+
+            R = ref.RefLib("f32_i32")
+            n = N_CELLS
+            t0 = time.time()
+            P = R.transition(ip, ind, W, n)
+            t_tr = time.time() - t0
+            per = []
+            for _ in range(args.steps):
+                gbs, st, dt, cores, libname = cpu_reference_diffusion(ip, ind, P, n, N_FEAT, target_s=8.0)
+                per.append((gbs, st, dt))
+            gbs = float(np.median([p[0] for p in per]))
+            line = {"impl": "reference", "metric": METRIC, "value": round(gbs, 3), "unit": "GB/s", "n_gpus": world,
+                    "steps": args.steps, "warmup": 0, "ms_per_step": round(1e3 * np.median([p[2] for p in per]), 3),
+                    "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+                    "data": "synthetic (seeded 10-component 50-D mixture, kNN on device)",
+                    "config": {"workload": "diffusion 500k cells k=30 64 cols 16 steps (FP32, row-normalised)",
+                               "cells": n, "k": K_NN, "features": N_FEAT, "diffusion_steps": N_STEPS,
+                               "nnz": int(ind.size), "reference_steps_per_sample": per[0][1]},
+                    "cpu_baseline": {"value": round(gbs, 3), "unit": "GB/s", "cores": cores, "kind": "reference",
+                                     "sample": f"scl_diffusion_diffuse_matrix on the full 500k graph, "
+                                               f"{per[0][1]} of 16 steps per sample ({libname}, {cpu_model()})"},
+                    "transition_ms_cpu": round(1e3 * t_tr, 3),
+                    "e2e": {"value": round(gbs, 3), "unit": "GB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+            print(json.dumps(line), flush=True)
+        if dist is not None:
+            dist.barrier()
+            dist.destroy_process_group()
+        return
+
+    # ---- graph build on the device (timed once, reported beside the metric) ----------
+    bt0 = torch.cuda.Event(enable_timing=True)
+    bt1 = torch.cuda.Event(enable_timing=True)
+    bt0.record(stream)
+    g = scl.gpu.GpuGraph.from_knn(ki, kd, stream=stream)
+    g.normalize(symmetric=False, stream=stream)
+    bt1.record(stream)
+    bt1.synchronize()
+    build_ms = bt0.elapsed_time(bt1)
+    n, _, nnz = g.shape
+    F, T = N_FEAT, N_STEPS
+    B32 = step_bytes(n, nnz, F)
+    B16 = step_bytes(n, nnz, F, s_val=2, s_x=2)
+    gen = torch.Generator(device=device).manual_seed(1 + rank)
+    X0 = torch.randn((n, F), device=device, dtype=torch.float32, generator=gen)
+    Y = torch.empty_like(X0)
+    flush = torch.empty(64 * 1024 * 1024, device=device, dtype=torch.float32)
+
+    def run_f32():
+        g.diffuse(X0, T, out=Y, stream=stream)
+
+    if dist is not None:
+        dist.barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(local) as clk:
+        times = timed_calls(torch, run_f32, args.steps, warmup, flush, stream)
+    torch.cuda.synchronize()
+    t_ms = float(np.mean(times))
+    if dist is not None:
+        tt = torch.tensor([t_ms], device=device)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        t_ms = float(tt.item())
+    value = world * B32 * T / (t_ms * 1e-3) / 1e9
+    per_launch_ms = t_ms / T
+    peak, peak_kind = load_peaks()
+    achieved = B32 / (per_launch_ms * 1e-3) / 1e9
+
+    # ---- FP64 reference on the device for the precision forms --------------------------
+    ip, ind, Pm = g.export()
+    forms = {}
+    if rank == 0:
+        g64 = scl.gpu.GpuGraph.from_knn(ki, kd, variant="f64_i64")  # same W, FP64 normalisation below
+        ip64, ind64, W32 = g64.export()
+        g64.close()
+        g64 = scl.gpu.GpuGraph.from_csr(ip64, ind64, W32.astype(np.float64), (n, n), variant="f64_i64")
+        g64.normalize(symmetric=False)
+        Y64 = g64.diffuse(X0.double(), T)
+        Y32 = Y.clone()
+        err32 = float(torch.linalg.norm(Y32.double() - Y64) / torch.linalg.norm(Y64))
+        forms["f32"] = {"gbs": round(value / world, 2), "ms": round(t_ms, 4), "rel_fro_err_vs_fp64": err32,
+                        "max_rel_err_vs_fp64": float(((Y32.double() - Y64).abs() / Y64.abs().clamp_min(1e-3)).max())}
+        for name, tdt in (("bf16", torch.bfloat16), ("f16", torch.float16)):
+            g.set_storage(tdt, stream=stream)
+            Xl = X0.to(tdt)
+            Yl = torch.empty((n, F), device=device, dtype=torch.float32)
+
+            def run_l():
+                g.diffuse(Xl, T, out=Yl, stream=stream)
+
+            tl = float(np.mean(timed_calls(torch, run_l, args.steps, warmup, flush, stream)))
+            err = float(torch.linalg.norm(Yl.double() - Y64) / torch.linalg.norm(Y64))
+            # per-step errors vs FP64 (rounded iterates)
+            step_err = []
+            Xs, X64s = Xl, X0.double()
+            for s in range(T):
+                Xs = g.diffuse(Xs, 1, out_dtype=tdt)
+                X64s = g64.diffuse(X64s, 1)
+                step_err.append(float(torch.linalg.norm(Xs.double() - X64s) / torch.linalg.norm(X64s)))
+            forms[name] = {"gbs": round(B16 * T / (tl * 1e-3) / 1e9, 2), "ms": round(tl, 4),
+                           "speedup_vs_f32": round(t_ms / tl, 3), "rel_fro_err_vs_fp64": err,
+                           "max_rel_err_vs_fp64": float(((Yl.double() - Y64).abs() / Y64.abs().clamp_min(1e-3)).max()),
+                           "per_step_rel_fro_err": [round(e, 7) for e in step_err]}
+        g.set_storage(torch.float32, stream=stream)
+        g64.close()
+        del Y64
+
+    # ---- end to end through the drop-in C ABI with pinned host buffers --------------------
+    e2e = None
+    if not args.no_e2e:
+        Xh = torch.empty((n, F), dtype=torch.float32).pin_memory()
+        iph = torch.from_numpy(ip.astype(np.int32)).pin_memory()
+        indh = torch.from_numpy(ind).pin_memory()
+        Ph = torch.from_numpy(Pm).pin_memory()
+        X0h = X0.cpu().numpy()
+        m = scl.CsrMatrix.wrap(iph.numpy(), indh.numpy(), Ph.numpy(), (n, n))
+        Xn = Xh.numpy()
+        et = []
+        for it in range(warmup + args.steps):
+            Xn[...] = X0h
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            scl.diffusion.diffuse_matrix(m, Xn, T)
+            dt = time.perf_counter() - t0
+            if it >= warmup:
+                et.append(dt)
+        st = scl.diffusion.last_stats(m.lib)
+        e_s = float(np.mean(et))
+        if dist is not None:
+            tt = torch.tensor([e_s], device=device)
+            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+            e_s = float(tt.item())
+        e2e = {"value": round(world * B32 * T / e_s / 1e9, 3), "unit": "GB/s",
+               "h2d_bytes_per_step": int(st["h2d_bytes"]), "d2h_bytes_per_step": int(st["d2h_bytes"]),
+               "ms_per_step": round(1e3 * e_s, 3), "api": "scl_diffusion_diffuse_matrix (libscl_f32_i32.so)",
+               "bit_exact_vs_device_path": bool(np.array_equal(Xn.view(np.uint32),
+                                                               Y.cpu().numpy().view(np.uint32)))}
+        del m
+
+    # ---- CPU baseline (rank 0, N=1) ------------------------------------------------------------
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        try:
+            gbs, st_, dt, cores, libname = cpu_reference_diffusion(ip, ind, Pm, n, F, target_s=12.0)
+            cpu = {"value": round(gbs, 3), "unit": "GB/s", "cores": cores, "kind": "reference",
+                   "sample": f"scl_diffusion_diffuse_matrix (scl-core compiled, {libname}) on the full 500k graph, "
+                             f"{st_} of 16 steps, {dt:.1f} s, {cpu_model()}"}
+        except Exception as e:  # the baseline is informational; never fail the run on it
+            cpu = {"value": None, "unit": "GB/s", "cores": os.cpu_count(), "kind": "reference",
+                   "sample": f"unavailable: {e}"}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": round(value, 3), "unit": "GB/s", "n_gpus": world, "steps": args.steps,
+            "warmup": warmup, "ms_per_step": round(t_ms, 4), "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (seeded 10-component 50-D mixture; kNN computed on device, untimed)",
+            "config": {"workload": "diffusion 500k cells k=30 64 cols 16 steps (FP32 plain, row-normalised)",
+                       "cells": n, "k": K_NN, "features": F, "diffusion_steps": T, "nnz": nnz,
+                       "bytes_per_spmm_step": B32, "l2": "flushed (256 MiB write) before every timed step",
+                       "parallelism": f"replicas x{world}"},
+            "gpu_launches": args.steps * T,
+            "roofline": {"bound": "hbm", "achieved": round(achieved, 2), "peak": peak, "unit": "GB/s",
+                         "frac": round(achieved / peak, 4), "traffic": None, "peak_kind": peak_kind,
+                         "kernel": "k_spmm<float,float,float,float,16,4,8>",
+                         "per_launch_ms": round(per_launch_ms, 5)},
+            "forms": forms,
+            "fwd_bwd_ms": None,
+            "graph_build_ms": round(build_ms, 3),
+            "knn_harness_s": round(t_knn, 2),
+            "e2e": e2e,
+            "cpu_baseline": cpu,
+            "clocks": clk.summary(),
+        }
+        print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

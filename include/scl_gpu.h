@@ -1,0 +1,88 @@
+/*
+ * scl_gpu.h — device-pointer extension C ABI of the B200 diffusion libraries.
+ *
+ * No counterpart in scl-core: scl-core is CPU-only and its diffusion ABI
+ * (scl/binding/c_api/diffusion.h) takes host arrays. These entry points keep
+ * the graph and the dense blocks resident in GPU memory and take raw device
+ * pointers plus a CUDA stream (passed as void*, 0 = legacy default stream), so
+ * an autograd wrapper or a caller with its own device buffers can drive the
+ * same kernels without host round trips. Calls are asynchronous on `stream`
+ * unless noted; only plain pointers, sizes and enums cross the boundary.
+ */
+#ifndef SCL_B200_GPU_H
+#define SCL_B200_GPU_H
+
+#include <stdint.h>
+
+#include "scl_core.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+  SCL_DTYPE_F32 = 0,
+  SCL_DTYPE_F64 = 1,
+  SCL_DTYPE_BF16 = 2,
+  SCL_DTYPE_F16 = 3,
+  SCL_DTYPE_I32 = 4,
+  SCL_DTYPE_I64 = 5
+} scl_dtype_t;
+
+typedef struct scl_gpu_graph scl_gpu_graph;
+typedef scl_gpu_graph* scl_gpu_graph_t;
+
+/* Gaussian kNN affinity graph built on the device from kNN lists
+ * (knn_idx int32 n x k, -1 = no neighbour; knn_dist float32 n x k):
+ * sigma_i = max of row i's distances (floored at 1e-10), w = exp(-(d/sigma_i)^2),
+ * then S = (W + W^T)/2 over the union of kNN pairs, rows sorted by column.
+ * The result holds S as its f32 weights. Synchronises `stream`. */
+SCL_EXPORT scl_error_t scl_gpu_graph_from_knn(scl_gpu_graph_t* out, int64_t n, int64_t k, const int32_t* knn_idx,
+                                              const float* knn_dist, void* stream);
+
+/* Copy a CSR matrix (host arrays when on_device == 0, device arrays otherwise)
+ * into a device graph. indptr: i32/i64 [n_rows + 1]; indices: i32/i64 [nnz];
+ * values: f32/f64 [nnz]. Indices are validated (SCL_ERROR_INDEX_OUT_OF_BOUNDS).
+ * Synchronises `stream`. */
+SCL_EXPORT scl_error_t scl_gpu_graph_from_csr(scl_gpu_graph_t* out, int64_t n_rows, int64_t n_cols, int64_t nnz,
+                                              const void* indptr, scl_dtype_t indptr_dtype, const void* indices,
+                                              scl_dtype_t indices_dtype, const void* values,
+                                              scl_dtype_t values_dtype, int on_device, void* stream);
+
+SCL_EXPORT scl_error_t scl_gpu_graph_destroy(scl_gpu_graph_t* graph);
+
+SCL_EXPORT scl_error_t scl_gpu_graph_shape(scl_gpu_graph_t graph, int64_t* n_rows, int64_t* n_cols, int64_t* nnz);
+
+/* Transition matrix in place (the device form of
+ * scl_diffusion_compute_transition_matrix): symmetric 0 = D^-1 W, 1 = D^-1/2 W D^-1/2.
+ * degree_mode 0 = FP64 degrees (default), 1 = value-type arithmetic as scl-core.
+ * The pre-normalisation weights and FP64 degrees are kept for the backward pass. */
+SCL_EXPORT scl_error_t scl_gpu_graph_normalize(scl_gpu_graph_t graph, int symmetric, int degree_mode, void* stream);
+
+/* Copy the graph out: indptr int64 [n_rows + 1], indices int32 [nnz], values in
+ * the graph's master dtype (f32 or f64) [nnz]; any pointer may be NULL.
+ * Host destinations when on_device == 0 (synchronises `stream`). */
+SCL_EXPORT scl_error_t scl_gpu_graph_export(scl_gpu_graph_t graph, int64_t* indptr, int32_t* indices, void* values,
+                                            int on_device, void* stream);
+
+/* Storage precision of the values the SpMM reads: F32, F64, BF16 or F16
+ * (rounded once, RNE, from the master values). Iterates are stored in the same
+ * type; accumulation is FP32 (FP64 for F64). */
+SCL_EXPORT scl_error_t scl_gpu_graph_set_storage(scl_gpu_graph_t graph, scl_dtype_t dtype, void* stream);
+
+/* Y = P^n_steps X on device buffers (row-major n_rows x n_features). X is read
+ * as x_dtype and rounded once to the storage dtype if they differ; the final
+ * iterate is written as y_dtype (storage dtype or F32). X may equal Y. */
+SCL_EXPORT scl_error_t scl_gpu_diffuse(scl_gpu_graph_t graph, const void* X, scl_dtype_t x_dtype, void* Y,
+                                       scl_dtype_t y_dtype, int64_t n_features, int64_t n_steps, void* stream);
+
+/* One Y = P X with an explicit launch shape (group lanes per row in
+ * {1,2,4,8,16,32}; vec = 16 bytes / element size, or 1). group <= 0 picks the
+ * default. X and Y must be in the storage dtype (Y may also be F32). */
+SCL_EXPORT scl_error_t scl_gpu_spmm(scl_gpu_graph_t graph, const void* X, void* Y, scl_dtype_t y_dtype,
+                                    int64_t n_features, int group, int vec, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* SCL_B200_GPU_H */

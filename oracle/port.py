@@ -1,0 +1,193 @@
+"""ORACLE — test infrastructure only.
+
+NumPy front-end of the C restatement in ``diffusion_oracle.c`` (built into
+``oracle/_build/liboracle_port.so`` by ``make -C oracle port``). All index
+arrays are converted to int64; every function returns new arrays.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from pathlib import Path
+
+import numpy as np
+
+_HERE = Path(__file__).resolve().parent
+_LIB_PATH = _HERE / "_build" / "liboracle_port.so"
+_lib = None
+
+F32, BF16, F16 = 0, 2, 3
+
+_p = ctypes.c_void_p
+_i64 = ctypes.c_int64
+_int = ctypes.c_int
+
+_SIGS = {
+    "oracle_row_sums_f32": ([_i64, _p, _p, _p], None),
+    "oracle_row_sums_f64": ([_i64, _p, _p, _p], None),
+    "oracle_transition_f32": ([_i64, _p, _p, _p, _int, _int], None),
+    "oracle_transition_f64": ([_i64, _p, _p, _p, _int], None),
+    "oracle_spmm_f32": ([_i64, _p, _p, _p, _p, _p, _i64], None),
+    "oracle_spmm_f64": ([_i64, _p, _p, _p, _p, _p, _i64], None),
+    "oracle_diffuse_matrix_f32": ([_i64, _p, _p, _p, _p, _i64, _i64], None),
+    "oracle_diffuse_matrix_f64": ([_i64, _p, _p, _p, _p, _i64, _i64], None),
+    "oracle_diffuse_lowp": ([_i64, _p, _p, _p, _p, _p, _i64, _i64, _int, _int], None),
+    "oracle_f32_to_bf16": ([ctypes.c_float], ctypes.c_uint16),
+    "oracle_bf16_to_f32": ([ctypes.c_uint16], ctypes.c_float),
+    "oracle_f32_to_f16": ([ctypes.c_float], ctypes.c_uint16),
+    "oracle_f16_to_f32": ([ctypes.c_uint16], ctypes.c_float),
+    "oracle_gauss_weights_f64": ([_i64, _i64, _p, _p, _p, _p], None),
+    "oracle_gauss_weights_f32": ([_i64, _i64, _p, _p, _p, _p], None),
+    "oracle_symmetrize_f64": ([_i64, _i64, _p, _p, _p, _p, _p], _i64),
+    "oracle_symmetrize_f32": ([_i64, _i64, _p, _p, _p, _p, _p], _i64),
+    "oracle_adjoint_f64": ([_i64, _p, _p, _p, _int, _p, _p, _i64, _i64, _p, _p], ctypes.c_double),
+}
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not _LIB_PATH.exists():
+            raise RuntimeError(f"oracle port library missing: {_LIB_PATH} (run `make -C oracle port`)")
+        _lib = ctypes.CDLL(str(_LIB_PATH))
+        for name, (argt, rest) in _SIGS.items():
+            fn = getattr(_lib, name)
+            fn.argtypes = argt
+            fn.restype = rest
+    return _lib
+
+
+def _ptr(a: np.ndarray):
+    return a.ctypes.data_as(ctypes.c_void_p)
+
+
+def _csr(indptr, indices):
+    return (np.ascontiguousarray(indptr, dtype=np.int64),
+            np.ascontiguousarray(indices, dtype=np.int64))
+
+
+def row_sums(indptr, values):
+    indptr = np.ascontiguousarray(indptr, dtype=np.int64)
+    n = indptr.size - 1
+    if values.dtype == np.float32:
+        out = np.empty(n, np.float32)
+        lib().oracle_row_sums_f32(n, _ptr(indptr), _ptr(values), _ptr(out))
+    else:
+        values = np.ascontiguousarray(values, dtype=np.float64)
+        out = np.empty(n, np.float64)
+        lib().oracle_row_sums_f64(n, _ptr(indptr), _ptr(values), _ptr(out))
+    return out
+
+
+def transition(indptr, indices, values, symmetric=False, degree_fp64=False):
+    """Normalised copy of ``values`` (diffusion.hpp:492-603)."""
+    indptr, indices = _csr(indptr, indices)
+    n = indptr.size - 1
+    if values.dtype == np.float32:
+        out = np.array(values, dtype=np.float32, copy=True)
+        lib().oracle_transition_f32(n, _ptr(indptr), _ptr(indices), _ptr(out), int(symmetric), int(degree_fp64))
+    else:
+        out = np.array(values, dtype=np.float64, copy=True)
+        lib().oracle_transition_f64(n, _ptr(indptr), _ptr(indices), _ptr(out), int(symmetric))
+    return out
+
+
+def spmm(indptr, indices, values, X):
+    indptr, indices = _csr(indptr, indices)
+    n = indptr.size - 1
+    X = np.ascontiguousarray(X)
+    F = X.shape[1]
+    Y = np.empty((n, F), X.dtype)
+    if X.dtype == np.float32:
+        v = np.ascontiguousarray(values, np.float32)
+        lib().oracle_spmm_f32(n, _ptr(indptr), _ptr(indices), _ptr(v), _ptr(X), _ptr(Y), F)
+    else:
+        v = np.ascontiguousarray(values, np.float64)
+        lib().oracle_spmm_f64(n, _ptr(indptr), _ptr(indices), _ptr(v), _ptr(X), _ptr(Y), F)
+    return Y
+
+
+def diffuse_matrix(indptr, indices, values, X, steps):
+    """X_steps = P^steps X0 (diffusion.hpp:638-664); dtype follows X."""
+    indptr, indices = _csr(indptr, indices)
+    n = indptr.size - 1
+    X = np.array(X, copy=True, order="C")
+    F = X.shape[1] if X.ndim == 2 else 1
+    if X.dtype == np.float32:
+        v = np.ascontiguousarray(values, np.float32)
+        lib().oracle_diffuse_matrix_f32(n, _ptr(indptr), _ptr(indices), _ptr(v), _ptr(X), F, steps)
+    else:
+        v = np.ascontiguousarray(values, np.float64)
+        lib().oracle_diffuse_matrix_f64(n, _ptr(indptr), _ptr(indices), _ptr(v), _ptr(X), F, steps)
+    return X
+
+
+def diffuse_lowp(indptr, indices, values_f32, X0_f32, steps, kind, final_f32=True):
+    indptr, indices = _csr(indptr, indices)
+    n = indptr.size - 1
+    v = np.ascontiguousarray(values_f32, np.float32)
+    X0 = np.ascontiguousarray(X0_f32, np.float32)
+    F = X0.shape[1]
+    Y = np.empty((n, F), np.float32)
+    lib().oracle_diffuse_lowp(n, _ptr(indptr), _ptr(indices), _ptr(v), _ptr(X0), _ptr(Y), F, steps,
+                              int(kind), int(final_f32))
+    return Y
+
+
+def to_bf16_bits(x):
+    f = lib().oracle_f32_to_bf16
+    return np.array([f(float(v)) for v in np.asarray(x, np.float32).ravel()], np.uint16)
+
+
+def to_f16_bits(x):
+    f = lib().oracle_f32_to_f16
+    return np.array([f(float(v)) for v in np.asarray(x, np.float32).ravel()], np.uint16)
+
+
+def gauss_weights(knn_idx, knn_dist):
+    """(sigma, w) for an n x k kNN list; FP64 when knn_dist is float64."""
+    knn_idx = np.ascontiguousarray(knn_idx, np.int64)
+    n, k = knn_idx.shape
+    if knn_dist.dtype == np.float32:
+        d = np.ascontiguousarray(knn_dist, np.float32)
+        sigma = np.empty(n, np.float32)
+        w = np.empty((n, k), np.float32)
+        lib().oracle_gauss_weights_f32(n, k, _ptr(knn_idx), _ptr(d), _ptr(sigma), _ptr(w))
+    else:
+        d = np.ascontiguousarray(knn_dist, np.float64)
+        sigma = np.empty(n, np.float64)
+        w = np.empty((n, k), np.float64)
+        lib().oracle_gauss_weights_f64(n, k, _ptr(knn_idx), _ptr(d), _ptr(sigma), _ptr(w))
+    return sigma, w
+
+
+def symmetrize(knn_idx, w):
+    """CSR (indptr, indices, values) of (W + W^T)/2 over the kNN union."""
+    knn_idx = np.ascontiguousarray(knn_idx, np.int64)
+    n, k = knn_idx.shape
+    if w.dtype == np.float32:
+        fn, dt = lib().oracle_symmetrize_f32, np.float32
+    else:
+        fn, dt = lib().oracle_symmetrize_f64, np.float64
+    w = np.ascontiguousarray(w, dt)
+    nnz = fn(n, k, _ptr(knn_idx), _ptr(w), None, None, None)
+    indptr = np.empty(n + 1, np.int64)
+    indices = np.empty(max(nnz, 1), np.int64)
+    values = np.empty(max(nnz, 1), dt)
+    fn(n, k, _ptr(knn_idx), _ptr(w), _ptr(indptr), _ptr(indices), _ptr(values))
+    return indptr, indices[:nnz], values[:nnz]
+
+
+def adjoint(indptr, indices, W, X0, Y, steps, symmetric=False):
+    """(loss, dL/dX0, dL/dW) in FP64 for L = sum((P^steps X0 - Y)^2)."""
+    indptr, indices = _csr(indptr, indices)
+    n = indptr.size - 1
+    W = np.ascontiguousarray(W, np.float64)
+    X0 = np.ascontiguousarray(X0, np.float64)
+    Y = np.ascontiguousarray(Y, np.float64)
+    F = X0.shape[1]
+    dX0 = np.empty_like(X0)
+    dW = np.empty_like(W)
+    loss = lib().oracle_adjoint_f64(n, _ptr(indptr), _ptr(indices), _ptr(W), int(symmetric), _ptr(X0), _ptr(Y),
+                                    F, steps, _ptr(dX0), _ptr(dW))
+    return loss, dX0, dW

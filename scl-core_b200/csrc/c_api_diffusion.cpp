@@ -1,0 +1,305 @@
+// Drop-in diffusion C ABI executed on the GPU.
+// Replaces scl/binding/c_api/diffusion.cpp:36-116 and 318-341 (argument
+// checks, defaults and messages kept) with uploads + CUDA kernels.
+#include <cstring>
+#include <vector>
+
+#include "abi.hpp"
+#include "scl_diffusion.h"
+
+using sclabi::Index;
+using sclabi::Real;
+using namespace sclgpu;
+
+namespace sclabi {
+
+// Device copy of a handle's primary-major arrays.
+struct DeviceMirror {
+  int device = -1;
+  DeviceCSR g;
+};
+
+}  // namespace sclabi
+
+namespace {
+
+thread_local int t_degree_mode = 0;
+struct Stats {
+  double device_ms = 0, h2d = 0, d2h = 0;
+};
+thread_local Stats t_stats;
+
+// Host -> device copy of the handle (indptr int64, indices int32, values Real).
+// Rows whose storage is adjacent are copied as one run.
+std::shared_ptr<sclabi::DeviceMirror> upload(const scl_sparse_matrix& m, cudaStream_t s, double& h2d) {
+  auto mir = std::make_shared<sclabi::DeviceMirror>();
+  mir->device = current_device();
+  DeviceCSR& g = mir->g;
+  const Index pdim = m.primary_dim();
+  const std::vector<int64_t> off = sclabi::offsets_of(m);
+  const int64_t nnz = off[pdim];
+  g.n_rows = pdim;
+  g.n_cols = m.secondary_dim();
+  g.nnz = nnz;
+  g.vtype = sclabi::kRealDType;
+  g.indptr = DevBuf((pdim + 1) * sizeof(int64_t), s);
+  g.indices = DevBuf(std::max<int64_t>(nnz, 1) * sizeof(int32_t), s);
+  g.values = DevBuf(std::max<int64_t>(nnz, 1) * sizeof(Real), s);
+  SCL_REQUIRE(m.secondary_dim() <= 0x7fffffff, SCL_ERROR_INVALID_ARGUMENT, "dimension exceeds the int32 column range");
+  SCL_CUDA(cudaMemcpyAsync(g.indptr.p, off.data(), (pdim + 1) * sizeof(int64_t), cudaMemcpyHostToDevice, s));
+  h2d += (double)(pdim + 1) * sizeof(int64_t);
+  DevBuf idx_tmp;
+  void* idx_dst = g.indices.p;
+  if (sizeof(Index) != sizeof(int32_t)) {
+    idx_tmp = DevBuf(std::max<int64_t>(nnz, 1) * sizeof(Index), s);
+    idx_dst = idx_tmp.p;
+  }
+  Index i = 0;
+  while (i < pdim) {
+    if (m.lengths[i] == 0) { ++i; continue; }
+    Index j = i + 1;
+    int64_t run = m.lengths[i];
+    while (j < pdim && (m.lengths[j] == 0 ||
+                        (m.data_ptrs[j] == m.data_ptrs[i] + run && m.index_ptrs[j] == m.index_ptrs[i] + run))) {
+      run += m.lengths[j];
+      ++j;
+    }
+    SCL_CUDA(cudaMemcpyAsync(static_cast<char*>(g.values.p) + off[i] * sizeof(Real), m.data_ptrs[i], run * sizeof(Real),
+                             cudaMemcpyHostToDevice, s));
+    SCL_CUDA(cudaMemcpyAsync(static_cast<char*>(idx_dst) + off[i] * sizeof(Index), m.index_ptrs[i], run * sizeof(Index),
+                             cudaMemcpyHostToDevice, s));
+    h2d += (double)run * (sizeof(Real) + sizeof(Index));
+    i = j;
+  }
+  if (idx_tmp.p) convert_indices(idx_tmp.p, sclabi::kIndexDType, g.indices.as<int32_t>(), nnz, s);
+  DevStatus st(s);
+  validate_csr(g, st.ptr(), s);
+  st.check(s, "invalid sparse structure: column index out of range or malformed offsets");
+  return mir;
+}
+
+std::shared_ptr<sclabi::DeviceMirror> device_graph(scl_sparse_matrix& m, cudaStream_t s, double& h2d) {
+  if (m.mirror && m.mirror->device == current_device()) return m.mirror;
+  return upload(m, s, h2d);
+}
+
+struct EventTimer {
+  cudaEvent_t a = nullptr, b = nullptr;
+  cudaStream_t s;
+  explicit EventTimer(cudaStream_t st) : s(st) {
+    SCL_CUDA(cudaEventCreate(&a));
+    SCL_CUDA(cudaEventCreate(&b));
+  }
+  ~EventTimer() {
+    if (a) cudaEventDestroy(a);
+    if (b) cudaEventDestroy(b);
+  }
+  void start() { SCL_CUDA(cudaEventRecord(a, s)); }
+  void stop() { SCL_CUDA(cudaEventRecord(b, s)); }
+  double ms() {
+    SCL_CUDA(cudaEventSynchronize(b));
+    float t = 0;
+    SCL_CUDA(cudaEventElapsedTime(&t, a, b));
+    return t;
+  }
+};
+
+// X (n x F) <- P^steps X on the device; shared by diffuse_matrix / magic_impute.
+void diffuse_host_block(scl_sparse_matrix& m, Real* X, Index n_nodes, Index n_features, Index n_steps) {
+  SCL_REQUIRE(m.valid, SCL_ERROR_INVALID_ARGUMENT, "Transition matrix is not valid");
+  SCL_REQUIRE(n_nodes == m.primary_dim(), SCL_ERROR_DIMENSION_MISMATCH,
+              "Diffusion: n_nodes must equal the transition matrix's primary dimension");
+  SCL_REQUIRE(m.secondary_dim() <= n_nodes, SCL_ERROR_DIMENSION_MISMATCH,
+              "Diffusion: column indices would address rows beyond n_nodes");
+  const int dev = current_device();
+  cudaStream_t s = library_stream(dev);
+  Stats st;
+  auto mir = device_graph(m, s, st.h2d);
+  const int64_t total = (int64_t)n_nodes * n_features;
+  DevBuf Xd(total * sizeof(Real), s);
+  SCL_CUDA(cudaMemcpyAsync(Xd.p, X, total * sizeof(Real), cudaMemcpyHostToDevice, s));
+  st.h2d += (double)total * sizeof(Real);
+  EventTimer tm(s);
+  tm.start();
+  diffuse(mir->g.view(), Xd.p, sclabi::kRealDType, Xd.p, sclabi::kRealDType, sclabi::kRealDType, n_features, n_steps, s);
+  tm.stop();
+  SCL_CUDA(cudaMemcpyAsync(X, Xd.p, total * sizeof(Real), cudaMemcpyDeviceToHost, s));
+  st.d2h += (double)total * sizeof(Real);
+  SCL_CUDA(cudaStreamSynchronize(s));
+  st.device_ms = tm.ms();
+  t_stats = st;
+}
+
+}  // namespace
+
+extern "C" {
+
+SCL_EXPORT scl_error_t scl_diffusion_compute_transition_matrix(scl_sparse_t adjacency, int symmetric) {
+  SCL_API_CHECK_NULL(adjacency, "Adjacency matrix is null");
+  SCL_API_TRY
+  Real* values = adjacency->contiguous_data();
+  SCL_API_CHECK(values != nullptr, SCL_ERROR_INVALID_ARGUMENT,
+                "Matrix must be contiguous for transition matrix computation");
+  SCL_API_CHECK(!symmetric || adjacency->rows == adjacency->cols, SCL_ERROR_DIMENSION_MISMATCH,
+                "Symmetric normalization needs a square matrix");
+  const int dev = current_device();
+  cudaStream_t s = library_stream(dev);
+  Stats st;
+  auto mir = device_graph(*adjacency, s, st.h2d);
+  EventTimer tm(s);
+  tm.start();
+  normalize(mir->g, symmetric != 0, t_degree_mode, nullptr, s);
+  tm.stop();
+  SCL_CUDA(cudaMemcpyAsync(values, mir->g.values.p, mir->g.nnz * sizeof(Real), cudaMemcpyDeviceToHost, s));
+  st.d2h += (double)mir->g.nnz * sizeof(Real);
+  SCL_CUDA(cudaStreamSynchronize(s));
+  st.device_ms = tm.ms();
+  t_stats = st;
+  SCL_API_RETURN_OK;
+  SCL_API_CATCH
+}
+
+SCL_EXPORT scl_error_t scl_diffusion_diffuse_vector(scl_sparse_t transition, scl_real_t* x, scl_size_t n_nodes,
+                                                    scl_index_t n_steps) {
+  SCL_API_CHECK_NULL(transition, "Transition matrix is null");
+  SCL_API_CHECK_NULL(x, "Vector x is null");
+  SCL_API_CHECK(n_nodes > 0 && n_steps > 0, SCL_ERROR_INVALID_ARGUMENT, "Dimensions must be positive");
+  SCL_API_TRY
+  scl_sparse_matrix& m = *transition;
+  SCL_REQUIRE(m.valid, SCL_ERROR_INVALID_ARGUMENT, "Transition matrix is not valid");
+  const int64_t N = m.primary_dim();
+  // diffusion.hpp:617: SCL_CHECK_DIM(x.len >= N, ...)
+  SCL_REQUIRE((int64_t)n_nodes >= N, SCL_ERROR_DIMENSION_MISMATCH, "Diffusion: vector size mismatch");
+  SCL_REQUIRE((int64_t)m.secondary_dim() <= (int64_t)n_nodes, SCL_ERROR_DIMENSION_MISMATCH,
+              "Diffusion: column indices would address entries beyond n_nodes");
+  const int dev = current_device();
+  cudaStream_t s = library_stream(dev);
+  Stats st;
+  auto mir = device_graph(m, s, st.h2d);
+  const int64_t nn = (int64_t)n_nodes;
+  DevBuf xd(nn * sizeof(Real), s);
+  SCL_CUDA(cudaMemcpyAsync(xd.p, x, nn * sizeof(Real), cudaMemcpyHostToDevice, s));
+  st.h2d += (double)nn * sizeof(Real);
+  EventTimer tm(s);
+  tm.start();
+  if (nn == N) {
+    diffuse(mir->g.view(), xd.p, sclabi::kRealDType, xd.p, sclabi::kRealDType, sclabi::kRealDType, 1, n_steps, s);
+  } else {
+    // Entries beyond the primary dimension keep their input values and are
+    // read by later steps, as in the reference's memcpy of N entries.
+    DevBuf tmp(std::max<int64_t>(N, 1) * sizeof(Real), s);
+    SpmmArgs a{};
+    const CsrView v = mir->g.view();
+    a.indptr = v.indptr; a.indices = v.indices; a.values = v.values; a.vtype = v.vtype;
+    a.n_rows = N; a.F = 1;
+    a.X = xd.p; a.xtype = sclabi::kRealDType; a.Y = tmp.p; a.ytype = sclabi::kRealDType;
+    for (Index t = 0; t < n_steps; ++t) {
+      spmm(a, s);
+      SCL_CUDA(cudaMemcpyAsync(xd.p, tmp.p, N * sizeof(Real), cudaMemcpyDeviceToDevice, s));
+    }
+  }
+  tm.stop();
+  SCL_CUDA(cudaMemcpyAsync(x, xd.p, nn * sizeof(Real), cudaMemcpyDeviceToHost, s));
+  st.d2h += (double)nn * sizeof(Real);
+  SCL_CUDA(cudaStreamSynchronize(s));
+  st.device_ms = tm.ms();
+  t_stats = st;
+  SCL_API_RETURN_OK;
+  SCL_API_CATCH
+}
+
+SCL_EXPORT scl_error_t scl_diffusion_diffuse_matrix(scl_sparse_t transition, scl_real_t* X, scl_index_t n_nodes,
+                                                    scl_index_t n_features, scl_index_t n_steps) {
+  SCL_API_CHECK_NULL(transition, "Transition matrix is null");
+  SCL_API_CHECK_NULL(X, "Matrix X is null");
+  SCL_API_CHECK(n_nodes > 0 && n_features > 0 && n_steps > 0, SCL_ERROR_INVALID_ARGUMENT,
+                "Dimensions must be positive");
+  SCL_API_TRY
+  diffuse_host_block(*transition, X, n_nodes, n_features, n_steps);
+  SCL_API_RETURN_OK;
+  SCL_API_CATCH
+}
+
+SCL_EXPORT scl_error_t scl_diffusion_magic_impute(scl_sparse_t transition, scl_real_t* X, scl_index_t n_nodes,
+                                                  scl_index_t n_features, scl_index_t t) {
+  SCL_API_CHECK_NULL(transition, "Transition matrix is null");
+  SCL_API_CHECK_NULL(X, "Matrix X is null");
+  SCL_API_CHECK(n_nodes > 0 && n_features > 0, SCL_ERROR_INVALID_ARGUMENT, "Dimensions must be positive");
+  SCL_API_TRY
+  const Index steps = (t == 0) ? 3 : t;  // diffusion.cpp:26 DEFAULT_N_STEPS
+  if (steps > 0) diffuse_host_block(*transition, X, n_nodes, n_features, steps);
+  SCL_API_RETURN_OK;
+  SCL_API_CATCH
+}
+
+#define SCL_NOT_IMPLEMENTED(name)                                                            \
+  do {                                                                                       \
+    sclabi::set_last_error(SCL_ERROR_NOT_IMPLEMENTED, name ": not implemented in the B200 build"); \
+    return SCL_ERROR_NOT_IMPLEMENTED;                                                        \
+  } while (0)
+
+SCL_EXPORT scl_error_t scl_diffusion_compute_dpt(scl_sparse_t, scl_index_t, scl_real_t*, scl_size_t, scl_index_t,
+                                                 scl_real_t) {
+  SCL_NOT_IMPLEMENTED("scl_diffusion_compute_dpt");
+}
+SCL_EXPORT scl_error_t scl_diffusion_compute_dpt_multi_root(scl_sparse_t, const scl_index_t*, scl_size_t, scl_real_t*,
+                                                            scl_size_t, scl_index_t) {
+  SCL_NOT_IMPLEMENTED("scl_diffusion_compute_dpt_multi_root");
+}
+SCL_EXPORT scl_error_t scl_diffusion_random_walk_with_restart(scl_sparse_t, const scl_index_t*, scl_size_t, scl_real_t*,
+                                                              scl_size_t, scl_real_t, scl_index_t, scl_real_t) {
+  SCL_NOT_IMPLEMENTED("scl_diffusion_random_walk_with_restart");
+}
+SCL_EXPORT scl_error_t scl_diffusion_personalized_pagerank(scl_sparse_t, scl_index_t, scl_real_t*, scl_size_t,
+                                                           scl_real_t, scl_index_t, scl_real_t) {
+  SCL_NOT_IMPLEMENTED("scl_diffusion_personalized_pagerank");
+}
+SCL_EXPORT scl_error_t scl_diffusion_diffusion_map_embedding(scl_sparse_t, scl_real_t*, scl_index_t, scl_index_t,
+                                                             scl_index_t) {
+  SCL_NOT_IMPLEMENTED("scl_diffusion_diffusion_map_embedding");
+}
+SCL_EXPORT scl_error_t scl_diffusion_heat_kernel_signature(scl_sparse_t, scl_real_t*, scl_size_t, scl_real_t,
+                                                           scl_index_t) {
+  SCL_NOT_IMPLEMENTED("scl_diffusion_heat_kernel_signature");
+}
+SCL_EXPORT scl_error_t scl_diffusion_diffusion_distance(scl_sparse_t, scl_real_t*, scl_size_t, scl_index_t) {
+  SCL_NOT_IMPLEMENTED("scl_diffusion_diffusion_distance");
+}
+SCL_EXPORT scl_error_t scl_diffusion_lazy_random_walk(scl_sparse_t, scl_real_t*, scl_size_t, scl_index_t, scl_real_t) {
+  SCL_NOT_IMPLEMENTED("scl_diffusion_lazy_random_walk");
+}
+
+SCL_EXPORT scl_error_t scl_diffusion_gpu_set_degree_mode(int mode) {
+  SCL_API_CHECK(mode == 0 || mode == 1, SCL_ERROR_INVALID_ARGUMENT, "degree mode must be 0 (FP64) or 1 (native)");
+  t_degree_mode = mode;
+  SCL_API_RETURN_OK;
+}
+
+SCL_EXPORT scl_error_t scl_diffusion_gpu_attach(scl_sparse_t handle) {
+  SCL_API_CHECK_NULL(handle, "Matrix is null");
+  SCL_API_TRY
+  const int dev = current_device();
+  cudaStream_t s = library_stream(dev);
+  double h2d = 0;
+  handle->mirror = upload(*handle, s, h2d);
+  SCL_CUDA(cudaStreamSynchronize(s));
+  SCL_API_RETURN_OK;
+  SCL_API_CATCH
+}
+
+SCL_EXPORT scl_error_t scl_diffusion_gpu_detach(scl_sparse_t handle) {
+  SCL_API_CHECK_NULL(handle, "Matrix is null");
+  SCL_API_TRY
+  handle->mirror.reset();
+  SCL_API_RETURN_OK;
+  SCL_API_CATCH
+}
+
+SCL_EXPORT scl_error_t scl_diffusion_gpu_last_stats(double* device_ms, double* h2d_bytes, double* d2h_bytes) {
+  if (device_ms) *device_ms = t_stats.device_ms;
+  if (h2d_bytes) *h2d_bytes = t_stats.h2d;
+  if (d2h_bytes) *d2h_bytes = t_stats.d2h;
+  SCL_API_RETURN_OK;
+}
+
+}  // extern "C"

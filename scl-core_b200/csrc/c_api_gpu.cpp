@@ -1,0 +1,238 @@
+// Device-pointer extension C ABI (scl_gpu.h). No scl-core counterpart: these
+// entry points keep the graph resident on the GPU and take raw device buffers
+// and a caller stream, for the autograd wrapper and device-side callers.
+#include <cstring>
+#include <vector>
+
+#include "abi.hpp"
+#include "scl_gpu.h"
+
+using namespace sclgpu;
+
+struct scl_gpu_graph {
+  int device = -1;
+  DeviceCSR g;              // structure + master values (f32 or f64)
+  DevBuf store_vals;        // values in the storage dtype when it differs from master
+  DType store_type = kF32;  // dtype the SpMM reads
+  // kept by normalize() for the backward pass
+  DevBuf weights;           // pre-normalisation values (master dtype)
+  DevBuf degrees;           // FP64 row degrees of `weights`
+  int symmetric = 0;
+  bool normalized = false;
+
+  CsrView storage_view() const {
+    CsrView v = g.view();
+    if (store_type != g.vtype) {
+      v.values = store_vals.p;
+      v.vtype = store_type;
+    }
+    return v;
+  }
+};
+
+namespace {
+
+inline cudaStream_t as_stream(void* s) { return reinterpret_cast<cudaStream_t>(s); }
+
+DType checked_dtype(int t) {
+  SCL_REQUIRE(t >= SCL_DTYPE_F32 && t <= SCL_DTYPE_I64, SCL_ERROR_INVALID_ARGUMENT, "unknown dtype");
+  return static_cast<DType>(t);
+}
+
+void ensure_device(const scl_gpu_graph* g) {
+  SCL_REQUIRE(g->device == current_device(), SCL_ERROR_INVALID_ARGUMENT,
+              "graph lives on another device than the current one");
+}
+
+}  // namespace
+
+extern "C" {
+
+SCL_EXPORT scl_error_t scl_gpu_graph_from_knn(scl_gpu_graph_t* out, int64_t n, int64_t k, const int32_t* knn_idx,
+                                              const float* knn_dist, void* stream) {
+  SCL_API_CHECK_NULL(out, "Output pointer is null");
+  SCL_API_CHECK_NULL(knn_idx, "kNN index array is null");
+  SCL_API_CHECK_NULL(knn_dist, "kNN distance array is null");
+  SCL_API_CHECK(n > 0 && k > 0, SCL_ERROR_INVALID_ARGUMENT, "Dimensions must be positive");
+  SCL_API_TRY
+  cudaStream_t s = as_stream(stream);
+  auto h = std::make_unique<scl_gpu_graph>();
+  h->device = current_device();
+  DevBuf sigma(n * sizeof(float), s), w(n * k * sizeof(float), s);
+  gauss_weights(knn_idx, knn_dist, n, k, sigma.as<float>(), w.as<float>(), s);
+  symmetrize_knn(knn_idx, w.as<float>(), n, k, h->g, s);
+  h->store_type = kF32;
+  SCL_CUDA(cudaStreamSynchronize(s));
+  *out = h.release();
+  SCL_API_RETURN_OK;
+  SCL_API_CATCH
+}
+
+SCL_EXPORT scl_error_t scl_gpu_graph_from_csr(scl_gpu_graph_t* out, int64_t n_rows, int64_t n_cols, int64_t nnz,
+                                              const void* indptr, scl_dtype_t indptr_dtype, const void* indices,
+                                              scl_dtype_t indices_dtype, const void* values,
+                                              scl_dtype_t values_dtype, int on_device, void* stream) {
+  SCL_API_CHECK_NULL(out, "Output pointer is null");
+  SCL_API_CHECK_NULL(indptr, "Offset array pointer is null");
+  SCL_API_CHECK(n_rows > 0 && n_cols > 0, SCL_ERROR_INVALID_ARGUMENT, "Matrix dimensions must be positive");
+  SCL_API_CHECK(nnz >= 0, SCL_ERROR_INVALID_ARGUMENT, "Number of non-zeros must be non-negative");
+  SCL_API_CHECK(nnz == 0 || (indices != nullptr && values != nullptr), SCL_ERROR_NULL_POINTER,
+                "Index or value array pointer is null");
+  SCL_API_CHECK(n_cols <= 0x7fffffffLL, SCL_ERROR_INVALID_ARGUMENT, "n_cols exceeds the int32 column range");
+  SCL_API_TRY
+  const DType tp = checked_dtype(indptr_dtype), ti = checked_dtype(indices_dtype), tv = checked_dtype(values_dtype);
+  SCL_REQUIRE(tv == kF32 || tv == kF64, SCL_ERROR_TYPE_MISMATCH, "values must be f32 or f64");
+  cudaStream_t s = as_stream(stream);
+  auto h = std::make_unique<scl_gpu_graph>();
+  h->device = current_device();
+  DeviceCSR& g = h->g;
+  g.n_rows = n_rows;
+  g.n_cols = n_cols;
+  g.nnz = nnz;
+  g.vtype = tv;
+  g.indptr = DevBuf((n_rows + 1) * 8, s);
+  g.indices = DevBuf(std::max<int64_t>(nnz, 1) * 4, s);
+  g.values = DevBuf(std::max<int64_t>(nnz, 1) * dtype_size(tv), s);
+  const cudaMemcpyKind kind = on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
+  DevBuf tp_buf((n_rows + 1) * dtype_size(tp), s);
+  SCL_CUDA(cudaMemcpyAsync(tp_buf.p, indptr, (n_rows + 1) * dtype_size(tp), kind, s));
+  convert_offsets(tp_buf.p, tp, g.indptr.as<int64_t>(), n_rows + 1, s);
+  if (nnz > 0) {
+    DevBuf ti_buf(nnz * dtype_size(ti), s);
+    SCL_CUDA(cudaMemcpyAsync(ti_buf.p, indices, nnz * dtype_size(ti), kind, s));
+    convert_indices(ti_buf.p, ti, g.indices.as<int32_t>(), nnz, s);
+    SCL_CUDA(cudaMemcpyAsync(g.values.p, values, nnz * dtype_size(tv), kind, s));
+  }
+  DevStatus st(s);
+  validate_csr(g, st.ptr(), s);
+  st.check(s, "invalid CSR structure: column index out of range or malformed offsets");
+  h->store_type = tv;
+  *out = h.release();
+  SCL_API_RETURN_OK;
+  SCL_API_CATCH
+}
+
+SCL_EXPORT scl_error_t scl_gpu_graph_destroy(scl_gpu_graph_t* graph) {
+  if (graph == nullptr || *graph == nullptr) SCL_API_RETURN_OK;
+  SCL_API_TRY
+  delete *graph;
+  *graph = nullptr;
+  SCL_API_RETURN_OK;
+  SCL_API_CATCH
+}
+
+SCL_EXPORT scl_error_t scl_gpu_graph_shape(scl_gpu_graph_t graph, int64_t* n_rows, int64_t* n_cols, int64_t* nnz) {
+  SCL_API_CHECK_NULL(graph, "Graph is null");
+  if (n_rows) *n_rows = graph->g.n_rows;
+  if (n_cols) *n_cols = graph->g.n_cols;
+  if (nnz) *nnz = graph->g.nnz;
+  SCL_API_RETURN_OK;
+}
+
+SCL_EXPORT scl_error_t scl_gpu_graph_normalize(scl_gpu_graph_t graph, int symmetric, int degree_mode, void* stream) {
+  SCL_API_CHECK_NULL(graph, "Graph is null");
+  SCL_API_CHECK(degree_mode == 0 || degree_mode == 1, SCL_ERROR_INVALID_ARGUMENT, "degree mode must be 0 or 1");
+  SCL_API_TRY
+  ensure_device(graph);
+  cudaStream_t s = as_stream(stream);
+  DeviceCSR& g = graph->g;
+  const size_t vb = std::max<int64_t>(g.nnz, 1) * dtype_size(g.vtype);
+  graph->weights = DevBuf(vb, s);
+  SCL_CUDA(cudaMemcpyAsync(graph->weights.p, g.values.p, g.nnz * dtype_size(g.vtype), cudaMemcpyDeviceToDevice, s));
+  graph->degrees = DevBuf(std::max<int64_t>(g.n_rows, 1) * sizeof(double), s);
+  normalize(g, symmetric != 0, degree_mode, graph->degrees.as<double>(), s);
+  graph->symmetric = symmetric != 0;
+  graph->normalized = true;
+  if (graph->store_type != g.vtype) {
+    graph->store_vals = DevBuf(std::max<int64_t>(g.nnz, 1) * dtype_size(graph->store_type), s);
+    convert_values(g.values.p, g.vtype, graph->store_vals.p, graph->store_type, g.nnz, s);
+  }
+  SCL_API_RETURN_OK;
+  SCL_API_CATCH
+}
+
+SCL_EXPORT scl_error_t scl_gpu_graph_export(scl_gpu_graph_t graph, int64_t* indptr, int32_t* indices, void* values,
+                                            int on_device, void* stream) {
+  SCL_API_CHECK_NULL(graph, "Graph is null");
+  SCL_API_TRY
+  ensure_device(graph);
+  cudaStream_t s = as_stream(stream);
+  const DeviceCSR& g = graph->g;
+  const cudaMemcpyKind kind = on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost;
+  if (indptr) SCL_CUDA(cudaMemcpyAsync(indptr, g.indptr.p, (g.n_rows + 1) * 8, kind, s));
+  if (indices && g.nnz) SCL_CUDA(cudaMemcpyAsync(indices, g.indices.p, g.nnz * 4, kind, s));
+  if (values && g.nnz) SCL_CUDA(cudaMemcpyAsync(values, g.values.p, g.nnz * dtype_size(g.vtype), kind, s));
+  if (!on_device) SCL_CUDA(cudaStreamSynchronize(s));
+  SCL_API_RETURN_OK;
+  SCL_API_CATCH
+}
+
+SCL_EXPORT scl_error_t scl_gpu_graph_set_storage(scl_gpu_graph_t graph, scl_dtype_t dtype, void* stream) {
+  SCL_API_CHECK_NULL(graph, "Graph is null");
+  SCL_API_TRY
+  ensure_device(graph);
+  const DType t = checked_dtype(dtype);
+  SCL_REQUIRE(is_float_dtype(t), SCL_ERROR_TYPE_MISMATCH, "storage dtype must be f32, f64, bf16 or f16");
+  cudaStream_t s = as_stream(stream);
+  DeviceCSR& g = graph->g;
+  graph->store_type = t;
+  if (t == g.vtype) {
+    graph->store_vals.reset();
+  } else {
+    graph->store_vals = DevBuf(std::max<int64_t>(g.nnz, 1) * dtype_size(t), s);
+    convert_values(g.values.p, g.vtype, graph->store_vals.p, t, g.nnz, s);
+  }
+  SCL_API_RETURN_OK;
+  SCL_API_CATCH
+}
+
+SCL_EXPORT scl_error_t scl_gpu_diffuse(scl_gpu_graph_t graph, const void* X, scl_dtype_t x_dtype, void* Y,
+                                       scl_dtype_t y_dtype, int64_t n_features, int64_t n_steps, void* stream) {
+  SCL_API_CHECK_NULL(graph, "Graph is null");
+  SCL_API_CHECK_NULL(X, "Matrix X is null");
+  SCL_API_CHECK_NULL(Y, "Matrix Y is null");
+  SCL_API_CHECK(n_features > 0 && n_steps >= 0, SCL_ERROR_INVALID_ARGUMENT, "Dimensions must be positive");
+  SCL_API_TRY
+  ensure_device(graph);
+  const DType xt = checked_dtype(x_dtype), yt = checked_dtype(y_dtype);
+  SCL_REQUIRE(is_float_dtype(xt) && is_float_dtype(yt), SCL_ERROR_TYPE_MISMATCH, "X and Y must be float dtypes");
+  SCL_REQUIRE(yt == graph->store_type || yt == kF32, SCL_ERROR_TYPE_MISMATCH,
+              "Y must be the storage dtype or f32");
+  diffuse(graph->storage_view(), X, xt, Y, yt, graph->store_type, n_features, n_steps, as_stream(stream));
+  SCL_API_RETURN_OK;
+  SCL_API_CATCH
+}
+
+SCL_EXPORT scl_error_t scl_gpu_spmm(scl_gpu_graph_t graph, const void* X, void* Y, scl_dtype_t y_dtype,
+                                    int64_t n_features, int group, int vec, void* stream) {
+  SCL_API_CHECK_NULL(graph, "Graph is null");
+  SCL_API_CHECK_NULL(X, "Matrix X is null");
+  SCL_API_CHECK_NULL(Y, "Matrix Y is null");
+  SCL_API_CHECK(n_features > 0, SCL_ERROR_INVALID_ARGUMENT, "Dimensions must be positive");
+  SCL_API_TRY
+  ensure_device(graph);
+  const DType yt = checked_dtype(y_dtype);
+  SCL_REQUIRE(yt == graph->store_type || yt == kF32, SCL_ERROR_TYPE_MISMATCH, "Y must be the storage dtype or f32");
+  const CsrView v = graph->storage_view();
+  SpmmArgs a{};
+  a.indptr = v.indptr;
+  a.indices = v.indices;
+  a.values = v.values;
+  a.vtype = v.vtype;
+  a.n_rows = v.n_rows;
+  a.F = n_features;
+  a.X = X;
+  a.xtype = graph->store_type;
+  a.Y = Y;
+  a.ytype = yt;
+  SpmmPlan plan = default_spmm_plan(n_features, a.xtype, X, Y, yt);
+  if (group > 0) {
+    plan.group = group;
+    plan.vec = vec;
+  }
+  spmm_with_plan(a, plan, as_stream(stream));
+  SCL_API_RETURN_OK;
+  SCL_API_CATCH
+}
+
+}  // extern "C"

@@ -1,0 +1,197 @@
+// Internal C++ interface of the B200 diffusion engine.
+//
+// Everything here is host-callable C++ implemented in the .cu files; the C ABI
+// layers (c_api_*.cpp) are the only callers. No torch types anywhere: device
+// memory comes from a per-device stream-ordered pool owned by the engine, or
+// from the caller as raw device pointers.
+#pragma once
+
+#include <cstddef>
+#include <cstdint>
+#include <stdexcept>
+#include <string>
+
+#include <cuda_runtime.h>
+
+namespace sclgpu {
+
+// Error codes mirror scl/binding/c_api/core/core.h:128-166.
+enum : int32_t {
+  kOk = 0,
+  kErrUnknown = 1,
+  kErrInternal = 2,
+  kErrOutOfMemory = 3,
+  kErrNullPointer = 4,
+  kErrInvalidArgument = 10,
+  kErrDimensionMismatch = 11,
+  kErrIndexOutOfBounds = 14,
+  kErrTypeMismatch = 21,
+  kErrNotImplemented = 40,
+  kErrFeatureUnavailable = 41,
+  kErrConvergence = 54,
+};
+
+struct Error : std::runtime_error {
+  int32_t code;
+  Error(int32_t c, const std::string& m) : std::runtime_error(m), code(c) {}
+};
+
+[[noreturn]] void throw_cuda(cudaError_t e, const char* what, const char* file, int line);
+
+#define SCL_CUDA(call)                                                      \
+  do {                                                                      \
+    cudaError_t e_ = (call);                                                \
+    if (e_ != cudaSuccess) ::sclgpu::throw_cuda(e_, #call, __FILE__, __LINE__); \
+  } while (0)
+
+#define SCL_REQUIRE(cond, code, msg)                 \
+  do {                                               \
+    if (!(cond)) throw ::sclgpu::Error((code), (msg)); \
+  } while (0)
+
+// Storage / element types accepted by the engine.
+enum DType : int32_t { kF32 = 0, kF64 = 1, kBF16 = 2, kF16 = 3, kI32 = 4, kI64 = 5 };
+size_t dtype_size(DType t);
+bool is_float_dtype(DType t);
+
+// ---------------------------------------------------------------------------
+// Per-device runtime: one library stream and one stream-ordered memory pool.
+// ---------------------------------------------------------------------------
+int current_device();                 // throws kErrFeatureUnavailable without a GPU
+cudaStream_t library_stream(int dev);  // non-blocking stream owned by the engine
+void* dev_alloc(size_t bytes, cudaStream_t s);
+void dev_free(void* p, cudaStream_t s);
+int sm_count(int dev);
+
+// RAII device buffer from the engine pool (freed on the given stream).
+struct DevBuf {
+  void* p = nullptr;
+  size_t bytes = 0;
+  cudaStream_t s = nullptr;
+  DevBuf() = default;
+  DevBuf(size_t b, cudaStream_t st) : bytes(b), s(st) { p = b ? dev_alloc(b, st) : nullptr; }
+  DevBuf(const DevBuf&) = delete;
+  DevBuf& operator=(const DevBuf&) = delete;
+  DevBuf(DevBuf&& o) noexcept : p(o.p), bytes(o.bytes), s(o.s) { o.p = nullptr; o.bytes = 0; }
+  DevBuf& operator=(DevBuf&& o) noexcept {
+    if (this != &o) { reset(); p = o.p; bytes = o.bytes; s = o.s; o.p = nullptr; o.bytes = 0; }
+    return *this;
+  }
+  ~DevBuf() { reset(); }
+  void reset() { if (p) dev_free(p, s); p = nullptr; bytes = 0; }
+  template <class T> T* as() const { return static_cast<T*>(p); }
+};
+
+// ---------------------------------------------------------------------------
+// Device CSR graph (primary-major: rows of a CSR handle, columns of a CSC one).
+// Row offsets are int64 (indptr), column indices int32, values in `vtype`.
+// ---------------------------------------------------------------------------
+// Non-owning view of a device CSR (structure + one value array).
+struct CsrView {
+  int64_t n_rows = 0;
+  int64_t n_cols = 0;
+  int64_t nnz = 0;
+  const int64_t* indptr = nullptr;
+  const int32_t* indices = nullptr;
+  const void* values = nullptr;
+  DType vtype = kF32;
+};
+
+struct DeviceCSR {
+  int64_t n_rows = 0;   // primary dimension
+  int64_t n_cols = 0;   // secondary dimension
+  int64_t nnz = 0;
+  DevBuf indptr;        // int64[n_rows + 1]
+  DevBuf indices;       // int32[nnz]
+  DevBuf values;        // vtype[nnz]
+  DType vtype = kF32;
+  CsrView view() const {
+    CsrView v;
+    v.n_rows = n_rows; v.n_cols = n_cols; v.nnz = nnz;
+    v.indptr = indptr.as<int64_t>(); v.indices = indices.as<int32_t>();
+    v.values = values.p; v.vtype = vtype;
+    return v;
+  }
+};
+
+// Status word written by kernels that validate inputs or wait with a bound.
+// Layout: [0] = error code (0 ok), [1] = first offending index (low 32 bits).
+struct DevStatus {
+  DevBuf buf;
+  explicit DevStatus(cudaStream_t s);
+  void check(cudaStream_t s, const char* what);  // syncs s, throws on error
+  int32_t* ptr() const { return buf.as<int32_t>(); }
+};
+
+// ---- conversions / validation --------------------------------------------
+// Convert an index array of type `src` (kI32/kI64) on the device to int32 or int64.
+void convert_indices(const void* src, DType src_t, int32_t* dst, int64_t count, cudaStream_t s);
+void convert_offsets(const void* src, DType src_t, int64_t* dst, int64_t count, cudaStream_t s);
+void convert_values(const void* src, DType src_t, void* dst, DType dst_t, int64_t count, cudaStream_t s);
+// Checks 0 <= indices < n_cols, indptr[0] == 0, indptr non-decreasing, indptr[n] == nnz.
+void validate_csr(const DeviceCSR& g, int32_t* status, cudaStream_t s);
+
+// ---- SpMM / power iteration ------------------------------------------------
+struct SpmmArgs {
+  const int64_t* indptr;
+  const int32_t* indices;
+  const void* values;
+  DType vtype;
+  int64_t n_rows;
+  int64_t F;
+  const void* X;   // n_cols x F, row-major
+  DType xtype;
+  void* Y;         // n_rows x F, row-major
+  DType ytype;
+  const int32_t* row_map = nullptr;  // optional: output row r is written to Y[row_map[r]]
+};
+// Launch shape of the SpMM kernel: `group` lanes own one output row and each
+// lane owns `vec` contiguous columns (16 bytes of X) per pass; vec == 1 is the
+// scalar fallback for rows whose pitch is not a multiple of 16 bytes.
+constexpr int kSpmmThreads = 256;
+struct SpmmPlan {
+  int group = 32;
+  int vec = 1;
+};
+SpmmPlan default_spmm_plan(int64_t F, DType xtype, const void* X, const void* Y, DType ytype);
+
+// One Y = P X. Each output element is the sequential fma chain over the row's
+// nonzeros in stored order (FP32 accumulation, FP64 when values/X are f64).
+void spmm(const SpmmArgs& a, cudaStream_t s);
+void spmm_with_plan(const SpmmArgs& a, const SpmmPlan& plan, cudaStream_t s);
+
+// Y = P^steps X0. Intermediate iterates are stored as `mtype` (which must equal
+// the graph's value dtype) in pool buffers; the last step writes Y in `ytype`.
+// X0 may equal Y (in place). `plan` overrides the default launch shape.
+void diffuse(const CsrView& g, const void* X0, DType xtype, void* Y, DType ytype, DType mtype, int64_t F,
+             int64_t steps, cudaStream_t s, const SpmmPlan* plan = nullptr);
+
+// ---- transition build -------------------------------------------------------
+// degrees[i] = sequential FP64 sum of row i's values.
+void row_degrees_fp64(const DeviceCSR& g, double* degrees, cudaStream_t s);
+// In-place normalisation of g.values (f32 or f64): row (D^-1 W) or symmetric
+// (D^-1/2 W D^-1/2); zero scale where d <= 1e-15. degree_mode 0 = FP64 degrees
+// (one rounding of v*scale), 1 = degrees and scales in the value type exactly
+// as scl-core computes them.
+void normalize(DeviceCSR& g, int symmetric, int degree_mode, double* degrees_out, cudaStream_t s);
+
+// Gaussian kNN weights: sigma_i = max(valid dists, 1e-10); w = expf(-(d/sigma)^2).
+void gauss_weights(const int32_t* knn_idx, const float* knn_dist, int64_t n, int64_t k, float* sigma,
+                   float* w, cudaStream_t s);
+// (W + W^T)/2 over the union of kNN pairs -> fresh DeviceCSR (f32 values).
+void symmetrize_knn(const int32_t* knn_idx, const float* w, int64_t n, int64_t k, DeviceCSR& out,
+                    cudaStream_t s);
+
+// ---- sorting / scans (building blocks) ----------------------------------------
+// Stable LSD radix sort of 64-bit keys with a 32-bit payload, sorting on the
+// low `key_bits` bits. Results in keys_out/vals_out; inputs are clobbered.
+void radix_sort_pairs(uint64_t* keys, uint32_t* vals, uint64_t* keys_out, uint32_t* vals_out, int64_t count,
+                      int key_bits, cudaStream_t s);
+// Exclusive prefix sum over int64 (out may equal in). Returns nothing; total in out[count].
+void exclusive_scan_i64(const int64_t* in, int64_t* out, int64_t count, cudaStream_t s);
+
+// Transpose structure: for CSR g (n_rows x n_cols) build the CSR of g^T and the
+// map tmap[q] = position in g of the entry that lands at q in g^T.
+void transpose_map(const DeviceCSR& g, DeviceCSR& gt, DevBuf& tmap, cudaStream_t s);
+
+}  // namespace sclgpu

@@ -1,0 +1,73 @@
+"""NumPy-level diffusion calls through the drop-in C ABI (scl_diffusion.h).
+
+Each function takes a ``CsrMatrix`` and NumPy arrays in host memory, exactly as
+a caller of scl-core's ``scl_diffusion_*`` functions would, and runs on the GPU.
+"""
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+
+from .core.error import check_error
+from .core.sparse import CsrMatrix
+
+
+def _as_real(mat: CsrMatrix, X: np.ndarray) -> np.ndarray:
+    if X.dtype != mat.real_dtype or not X.flags["C_CONTIGUOUS"] or not X.flags["WRITEABLE"]:
+        raise TypeError(f"X must be a writeable C-contiguous {np.dtype(mat.real_dtype).name} array")
+    return X
+
+
+def compute_transition_matrix(mat: CsrMatrix, symmetric: bool = False) -> None:
+    """In-place row (or symmetric) normalisation of the handle's values."""
+    check_error(mat.lib.scl_diffusion_compute_transition_matrix(mat.handle, int(bool(symmetric))),
+                "compute_transition_matrix", mat.lib)
+
+
+def diffuse_matrix(mat: CsrMatrix, X: np.ndarray, n_steps: int) -> np.ndarray:
+    """X <- P^n_steps X in place (n x F row-major); returns X."""
+    X = _as_real(mat, X)
+    n, F = X.shape
+    P = ctypes.POINTER(mat.lib.real_type)
+    check_error(mat.lib.scl_diffusion_diffuse_matrix(mat.handle, X.ctypes.data_as(P), n, F, int(n_steps)),
+                "diffuse_matrix", mat.lib)
+    return X
+
+
+def diffuse_vector(mat: CsrMatrix, x: np.ndarray, n_steps: int) -> np.ndarray:
+    x = _as_real(mat, x)
+    P = ctypes.POINTER(mat.lib.real_type)
+    check_error(mat.lib.scl_diffusion_diffuse_vector(mat.handle, x.ctypes.data_as(P), x.shape[0], int(n_steps)),
+                "diffuse_vector", mat.lib)
+    return x
+
+
+def magic_impute(mat: CsrMatrix, X: np.ndarray, t: int = 0) -> np.ndarray:
+    X = _as_real(mat, X)
+    n, F = X.shape
+    P = ctypes.POINTER(mat.lib.real_type)
+    check_error(mat.lib.scl_diffusion_magic_impute(mat.handle, X.ctypes.data_as(P), n, F, int(t)),
+                "magic_impute", mat.lib)
+    return X
+
+
+def set_degree_mode(mat_or_lib, mode: int) -> None:
+    """0 = FP64 degrees (default), 1 = value-type degrees as scl-core computes them."""
+    lib = getattr(mat_or_lib, "lib", mat_or_lib)
+    check_error(lib.scl_diffusion_gpu_set_degree_mode(int(mode)), "set_degree_mode", lib)
+
+
+def attach(mat: CsrMatrix) -> None:
+    check_error(mat.lib.scl_diffusion_gpu_attach(mat.handle), "attach", mat.lib)
+
+
+def detach(mat: CsrMatrix) -> None:
+    check_error(mat.lib.scl_diffusion_gpu_detach(mat.handle), "detach", mat.lib)
+
+
+def last_stats(lib) -> dict:
+    ms, h2d, d2h = ctypes.c_double(), ctypes.c_double(), ctypes.c_double()
+    check_error(lib.scl_diffusion_gpu_last_stats(ctypes.byref(ms), ctypes.byref(h2d), ctypes.byref(d2h)),
+                "last_stats", lib)
+    return {"device_ms": ms.value, "h2d_bytes": h2d.value, "d2h_bytes": d2h.value}

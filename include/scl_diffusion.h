@@ -78,6 +78,13 @@ SCL_EXPORT scl_error_t scl_diffusion_lazy_random_walk(scl_sparse_t transition, s
  *     (bit-identical to the reference build of the same precision). */
 SCL_EXPORT scl_error_t scl_diffusion_gpu_set_degree_mode(int mode);
 
+/* Locality reordering of diffuse_matrix on this thread: -1 = automatic (when
+ * the dense block is at least 32 MiB and n_steps >= 2; default), 0 = off,
+ * 1 = always. Results are bit-identical either way: rows of each connected
+ * component are grouped for cache locality and every row keeps its stored
+ * entry order. */
+SCL_EXPORT scl_error_t scl_diffusion_gpu_set_reorder(int mode);
+
 /* Keep a device copy of the handle's arrays between calls. Later diffusion
  * calls on the handle skip the upload of the graph; the caller promises not to
  * modify the wrapped arrays except through this library until detach. */

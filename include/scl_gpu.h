@@ -76,11 +76,32 @@ SCL_EXPORT scl_error_t scl_gpu_graph_set_storage(scl_gpu_graph_t graph, scl_dtyp
 SCL_EXPORT scl_error_t scl_gpu_diffuse(scl_gpu_graph_t graph, const void* X, scl_dtype_t x_dtype, void* Y,
                                        scl_dtype_t y_dtype, int64_t n_features, int64_t n_steps, void* stream);
 
-/* One Y = P X with an explicit launch shape (group lanes per row in
- * {1,2,4,8,16,32}; vec = 16 bytes / element size, or 1). group <= 0 picks the
- * default. X and Y must be in the storage dtype (Y may also be F32). */
+/* Locality reordering used by scl_gpu_diffuse: mode 1 groups the rows of each
+ * connected component together (P' = Pi P Pi^T, X gathered once and the result
+ * scattered back on the last step); mode 0 drops it. Each row keeps its stored
+ * entry order, so results are bit-identical with and without it. The
+ * permutation is rebuilt only by this call; value changes (normalize,
+ * set_storage) are picked up automatically. Synchronises `stream`. */
+SCL_EXPORT scl_error_t scl_gpu_graph_reorder(scl_gpu_graph_t graph, int mode, void* stream);
+
+/* Launch shape scl_gpu_diffuse uses for this graph at `n_features` columns in
+ * the current storage dtype (same meaning as scl_gpu_spmm's shape arguments);
+ * group <= 0 removes it (built-in default). Every shape computes the same bits. */
+SCL_EXPORT scl_error_t scl_gpu_graph_set_plan(scl_gpu_graph_t graph, int64_t n_features, int group, int vec, int kind,
+                                              int stage);
+
+/* The reordering's permutation (perm[new] = old, host int32 [n_rows]) and the
+ * number of component-labelling rounds it took; either pointer may be NULL. */
+SCL_EXPORT scl_error_t scl_gpu_graph_reorder_info(scl_gpu_graph_t graph, int32_t* perm, int* cc_rounds, void* stream);
+
+/* One Y = P X (original row order) with an explicit launch shape: group lanes
+ * per row in {1,2,4,8,16,32}; vec = 16 bytes / element size, or 1; kind 0 =
+ * register-gather kernel, 1 = cp.async shared-memory pipeline (vec > 1,
+ * group >= 4) with `stage` in {4, 8, 16} entries per stage. group <= 0 picks
+ * the default shape. X and Y must be in the storage dtype (Y may also be F32).
+ * Every shape computes the same bits. */
 SCL_EXPORT scl_error_t scl_gpu_spmm(scl_gpu_graph_t graph, const void* X, void* Y, scl_dtype_t y_dtype,
-                                    int64_t n_features, int group, int vec, void* stream);
+                                    int64_t n_features, int group, int vec, int kind, int stage, void* stream);
 
 #ifdef __cplusplus
 }

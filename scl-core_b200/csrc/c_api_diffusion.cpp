@@ -17,6 +17,7 @@ namespace sclabi {
 struct DeviceMirror {
   int device = -1;
   DeviceCSR g;
+  std::unique_ptr<Reordered> reo;  // locality reordering (built on demand)
 };
 
 }  // namespace sclabi
@@ -24,6 +25,16 @@ struct DeviceMirror {
 namespace {
 
 thread_local int t_degree_mode = 0;
+// -1 = automatic (reorder when X is at least kReorderMinBytes and >= 2 steps),
+//  0 = never, 1 = always (square matrices only).
+thread_local int t_reorder_mode = -1;
+constexpr int64_t kReorderMinBytes = 32ll << 20;
+
+bool want_reorder(const DeviceCSR& g, int64_t F, int64_t steps, size_t esz) {
+  if (g.n_rows != g.n_cols || g.n_rows < 2 || t_reorder_mode == 0) return false;
+  if (t_reorder_mode == 1) return true;
+  return steps >= 2 && g.n_rows * F * (int64_t)esz >= kReorderMinBytes;
+}
 struct Stats {
   double device_ms = 0, h2d = 0, d2h = 0;
 };
@@ -121,7 +132,17 @@ void diffuse_host_block(scl_sparse_matrix& m, Real* X, Index n_nodes, Index n_fe
   st.h2d += (double)total * sizeof(Real);
   EventTimer tm(s);
   tm.start();
-  diffuse(mir->g.view(), Xd.p, sclabi::kRealDType, Xd.p, sclabi::kRealDType, sclabi::kRealDType, n_features, n_steps, s);
+  if (want_reorder(mir->g, n_features, n_steps, sizeof(Real))) {
+    if (!mir->reo) {
+      mir->reo = std::make_unique<Reordered>();
+      build_reorder(mir->g.view(), *mir->reo, s);
+    }
+    if (!mir->reo->values_ok) reorder_values(mir->g.values.p, mir->g.vtype, *mir->reo, s);
+    diffuse_reordered(*mir->reo, Xd.p, sclabi::kRealDType, Xd.p, sclabi::kRealDType, n_features, n_steps, s);
+  } else {
+    diffuse(mir->g.view(), Xd.p, sclabi::kRealDType, Xd.p, sclabi::kRealDType, sclabi::kRealDType, n_features,
+            n_steps, s);
+  }
   tm.stop();
   SCL_CUDA(cudaMemcpyAsync(X, Xd.p, total * sizeof(Real), cudaMemcpyDeviceToHost, s));
   st.d2h += (double)total * sizeof(Real);
@@ -149,6 +170,7 @@ SCL_EXPORT scl_error_t scl_diffusion_compute_transition_matrix(scl_sparse_t adja
   EventTimer tm(s);
   tm.start();
   normalize(mir->g, symmetric != 0, t_degree_mode, nullptr, s);
+  if (mir->reo) mir->reo->values_ok = false;
   tm.stop();
   SCL_CUDA(cudaMemcpyAsync(values, mir->g.values.p, mir->g.nnz * sizeof(Real), cudaMemcpyDeviceToHost, s));
   st.d2h += (double)mir->g.nnz * sizeof(Real);
@@ -272,6 +294,13 @@ SCL_EXPORT scl_error_t scl_diffusion_lazy_random_walk(scl_sparse_t, scl_real_t*,
 SCL_EXPORT scl_error_t scl_diffusion_gpu_set_degree_mode(int mode) {
   SCL_API_CHECK(mode == 0 || mode == 1, SCL_ERROR_INVALID_ARGUMENT, "degree mode must be 0 (FP64) or 1 (native)");
   t_degree_mode = mode;
+  SCL_API_RETURN_OK;
+}
+
+SCL_EXPORT scl_error_t scl_diffusion_gpu_set_reorder(int mode) {
+  SCL_API_CHECK(mode >= -1 && mode <= 1, SCL_ERROR_INVALID_ARGUMENT,
+                "reorder mode must be -1 (automatic), 0 (off) or 1 (on)");
+  t_reorder_mode = mode;
   SCL_API_RETURN_OK;
 }
 

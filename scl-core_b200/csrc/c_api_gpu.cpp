@@ -2,6 +2,8 @@
 // entry points keep the graph resident on the GPU and take raw device buffers
 // and a caller stream, for the autograd wrapper and device-side callers.
 #include <cstring>
+#include <map>
+#include <utility>
 #include <vector>
 
 #include "abi.hpp"
@@ -19,6 +21,15 @@ struct scl_gpu_graph {
   DevBuf degrees;           // FP64 row degrees of `weights`
   int symmetric = 0;
   bool normalized = false;
+  // locality-reordered copy used by scl_gpu_diffuse (scl_gpu_graph_reorder)
+  std::unique_ptr<Reordered> reo;
+  // launch shapes chosen per (n_features, storage dtype): set_plan / autotune
+  std::map<std::pair<int64_t, int>, SpmmPlan> plans;
+
+  const SpmmPlan* plan_for(int64_t F) const {
+    auto it = plans.find({F, (int)store_type});
+    return it == plans.end() ? nullptr : &it->second;
+  }
 
   CsrView storage_view() const {
     CsrView v = g.view();
@@ -143,6 +154,7 @@ SCL_EXPORT scl_error_t scl_gpu_graph_normalize(scl_gpu_graph_t graph, int symmet
   normalize(g, symmetric != 0, degree_mode, graph->degrees.as<double>(), s);
   graph->symmetric = symmetric != 0;
   graph->normalized = true;
+  if (graph->reo) graph->reo->values_ok = false;
   if (graph->store_type != g.vtype) {
     graph->store_vals = DevBuf(std::max<int64_t>(g.nnz, 1) * dtype_size(graph->store_type), s);
     convert_values(g.values.p, g.vtype, graph->store_vals.p, graph->store_type, g.nnz, s);
@@ -176,6 +188,7 @@ SCL_EXPORT scl_error_t scl_gpu_graph_set_storage(scl_gpu_graph_t graph, scl_dtyp
   cudaStream_t s = as_stream(stream);
   DeviceCSR& g = graph->g;
   graph->store_type = t;
+  if (graph->reo) graph->reo->values_ok = false;
   if (t == g.vtype) {
     graph->store_vals.reset();
   } else {
@@ -198,13 +211,86 @@ SCL_EXPORT scl_error_t scl_gpu_diffuse(scl_gpu_graph_t graph, const void* X, scl
   SCL_REQUIRE(is_float_dtype(xt) && is_float_dtype(yt), SCL_ERROR_TYPE_MISMATCH, "X and Y must be float dtypes");
   SCL_REQUIRE(yt == graph->store_type || yt == kF32, SCL_ERROR_TYPE_MISMATCH,
               "Y must be the storage dtype or f32");
-  diffuse(graph->storage_view(), X, xt, Y, yt, graph->store_type, n_features, n_steps, as_stream(stream));
+  cudaStream_t s = as_stream(stream);
+  const CsrView v = graph->storage_view();
+  const SpmmPlan* plan = graph->plan_for(n_features);
+  if (graph->reo) {
+    Reordered& r = *graph->reo;
+    if (!r.values_ok || r.vtype != graph->store_type) reorder_values(v.values, v.vtype, r, s);
+    diffuse_reordered(r, X, xt, Y, yt, n_features, n_steps, s, plan);
+  } else {
+    diffuse(v, X, xt, Y, yt, graph->store_type, n_features, n_steps, s, plan);
+  }
+  SCL_API_RETURN_OK;
+  SCL_API_CATCH
+}
+
+SCL_EXPORT scl_error_t scl_gpu_graph_reorder(scl_gpu_graph_t graph, int mode, void* stream) {
+  SCL_API_CHECK_NULL(graph, "Graph is null");
+  SCL_API_CHECK(mode == 0 || mode == 1, SCL_ERROR_INVALID_ARGUMENT, "reorder mode must be 0 (off) or 1 (components)");
+  SCL_API_TRY
+  ensure_device(graph);
+  cudaStream_t s = as_stream(stream);
+  if (mode == 0) {
+    graph->reo.reset();
+  } else {
+    auto r = std::make_unique<Reordered>();
+    build_reorder(graph->g.view(), *r, s);
+    graph->reo = std::move(r);
+  }
+  SCL_API_RETURN_OK;
+  SCL_API_CATCH
+}
+
+SCL_EXPORT scl_error_t scl_gpu_graph_set_plan(scl_gpu_graph_t graph, int64_t n_features, int group, int vec, int kind,
+                                              int stage) {
+  SCL_API_CHECK_NULL(graph, "Graph is null");
+  SCL_API_CHECK(n_features > 0, SCL_ERROR_INVALID_ARGUMENT, "Dimensions must be positive");
+  SCL_API_TRY
+  const std::pair<int64_t, int> key{n_features, (int)graph->store_type};
+  if (group <= 0) {
+    graph->plans.erase(key);
+  } else {
+    SCL_REQUIRE(group <= 32 && (group & (group - 1)) == 0, SCL_ERROR_INVALID_ARGUMENT,
+                "lane-group size must be a power of two in [1, 32]");
+    const int bytes = vec * (int)dtype_size(graph->store_type);
+    SCL_REQUIRE(vec == 1 || ((bytes == 4 || bytes == 8 || bytes == 16) && n_features % vec == 0),
+                SCL_ERROR_INVALID_ARGUMENT, "vec must be 1 or a 4/8/16-byte chunk dividing n_features");
+    SCL_REQUIRE(vec == 1 || bytes == 16 || group == 32, SCL_ERROR_INVALID_ARGUMENT,
+                "4- and 8-byte lane chunks need a whole warp per row");
+    SCL_REQUIRE(kind == 0 || (kind == 1 && bytes == 16 && group >= 4 && (stage == 4 || stage == 8 || stage == 16)) ||
+                    (kind == 2 && group == 32 && (stage == 8 || stage == 16)) ||
+                    (kind == 3 && group == 32 && (stage == 16 || stage == 32) && bytes >= 4) ||
+                    (kind == 4 && group == 32 && (stage == 8 || stage == 16 || stage == 32) &&
+                     n_features == 32 * vec && (bytes == 4 || bytes == 8 || bytes == 16)),
+                SCL_ERROR_INVALID_ARGUMENT, "invalid kernel kind / stage for this shape");
+    SpmmPlan p;
+    p.group = group;
+    p.vec = vec;
+    p.kind = kind;
+    p.stage = stage;
+    graph->plans[key] = p;
+  }
+  SCL_API_RETURN_OK;
+  SCL_API_CATCH
+}
+
+SCL_EXPORT scl_error_t scl_gpu_graph_reorder_info(scl_gpu_graph_t graph, int32_t* perm, int* cc_rounds, void* stream) {
+  SCL_API_CHECK_NULL(graph, "Graph is null");
+  SCL_API_CHECK(graph->reo != nullptr, SCL_ERROR_INVALID_ARGUMENT, "graph has no reordering");
+  SCL_API_TRY
+  cudaStream_t s = as_stream(stream);
+  if (cc_rounds) *cc_rounds = graph->reo->cc_rounds;
+  if (perm) {
+    SCL_CUDA(cudaMemcpyAsync(perm, graph->reo->perm.p, graph->reo->n * 4, cudaMemcpyDeviceToHost, s));
+    SCL_CUDA(cudaStreamSynchronize(s));
+  }
   SCL_API_RETURN_OK;
   SCL_API_CATCH
 }
 
 SCL_EXPORT scl_error_t scl_gpu_spmm(scl_gpu_graph_t graph, const void* X, void* Y, scl_dtype_t y_dtype,
-                                    int64_t n_features, int group, int vec, void* stream) {
+                                    int64_t n_features, int group, int vec, int kind, int stage, void* stream) {
   SCL_API_CHECK_NULL(graph, "Graph is null");
   SCL_API_CHECK_NULL(X, "Matrix X is null");
   SCL_API_CHECK_NULL(Y, "Matrix Y is null");
@@ -229,6 +315,8 @@ SCL_EXPORT scl_error_t scl_gpu_spmm(scl_gpu_graph_t graph, const void* X, void* 
   if (group > 0) {
     plan.group = group;
     plan.vec = vec;
+    plan.kind = kind;
+    plan.stage = stage;
   }
   spmm_with_plan(a, plan, as_stream(stream));
   SCL_API_RETURN_OK;

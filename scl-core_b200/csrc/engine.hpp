@@ -148,10 +148,14 @@ struct SpmmArgs {
 // Launch shape of the SpMM kernel: `group` lanes own one output row and each
 // lane owns `vec` contiguous columns (16 bytes of X) per pass; vec == 1 is the
 // scalar fallback for rows whose pitch is not a multiple of 16 bytes.
+// kind 0 = register-gather kernel, kind 1 = cp.async shared-memory pipeline
+// (16-byte lane chunks only) with `stage` entries per pipeline stage (4/8/16).
 constexpr int kSpmmThreads = 256;
 struct SpmmPlan {
   int group = 32;
   int vec = 1;
+  int kind = 0;
+  int stage = 8;
 };
 SpmmPlan default_spmm_plan(int64_t F, DType xtype, const void* X, const void* Y, DType ytype);
 
@@ -165,6 +169,28 @@ void spmm_with_plan(const SpmmArgs& a, const SpmmPlan& plan, cudaStream_t s);
 // X0 may equal Y (in place). `plan` overrides the default launch shape.
 void diffuse(const CsrView& g, const void* X0, DType xtype, void* Y, DType ytype, DType mtype, int64_t F,
              int64_t steps, cudaStream_t s, const SpmmPlan* plan = nullptr);
+
+// ---- locality reordering ------------------------------------------------------
+// Rows grouped by connected component (stable within a component); entries of
+// each row keep their original order, so diffusion results are bit-identical.
+struct Reordered {
+  int64_t n = 0, nnz = 0;
+  int cc_rounds = 0;
+  DevBuf perm;     // int32[n]   new row -> old row
+  DevBuf iperm;    // int32[n]   old row -> new row
+  DevBuf indptr;   // int64[n+1] permuted structure
+  DevBuf indices;  // int32[nnz] renamed column ids
+  DevBuf emap;     // int32[nnz] new entry -> old entry
+  DevBuf values;   // vtype[nnz] values gathered through emap
+  DType vtype = kF32;
+  bool values_ok = false;
+};
+void build_reorder(const CsrView& g, Reordered& r, cudaStream_t s);
+void reorder_values(const void* vals, DType t, Reordered& r, cudaStream_t s);
+// Y = P^steps X0 through the permuted structure: X0 is gathered into permuted
+// order once, the last step scatters rows back (Y may equal X0).
+void diffuse_reordered(const Reordered& r, const void* X0, DType xtype, void* Y, DType ytype, int64_t F,
+                       int64_t steps, cudaStream_t s, const SpmmPlan* plan = nullptr);
 
 // ---- transition build -------------------------------------------------------
 // degrees[i] = sequential FP64 sum of row i's values.

@@ -46,15 +46,23 @@ __device__ __forceinline__ float fma_acc(float a, float b, float c) { return __f
 __device__ __forceinline__ double fma_acc(double a, double b, double c) { return __fma_rn(a, b, c); }
 
 // ---- vector load / store of VEC contiguous elements ------------------------
+// Lane chunks of 4, 8 or 16 bytes are loaded with one vector instruction.
+template <int BYTES> struct RawVec;
+template <> struct RawVec<4> { using type = unsigned int; };
+template <> struct RawVec<8> { using type = uint2; };
+template <> struct RawVec<16> { using type = uint4; };
+
 template <class T, int VEC>
 struct VecIO {
-  static_assert(VEC * sizeof(T) == 16 || VEC == 1, "VEC must cover 16 bytes or be scalar");
+  static constexpr int BYTES = VEC * (int)sizeof(T);
+  static_assert(VEC == 1 || BYTES == 4 || BYTES == 8 || BYTES == 16, "lane chunk must be 4, 8 or 16 bytes");
   template <class A>
   static __device__ __forceinline__ void load(const T* __restrict__ p, A (&out)[VEC]) {
     if constexpr (VEC == 1) {
       out[0] = to_acc<A, T>(__ldg(p));
     } else {
-      const uint4 raw = __ldg(reinterpret_cast<const uint4*>(p));
+      using R = typename RawVec<BYTES>::type;
+      const R raw = __ldg(reinterpret_cast<const R*>(p));
       const T* e = reinterpret_cast<const T*>(&raw);
 #pragma unroll
       for (int i = 0; i < VEC; ++i) out[i] = to_acc<A, T>(e[i]);
@@ -74,15 +82,22 @@ struct VecStore {
       T* e = reinterpret_cast<T*>(&raw);
 #pragma unroll
       for (int i = 0; i < VEC; ++i) e[i] = from_acc<T, A>(in[i]);
-      *reinterpret_cast<uint4*>(p) = raw;
+      __stcs(reinterpret_cast<uint4*>(p), raw);  // streaming store: Y is not re-read this step
     } else if constexpr (BYTES == 32) {  // f32 output of a bf16/f16 (8-wide) chunk
       uint4 raw[2];
       T* e = reinterpret_cast<T*>(raw);
 #pragma unroll
       for (int i = 0; i < VEC; ++i) e[i] = from_acc<T, A>(in[i]);
-      reinterpret_cast<uint4*>(p)[0] = raw[0];
-      reinterpret_cast<uint4*>(p)[1] = raw[1];
-    } else {  // 8-byte chunks (e.g. bf16 output from a 4-wide f32 chunk)
+      __stcs(reinterpret_cast<uint4*>(p), raw[0]);
+      __stcs(reinterpret_cast<uint4*>(p) + 1, raw[1]);
+    } else if constexpr (BYTES == 8 || BYTES == 4) {
+      using R = typename RawVec<BYTES>::type;
+      R raw;
+      T* e = reinterpret_cast<T*>(&raw);
+#pragma unroll
+      for (int i = 0; i < VEC; ++i) e[i] = from_acc<T, A>(in[i]);
+      *reinterpret_cast<R*>(p) = raw;
+    } else {
 #pragma unroll
       for (int i = 0; i < VEC; ++i) p[i] = from_acc<T, A>(in[i]);
     }
@@ -116,9 +131,11 @@ k_spmm(const int64_t* __restrict__ indptr, const int32_t* __restrict__ indices, 
   const int lane = threadIdx.x & 31;
   const int lg = lane & (G - 1);                       // lane within group
   const unsigned gmask = (G == 32) ? 0xffffffffu : (((1u << G) - 1u) << (lane & ~(G - 1)));
-  const int64_t row = ((int64_t)blockIdx.x * kSpmmThreads + threadIdx.x) / G;
-  if (row >= n_rows) return;  // whole groups exit together (G divides 32)
-
+  // Persistent grid: each lane group walks rows gid, gid + n_groups, ... so a
+  // group that finishes a short row immediately takes another (row lengths
+  // are heavily skewed; whole groups advance together since G divides 32).
+  const int64_t n_groups = ((int64_t)gridDim.x * kSpmmThreads) / G;
+  for (int64_t row = ((int64_t)blockIdx.x * kSpmmThreads + threadIdx.x) / G; row < n_rows; row += n_groups) {
   const int64_t start = indptr[row];
   const int64_t end = indptr[row + 1];
   const int64_t out_row = row_map ? (int64_t)row_map[row] : row;
@@ -137,8 +154,9 @@ k_spmm(const int64_t* __restrict__ indptr, const int32_t* __restrict__ indices, 
       int32_t j_l = 0;
       VT v_l = VT(0);
       if (m < end) {
-        j_l = __ldg(indices + m);
-        v_l = values[m];
+        // the CSR stream is read once per step: evict-first, keep L2 for X
+        j_l = __ldcs(indices + m);
+        v_l = __ldcs(values + m);
       }
       const int cnt = (int)((end - base) < G ? (end - base) : G);
       int t = 0;
@@ -172,6 +190,533 @@ k_spmm(const int64_t* __restrict__ indptr, const int32_t* __restrict__ indices, 
     }
     if (active) VecStore<YT, VEC>::store(Y + out_row * F + col, acc);
   }
+  }  // rows
+}
+
+// ---- pipelined variant: gathered rows land in shared memory via cp.async ----
+// Same lane mapping and the same per-element fma order as k_spmm. A group of G
+// lanes processes its row in chunks of S entries: lane t of the group loads
+// entry t's (index, value) (one coalesced load), then every lane issues S
+// 16-byte cp.async copies of ITS column chunk of the S gathered X rows into a
+// double-buffered stage. While stage c is consumed (ld.shared + fma), stage
+// c+1's indices and copies are already in flight, so memory latency overlaps
+// the math and in-flight data costs no registers. Each lane only reads back the
+// bytes it copied itself, so per-thread cp.async.wait_group is the only
+// synchronisation needed. Requires the 16-byte vector mapping (VEC*sizeof(XT)
+// == 16) and S <= G.
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
+
+template <int S>
+constexpr int pipe_smem_bytes() { return kSpmmThreads * 2 * S * 16; }
+
+template <class VT, class XT, class YT, class AT, int G, int VEC, int S>
+__global__ void __launch_bounds__(kSpmmThreads)
+k_spmm_pipe(const int64_t* __restrict__ indptr, const int32_t* __restrict__ indices, const VT* __restrict__ values,
+            const XT* __restrict__ X, YT* __restrict__ Y, const int32_t* __restrict__ row_map, int64_t n_rows,
+            int64_t F) {
+  static_assert(VEC * sizeof(XT) == 16, "pipelined SpMM needs 16-byte lane chunks");
+  static_assert(S <= G, "stage size must not exceed the group size");
+  extern __shared__ uint4 smem_pipe[];
+  const int lane = threadIdx.x & 31;
+  const int lg = lane & (G - 1);
+  const unsigned gmask = (G == 32) ? 0xffffffffu : (((1u << G) - 1u) << (lane & ~(G - 1)));
+  // this lane's slots: stage b, entry t -> smem_pipe[((b * S + t) * kSpmmThreads) + threadIdx.x]
+  uint4* my = smem_pipe + threadIdx.x;
+  const int64_t n_groups = ((int64_t)gridDim.x * kSpmmThreads) / G;
+  for (int64_t row = ((int64_t)blockIdx.x * kSpmmThreads + threadIdx.x) / G; row < n_rows; row += n_groups) {
+  const int64_t start = indptr[row];
+  const int64_t end = indptr[row + 1];
+  const int64_t out_row = row_map ? (int64_t)row_map[row] : row;
+  constexpr int CPP = G * VEC;
+
+  for (int64_t c0 = 0; c0 < F; c0 += CPP) {
+    const int64_t col = c0 + (int64_t)lg * VEC;
+    const bool active = col < F;
+    const XT* __restrict__ Xc = X + col;
+    AT acc[VEC];
+#pragma unroll
+    for (int i = 0; i < VEC; ++i) acc[i] = AT(0);
+
+    // chunk c covers entries [start + c*S, start + c*S + S)
+    int32_t j_cur = 0;
+    VT v_cur = VT(0);
+    {
+      const int64_t m = start + lg;
+      if (lg < S && m < end) {
+        j_cur = __ldcs(indices + m);
+        v_cur = __ldcs(values + m);
+      }
+    }
+    auto issue = [&](int stage, int32_t jreg, int64_t base) {
+      const int cnt = (int)((end - base) < S ? (end - base) : S);
+#pragma unroll
+      for (int t = 0; t < S; ++t) {
+        const int32_t jj = __shfl_sync(gmask, jreg, t, G);
+        if (t < cnt && active) cp_async16(my + (stage * S + t) * kSpmmThreads, Xc + (int64_t)jj * F);
+      }
+      cp_async_commit();
+    };
+    if (start < end) issue(0, j_cur, start);
+    int stage = 0;
+    for (int64_t base = start; base < end; base += S) {
+      const int cnt = (int)((end - base) < S ? (end - base) : S);
+      const int64_t nbase = base + S;
+      int32_t j_nxt = 0;
+      VT v_nxt = VT(0);
+      if (nbase < end) {
+        const int64_t m = nbase + lg;
+        if (lg < S && m < end) {
+          j_nxt = __ldcs(indices + m);
+          v_nxt = __ldcs(values + m);
+        }
+        issue(stage ^ 1, j_nxt, nbase);
+        cp_async_wait<1>();
+      } else {
+        cp_async_wait<0>();
+      }
+#pragma unroll
+      for (int t = 0; t < S; ++t) {
+        if (t < cnt) {
+          const AT vv = to_acc<AT, VT>(shfl_val<VT>(gmask, v_cur, t, G));
+          if (active) {
+            const uint4 raw = my[(stage * S + t) * kSpmmThreads];
+            const XT* e = reinterpret_cast<const XT*>(&raw);
+#pragma unroll
+            for (int i = 0; i < VEC; ++i) acc[i] = fma_acc(vv, to_acc<AT, XT>(e[i]), acc[i]);
+          }
+        }
+      }
+      j_cur = j_nxt;
+      v_cur = v_nxt;
+      stage ^= 1;
+    }
+    if (active) VecStore<YT, VEC>::store(Y + out_row * F + col, acc);
+  }
+  }  // rows
+}
+
+// ---- streaming variant: a warp walks the nonzero stream of a row block --------
+// A warp takes a task of up to 31 consecutive rows (lane l holds indptr[r0+l])
+// and walks their contiguous entries [indptr[r0], indptr[r1]) in chunks of 32:
+// each chunk's (index, value) pairs are loaded one chunk ahead, and gathers are
+// issued in predicated batches of U regardless of where rows begin or end, so
+// no row pays a fresh index->gather latency chain and no tail runs one load at
+// a time. A warp-uniform test e >= row_end flushes the finished row (its
+// accumulator is stored and reset) — rows with no entries are flushed as
+// zeros. Every row still accumulates exactly its own entries in stored order,
+// the same fma sequence as k_spmm. One warp covers a row with VEC elements per
+// lane (4-, 8- or 16-byte chunks); wider rows take several column passes.
+constexpr int kStreamRows = 31;
+
+template <class VT, class XT, class YT, class AT, int VEC, int U>
+__global__ void __launch_bounds__(kSpmmThreads)
+k_spmm_stream(const int64_t* __restrict__ indptr, const int32_t* __restrict__ indices, const VT* __restrict__ values,
+              const XT* __restrict__ X, YT* __restrict__ Y, const int32_t* __restrict__ row_map, int64_t n_rows,
+              int64_t F) {
+  const int lane = threadIdx.x & 31;
+  const int64_t n_warps = ((int64_t)gridDim.x * kSpmmThreads) >> 5;
+  const int64_t n_tasks = (n_rows + kStreamRows - 1) / kStreamRows;
+  constexpr int CPP = 32 * VEC;
+  for (int64_t task = ((int64_t)blockIdx.x * kSpmmThreads + threadIdx.x) >> 5; task < n_tasks; task += n_warps) {
+    const int64_t r0 = task * kStreamRows;
+    const int nr = (int)((n_rows - r0) < kStreamRows ? (n_rows - r0) : kStreamRows);
+    const int64_t ptr_l = (lane <= nr) ? __ldcs(indptr + r0 + lane) : 0;
+    const int64_t p0 = __shfl_sync(0xffffffffu, ptr_l, 0);
+    const int64_t p1 = __shfl_sync(0xffffffffu, ptr_l, nr);
+    for (int64_t c0 = 0; c0 < F; c0 += CPP) {
+      const int64_t col = c0 + (int64_t)lane * VEC;
+      const bool active = col < F;
+      const XT* __restrict__ Xc = X + col;
+      AT acc[VEC];
+#pragma unroll
+      for (int i = 0; i < VEC; ++i) acc[i] = AT(0);
+      int ri = 0;  // current row = r0 + ri
+      int64_t row_end = __shfl_sync(0xffffffffu, ptr_l, 1);
+      auto flush = [&]() {
+        if (active) {
+          const int64_t r = r0 + ri;
+          const int64_t orow = row_map ? (int64_t)row_map[r] : r;
+          VecStore<YT, VEC>::store(Y + orow * F + col, acc);
+        }
+#pragma unroll
+        for (int i = 0; i < VEC; ++i) acc[i] = AT(0);
+        ++ri;
+        if (ri < nr) row_end = __shfl_sync(0xffffffffu, ptr_l, ri + 1);
+      };
+      int32_t j_n = 0;
+      VT v_n = VT(0);
+      if (p0 + lane < p1) {
+        j_n = __ldcs(indices + p0 + lane);
+        v_n = __ldcs(values + p0 + lane);
+      }
+      for (int64_t c = p0; c < p1; c += 32) {
+        const int32_t j_l = j_n;
+        const VT v_l = v_n;
+        const int64_t mn = c + 32 + lane;
+        if (mn < p1) {  // next chunk's pairs are in flight during this chunk
+          j_n = __ldcs(indices + mn);
+          v_n = __ldcs(values + mn);
+        }
+        const int cnt = (int)((p1 - c) < 32 ? (p1 - c) : 32);
+#pragma unroll
+        for (int t = 0; t < 32; t += U) {
+          if (t >= cnt) break;
+          AT xv[U][VEC];
+          AT vv[U];
+#pragma unroll
+          for (int u = 0; u < U; ++u) {
+            const int32_t jj = __shfl_sync(0xffffffffu, j_l, t + u);
+            vv[u] = to_acc<AT, VT>(shfl_val<VT>(0xffffffffu, v_l, t + u, 32));
+            if (t + u < cnt && active) VecIO<XT, VEC>::load(Xc + (int64_t)jj * F, xv[u]);
+          }
+#pragma unroll
+          for (int u = 0; u < U; ++u) {
+            if (t + u < cnt) {
+              const int64_t e = c + t + u;
+              while (e >= row_end) flush();
+              if (active) {
+#pragma unroll
+                for (int i = 0; i < VEC; ++i) acc[i] = fma_acc(vv[u], xv[u][i], acc[i]);
+              }
+            }
+          }
+        }
+      }
+      while (ri < nr) flush();  // last row with entries, then trailing empty rows
+    }
+  }
+}
+
+// ---- stream + cp.async pipeline ------------------------------------------------
+// The row-block stream of k_spmm_stream with the gathers decoupled from the
+// consumer: for each chunk of S entries every lane fires S cp.async copies of
+// its LB-byte column chunk of the gathered X rows into a double-buffered stage
+// (lane-private slots, so the per-thread cp.async.wait_group is the only
+// synchronisation), then consumes the previous stage in entry order — fma into
+// the current row's accumulator, flushing rows as the stream crosses indptr.
+// Index/value pairs are prefetched two chunks ahead, so neither the index loads
+// nor the gathers sit on the consumer's critical path. Same fma sequence per
+// row as every other variant.
+template <int LB>
+__device__ __forceinline__ void cp_async_lb(void* smem, const void* gmem) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  if constexpr (LB == 16) asm volatile("cp.async.ca.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem) : "memory");
+  else if constexpr (LB == 8) asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(gmem) : "memory");
+  else asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+
+template <int LB, int S>
+constexpr int stream_pipe_smem_bytes() { return (kSpmmThreads / 32) * 2 * S * 32 * LB; }
+
+template <class VT, class XT, class YT, class AT, int VEC, int S>
+__global__ void __launch_bounds__(kSpmmThreads)
+k_spmm_spipe(const int64_t* __restrict__ indptr, const int32_t* __restrict__ indices, const VT* __restrict__ values,
+             const XT* __restrict__ X, YT* __restrict__ Y, const int32_t* __restrict__ row_map, int64_t n_rows,
+             int64_t F) {
+  constexpr int LB = VEC * (int)sizeof(XT);
+  static_assert(LB == 4 || LB == 8 || LB == 16, "lane chunk must be 4, 8 or 16 bytes");
+  static_assert(S <= 32, "a stage holds at most one chunk of 32 entries");
+  using R = typename RawVec<LB>::type;
+  extern __shared__ uint4 smem_spipe[];
+  const int lane = threadIdx.x & 31;
+  const int warp_in_block = threadIdx.x >> 5;
+  // slot (stage b, entry t) of this lane: base + ((b * S + t) * 32 + lane) * LB bytes
+  char* wbase = reinterpret_cast<char*>(smem_spipe) + (size_t)warp_in_block * 2 * S * 32 * LB;
+  auto slot = [&](int b, int t) -> R* { return reinterpret_cast<R*>(wbase + ((size_t)(b * S + t) * 32 + lane) * LB); };
+  const int64_t n_warps = ((int64_t)gridDim.x * kSpmmThreads) >> 5;
+  const int64_t n_tasks = (n_rows + kStreamRows - 1) / kStreamRows;
+  constexpr int CPP = 32 * VEC;
+  for (int64_t task = ((int64_t)blockIdx.x * kSpmmThreads + threadIdx.x) >> 5; task < n_tasks; task += n_warps) {
+    const int64_t r0 = task * kStreamRows;
+    const int nr = (int)((n_rows - r0) < kStreamRows ? (n_rows - r0) : kStreamRows);
+    const int64_t ptr_l = (lane <= nr) ? __ldcs(indptr + r0 + lane) : 0;
+    const int64_t p0 = __shfl_sync(0xffffffffu, ptr_l, 0);
+    const int64_t p1 = __shfl_sync(0xffffffffu, ptr_l, nr);
+    for (int64_t c0 = 0; c0 < F; c0 += CPP) {
+      const int64_t col = c0 + (int64_t)lane * VEC;
+      const bool active = col < F;
+      const XT* __restrict__ Xc = X + (active ? col : 0);
+      AT acc[VEC];
+#pragma unroll
+      for (int i = 0; i < VEC; ++i) acc[i] = AT(0);
+      int ri = 0;
+      int64_t row_end = __shfl_sync(0xffffffffu, ptr_l, 1);
+      // pairs of chunk k live in lane t < S as (j_k, v_k); chunks start at p0 + k*S
+      auto load_pair = [&](int64_t base, int32_t& j, VT& v) {
+        const int64_t m = base + lane;
+        j = 0;
+        v = VT(0);
+        if (lane < S && m < p1) {
+          j = __ldcs(indices + m);
+          v = __ldcs(values + m);
+        }
+      };
+      auto issue = [&](int b, int32_t j, int64_t base) {
+        const int cnt = (int)((p1 - base) < S ? (p1 - base) : S);
+#pragma unroll
+        for (int t = 0; t < S; ++t) {
+          const int32_t jj = __shfl_sync(0xffffffffu, j, t);
+          if (t < cnt && active) cp_async_lb<LB>(slot(b, t), Xc + (int64_t)jj * F);
+        }
+        cp_async_commit();
+      };
+      int32_t j0, j1;
+      VT v0, v1;
+      load_pair(p0, j0, v0);
+      load_pair(p0 + S, j1, v1);
+      if (p0 < p1) issue(0, j0, p0);
+      int b = 0;
+      for (int64_t c = p0; c < p1; c += S) {
+        // chunk c: pairs (j0, v0), data in stage b; chunk c+S: pairs (j1, v1)
+        int32_t j2;
+        VT v2;
+        load_pair(c + 2 * S, j2, v2);
+        if (c + S < p1) {
+          issue(b ^ 1, j1, c + S);
+          cp_async_wait<1>();
+        } else {
+          cp_async_wait<0>();
+        }
+        const int cnt = (int)((p1 - c) < S ? (p1 - c) : S);
+#pragma unroll
+        for (int t = 0; t < S; ++t) {
+          if (t < cnt) {
+            const int64_t e = c + t;
+            while (e >= row_end) {
+              if (active) {
+                const int64_t r = r0 + ri;
+                const int64_t orow = row_map ? (int64_t)row_map[r] : r;
+                VecStore<YT, VEC>::store(Y + orow * F + col, acc);
+              }
+#pragma unroll
+              for (int i = 0; i < VEC; ++i) acc[i] = AT(0);
+              ++ri;
+              row_end = __shfl_sync(0xffffffffu, ptr_l, ri + 1 <= nr ? ri + 1 : nr);
+            }
+            const AT vv = to_acc<AT, VT>(shfl_val<VT>(0xffffffffu, v0, t, 32));
+            if (active) {
+              const R raw = *slot(b, t);
+              const XT* ex = reinterpret_cast<const XT*>(&raw);
+#pragma unroll
+              for (int i = 0; i < VEC; ++i) acc[i] = fma_acc(vv, to_acc<AT, XT>(ex[i]), acc[i]);
+            }
+          }
+        }
+        j0 = j1; v0 = v1;
+        j1 = j2; v1 = v2;
+        b ^= 1;
+      }
+      // the row holding the last entry, then trailing empty rows
+      while (ri < nr) {
+        if (active) {
+          const int64_t r = r0 + ri;
+          const int64_t orow = row_map ? (int64_t)row_map[r] : r;
+          VecStore<YT, VEC>::store(Y + orow * F + col, acc);
+        }
+#pragma unroll
+        for (int i = 0; i < VEC; ++i) acc[i] = AT(0);
+        ++ri;
+      }
+    }
+  }
+}
+
+// ---- fixed-pitch warp-per-row kernel (the hot path for 128/256/512-byte rows) --
+// One warp per row, lane l owning bytes [l*LB, (l+1)*LB) of every gathered row,
+// with the row pitch ROWB = 32*LB a compile-time constant: a gather address is
+// one wide multiply-add of the 32-bit column index and the lane offset folds
+// into the load. The row's (index, value) pairs are staged 32 at a time in a
+// per-warp shared-memory double buffer (values already widened to the
+// accumulator type) and read back with 128-bit broadcast loads, 4 entries per
+// load — shuffles would cost two shared-pipe operations per entry. Full
+// batches of U gathers issue without predicates; only a row's last batch is
+// predicated. While a chunk is consumed the next one (the rest of the row, or
+// the next row's first chunk) is already in flight, and row bounds are fetched
+// a row ahead, so a row start costs one gather latency. Same per-element fma
+// order as every other variant.
+// OFF32: X spans < 4 GiB, so gather offsets are 32-bit from the uniform base.
+template <class VT, class XT, class YT, class AT, int ROWB, int U, bool OFF32>
+__global__ void __launch_bounds__(kSpmmThreads, (U == 8) ? 4 : ((U == 16) ? 3 : 1))
+k_spmm_row(const int64_t* __restrict__ indptr, const int32_t* __restrict__ indices, const VT* __restrict__ values,
+           const XT* __restrict__ X, YT* __restrict__ Y, const int32_t* __restrict__ row_map, int64_t n_rows) {
+  constexpr int LB = ROWB / 32;
+  constexpr int VEC = LB / (int)sizeof(XT);
+  constexpr int WARPS = kSpmmThreads / 32;
+  static_assert(LB == 4 || LB == 8 || LB == 16, "row pitch must be 128, 256 or 512 bytes");
+  static_assert(U == 8 || U == 16 || U == 32, "batch must divide 32");
+  static_assert(sizeof(AT) == 4 || sizeof(AT) == 8, "accumulator is f32 or f64");
+  using R = typename RawVec<LB>::type;
+  __shared__ __align__(16) int32_t s_j[WARPS][2][32];
+  __shared__ __align__(16) AT s_v[WARPS][2][32];
+  const int lane = threadIdx.x & 31;
+  const int w = threadIdx.x >> 5;
+  const int64_t nw = ((int64_t)gridDim.x * kSpmmThreads) >> 5;
+  int64_t row = ((int64_t)blockIdx.x * kSpmmThreads + threadIdx.x) >> 5;
+  if (row >= n_rows) return;
+  const char* __restrict__ Xb = reinterpret_cast<const char*>(X);
+  const char* __restrict__ Xl = Xb + lane * LB;
+  const uint32_t lofs = (uint32_t)(lane * LB);
+  auto gather = [&](int32_t j) -> R {
+    if constexpr (OFF32) return __ldg(reinterpret_cast<const R*>(Xb + ((uint32_t)j * (uint32_t)ROWB + lofs)));
+    else return __ldg(reinterpret_cast<const R*>(Xl + (size_t)(uint32_t)j * ROWB));
+  };
+  // bounds of this row and the next are known; the one after is fetched a row ahead
+  int64_t s_cur = indptr[row], e_cur = indptr[row + 1];
+  int64_t s_nx = 0, e_nx = 0;
+  if (row + nw < n_rows) {
+    s_nx = indptr[row + nw];
+    e_nx = indptr[row + nw + 1];
+  }
+  auto fetch = [&](int64_t pos, int64_t end, int32_t& j, AT& v) {
+    j = 0;
+    v = AT(0);
+    if (pos < end) {
+      j = __ldcs(indices + pos);
+      v = to_acc<AT, VT>(__ldcs(values + pos));
+    }
+  };
+  int buf = 0;
+  {
+    int32_t j;
+    AT v;
+    fetch(s_cur + lane, e_cur, j, v);
+    s_j[w][0][lane] = j;
+    s_v[w][0][lane] = v;
+    __syncwarp();
+  }
+  for (; row < n_rows; row += nw) {
+    const int64_t nn = row + 2 * nw;
+    int64_t s_nn = 0, e_nn = 0;
+    if (nn < n_rows) {
+      s_nn = indptr[nn];
+      e_nn = indptr[nn + 1];
+    }
+    AT acc[VEC];
+#pragma unroll
+    for (int i = 0; i < VEC; ++i) acc[i] = AT(0);
+    const int len = (int)(e_cur - s_cur);
+    for (int base = 0; base < len; base += 32) {
+      // next chunk in flight: the rest of this row, else the next row's first
+      int32_t j_n;
+      AT v_n;
+      if (base + 32 < len) fetch(s_cur + base + 32 + lane, e_cur, j_n, v_n);
+      else fetch(s_nx + lane, e_nx, j_n, v_n);
+      const int cnt = (len - base) < 32 ? (len - base) : 32;
+      const int32_t* __restrict__ jb = s_j[w][buf];
+      const AT* __restrict__ vb = s_v[w][buf];
+#pragma unroll
+      for (int t = 0; t < 32; t += U) {
+        if (t >= cnt) break;
+        // gather phase: indices from shared memory, U loads in flight
+        R xr[U];
+        const bool full = (t + U <= cnt);
+#pragma unroll
+        for (int q = 0; q < U; q += 4) {
+          const int4 j4 = *reinterpret_cast<const int4*>(jb + t + q);
+          if (full) {
+            xr[q] = gather(j4.x);
+            xr[q + 1] = gather(j4.y);
+            xr[q + 2] = gather(j4.z);
+            xr[q + 3] = gather(j4.w);
+          } else {
+            if (t + q < cnt) xr[q] = gather(j4.x);
+            if (t + q + 1 < cnt) xr[q + 1] = gather(j4.y);
+            if (t + q + 2 < cnt) xr[q + 2] = gather(j4.z);
+            if (t + q + 3 < cnt) xr[q + 3] = gather(j4.w);
+          }
+        }
+        // fma phase: values read from shared memory as they are needed
+#pragma unroll
+        for (int q = 0; q < U; q += 4) {
+          AT vq[4];
+          if constexpr (sizeof(AT) == 4) {
+            const float4 v4 = *reinterpret_cast<const float4*>(vb + t + q);
+            vq[0] = v4.x; vq[1] = v4.y; vq[2] = v4.z; vq[3] = v4.w;
+          } else {
+            const double2 va = *reinterpret_cast<const double2*>(vb + t + q);
+            const double2 vc = *reinterpret_cast<const double2*>(vb + t + q + 2);
+            vq[0] = va.x; vq[1] = va.y; vq[2] = vc.x; vq[3] = vc.y;
+          }
+#pragma unroll
+          for (int r = 0; r < 4; ++r) {
+            if (full || t + q + r < cnt) {
+              const XT* ex = reinterpret_cast<const XT*>(&xr[q + r]);
+#pragma unroll
+              for (int i = 0; i < VEC; ++i) acc[i] = fma_acc(vq[r], to_acc<AT, XT>(ex[i]), acc[i]);
+            }
+          }
+        }
+      }
+      // publish the next chunk into the other buffer (its previous contents
+      // were consumed one chunk ago, before the last __syncwarp)
+      s_j[w][buf ^ 1][lane] = j_n;
+      s_v[w][buf ^ 1][lane] = v_n;
+      __syncwarp();
+      buf ^= 1;
+    }
+    if (len == 0) {  // empty row: nothing was prefetched, stage the next row's first chunk
+      int32_t j;
+      AT v;
+      fetch(s_nx + lane, e_nx, j, v);
+      s_j[w][buf][lane] = j;
+      s_v[w][buf][lane] = v;
+      __syncwarp();
+    }
+    const int64_t orow = row_map ? (int64_t)row_map[row] : row;
+    VecStore<YT, VEC>::store(Y + orow * (ROWB / (int)sizeof(XT)) + lane * VEC, acc);
+    s_cur = s_nx;
+    e_cur = e_nx;
+    s_nx = s_nn;
+    e_nx = e_nn;
+  }
+}
+
+// Persistent grid size: resident blocks per SM (from the occupancy
+// calculator) times the SM count, capped by the blocks the rows need.
+template <class K>
+unsigned persistent_blocks(K kern, int smem, int64_t n_rows, int G) {
+  int dev = 0, per_sm = 0;
+  SCL_CUDA(cudaGetDevice(&dev));
+  SCL_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kSpmmThreads, smem));
+  const int64_t need = (n_rows * G + kSpmmThreads - 1) / kSpmmThreads;
+  int64_t b = (int64_t)std::max(per_sm, 1) * sm_count(dev);
+  if (b > need) b = need;
+  return (unsigned)std::max<int64_t>(b, 1);
+}
+
+template <class VT, class XT, class YT, class AT, int VEC, int S>
+void launch_pipe_s(int G, const SpmmArgs& a, cudaStream_t s) {
+  const int smem = pipe_smem_bytes<S>();
+  const auto* ip = a.indptr;
+  const auto* ix = a.indices;
+  const auto* vv = static_cast<const VT*>(a.values);
+  const auto* xx = static_cast<const XT*>(a.X);
+  auto* yy = static_cast<YT*>(a.Y);
+#define SCL_PIPE_CASE(GG)                                                                                \
+  case GG: {                                                                                             \
+    auto kern = k_spmm_pipe<VT, XT, YT, AT, GG, VEC, (S <= GG ? S : GG)>;                                 \
+    SCL_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));             \
+    SCL_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout,                   \
+                                  (int)cudaSharedmemCarveoutMaxShared));                                 \
+    const dim3 grid(persistent_blocks(kern, smem, a.n_rows, GG));                                        \
+    kern<<<grid, kSpmmThreads, smem, s>>>(ip, ix, vv, xx, yy, a.row_map, a.n_rows, a.F);                  \
+    break;                                                                                               \
+  }
+  switch (G) {
+    SCL_PIPE_CASE(4)
+    SCL_PIPE_CASE(8)
+    SCL_PIPE_CASE(16)
+    SCL_PIPE_CASE(32)
+    default: throw Error(kErrInvalidArgument, "pipelined SpMM needs a lane-group size of 4..32");
+  }
+#undef SCL_PIPE_CASE
+  SCL_CUDA(cudaGetLastError());
 }
 
 // G == 1 needs no shuffles but the template handles it (width-1 shuffles are
@@ -179,20 +724,18 @@ k_spmm(const int64_t* __restrict__ indptr, const int32_t* __restrict__ indices, 
 
 template <class VT, class XT, class YT, class AT, int VEC>
 void launch_g(int G, const SpmmArgs& a, cudaStream_t s) {
-  const int64_t rows_per_block = kSpmmThreads / G;
-  const int64_t blocks = (a.n_rows + rows_per_block - 1) / rows_per_block;
-  SCL_REQUIRE(blocks <= 0x7fffffffLL, kErrInvalidArgument, "too many rows for one launch");
   const auto* ip = a.indptr;
   const auto* ix = a.indices;
   const auto* vv = static_cast<const VT*>(a.values);
   const auto* xx = static_cast<const XT*>(a.X);
   auto* yy = static_cast<YT*>(a.Y);
-  const dim3 grid((unsigned)blocks);
-#define SCL_SPMM_CASE(GG, UU)                                                                      \
-  case GG:                                                                                         \
-    k_spmm<VT, XT, YT, AT, GG, VEC, UU><<<grid, kSpmmThreads, 0, s>>>(ip, ix, vv, xx, yy, a.row_map, \
-                                                                     a.n_rows, a.F);               \
-    break;
+#define SCL_SPMM_CASE(GG, UU)                                                                     \
+  case GG: {                                                                                      \
+    auto kern = k_spmm<VT, XT, YT, AT, GG, VEC, UU>;                                              \
+    const dim3 grid(persistent_blocks(kern, 0, a.n_rows, GG));                                    \
+    kern<<<grid, kSpmmThreads, 0, s>>>(ip, ix, vv, xx, yy, a.row_map, a.n_rows, a.F);             \
+    break;                                                                                        \
+  }
   switch (G) {
     SCL_SPMM_CASE(1, 1)
     SCL_SPMM_CASE(2, 2)
@@ -206,11 +749,132 @@ void launch_g(int G, const SpmmArgs& a, cudaStream_t s) {
   SCL_CUDA(cudaGetLastError());
 }
 
+template <class VT, class XT, class YT, class AT, int VEC, int U>
+void launch_stream_u(const SpmmArgs& a, cudaStream_t s) {
+  auto kern = k_spmm_stream<VT, XT, YT, AT, VEC, U>;
+  const int64_t tasks = (a.n_rows + kStreamRows - 1) / kStreamRows;
+  // one warp per task: ask for tasks*32 "rows" of one lane each
+  const dim3 grid(persistent_blocks(kern, 0, tasks, 32));
+  kern<<<grid, kSpmmThreads, 0, s>>>(a.indptr, a.indices, static_cast<const VT*>(a.values),
+                                     static_cast<const XT*>(a.X), static_cast<YT*>(a.Y), a.row_map, a.n_rows, a.F);
+  SCL_CUDA(cudaGetLastError());
+}
+
+template <class VT, class XT, class YT, class AT, int VEC, int S>
+void launch_spipe_s(const SpmmArgs& a, cudaStream_t s) {
+  constexpr int LB = VEC * (int)sizeof(XT);
+  auto kern = k_spmm_spipe<VT, XT, YT, AT, VEC, S>;
+  const int smem = stream_pipe_smem_bytes<LB, S>();
+  int dev = 0, max_smem = 0;
+  SCL_CUDA(cudaGetDevice(&dev));
+  SCL_CUDA(cudaDeviceGetAttribute(&max_smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+  SCL_REQUIRE(smem <= max_smem, kErrInvalidArgument, "stream pipeline stage does not fit in shared memory");
+  SCL_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+  SCL_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                (int)cudaSharedmemCarveoutMaxShared));
+  const int64_t tasks = (a.n_rows + kStreamRows - 1) / kStreamRows;
+  const dim3 grid(persistent_blocks(kern, smem, tasks, 32));
+  kern<<<grid, kSpmmThreads, smem, s>>>(a.indptr, a.indices, static_cast<const VT*>(a.values),
+                                        static_cast<const XT*>(a.X), static_cast<YT*>(a.Y), a.row_map, a.n_rows, a.F);
+  SCL_CUDA(cudaGetLastError());
+}
+
+template <class VT, class XT, class YT, class AT, int ROWB, int U>
+void launch_row_u(const SpmmArgs& a, cudaStream_t s) {
+  // rows of X addressed by the column indices: n_cols <= n_rows, X holds n_rows rows
+  const bool off32 = (uint64_t)a.n_rows * (uint64_t)ROWB < (1ull << 32);
+  auto kern = off32 ? k_spmm_row<VT, XT, YT, AT, ROWB, U, true> : k_spmm_row<VT, XT, YT, AT, ROWB, U, false>;
+  const dim3 grid(persistent_blocks(kern, 0, a.n_rows, 32));
+  kern<<<grid, kSpmmThreads, 0, s>>>(a.indptr, a.indices, static_cast<const VT*>(a.values),
+                                     static_cast<const XT*>(a.X), static_cast<YT*>(a.Y), a.row_map, a.n_rows);
+  SCL_CUDA(cudaGetLastError());
+}
+
+// kind 4: fixed-pitch warp-per-row kernel; stage = gathers per batch (8/16/32)
+template <class VT, class XT, class YT, class AT>
+void launch_row(const SpmmArgs& a, int U, cudaStream_t s) {
+  const int64_t rowb = a.F * (int64_t)sizeof(XT);
+#define SCL_ROW_CASE(RB)                                                         \
+  if constexpr (RB / 32 >= (int)sizeof(XT)) {                                    \
+    if (rowb == RB) {                                                            \
+      if (U == 8) return launch_row_u<VT, XT, YT, AT, RB, 8>(a, s);              \
+      if (U == 16) return launch_row_u<VT, XT, YT, AT, RB, 16>(a, s);            \
+      if (U == 32) return launch_row_u<VT, XT, YT, AT, RB, 32>(a, s);            \
+      throw Error(kErrInvalidArgument, "row SpMM batch must be 8, 16 or 32");    \
+    }                                                                            \
+  }
+  SCL_ROW_CASE(128)
+  SCL_ROW_CASE(256)
+  SCL_ROW_CASE(512)
+#undef SCL_ROW_CASE
+  throw Error(kErrInvalidArgument, "the fixed-pitch SpMM needs 128-, 256- or 512-byte rows");
+}
+
+// kind 2: register stream (stage = U in {8, 16}); kind 3: cp.async stream
+// pipeline (stage = entries per stage in {16, 32}).
+template <class VT, class XT, class YT, class AT, int VEC>
+void launch_stream(const SpmmArgs& a, int kind, int stage, cudaStream_t s) {
+  if (kind == 2 && stage == 8) return launch_stream_u<VT, XT, YT, AT, VEC, 8>(a, s);
+  if (kind == 2 && stage == 16) return launch_stream_u<VT, XT, YT, AT, VEC, 16>(a, s);
+  if (kind == 3 && stage == 16) return launch_spipe_s<VT, XT, YT, AT, VEC, 16>(a, s);
+  if (kind == 3 && stage == 32) return launch_spipe_s<VT, XT, YT, AT, VEC, 32>(a, s);
+  throw Error(kErrInvalidArgument, "stream SpMM stage must be 8/16 (kind 2) or 16/32 (kind 3)");
+}
+
+// Whole warp per row with a narrow lane chunk (4 or 8 bytes).
+template <class VT, class XT, class YT, class AT, int VEC>
+void launch_warp(const SpmmArgs& a, cudaStream_t s) {
+  auto kern = k_spmm<VT, XT, YT, AT, 32, VEC, 8>;
+  const dim3 grid(persistent_blocks(kern, 0, a.n_rows, 32));
+  kern<<<grid, kSpmmThreads, 0, s>>>(a.indptr, a.indices, static_cast<const VT*>(a.values),
+                                     static_cast<const XT*>(a.X), static_cast<YT*>(a.Y), a.row_map, a.n_rows, a.F);
+  SCL_CUDA(cudaGetLastError());
+}
+
 template <class VT, class XT, class YT, class AT>
 void launch_typed(const SpmmArgs& a, const SpmmPlan& plan, cudaStream_t s) {
   constexpr int kVec = 16 / (int)sizeof(XT);
-  if (plan.vec > 1) launch_g<VT, XT, YT, AT, kVec>(plan.group, a, s);
-  else launch_g<VT, XT, YT, AT, 1>(plan.group, a, s);
+  if (plan.vec > 1 && plan.kind == 1) {
+    switch (plan.stage) {
+      case 4: return launch_pipe_s<VT, XT, YT, AT, kVec, 4>(plan.group, a, s);
+      case 8: return launch_pipe_s<VT, XT, YT, AT, kVec, 8>(plan.group, a, s);
+      case 16: return launch_pipe_s<VT, XT, YT, AT, kVec, 16>(plan.group, a, s);
+      default: throw Error(kErrInvalidArgument, "pipeline stage must be 4, 8 or 16");
+    }
+  }
+  constexpr int kVec8 = 8 / (int)sizeof(XT);  // 8-byte lane chunks
+  constexpr int kVec4 = 4 / (int)sizeof(XT);  // 4-byte lane chunks
+  if (plan.kind == 4) {
+    SCL_REQUIRE(plan.group == 32 && plan.vec * (int64_t)sizeof(XT) * 32 == a.F * (int64_t)sizeof(XT),
+                kErrInvalidArgument, "the fixed-pitch SpMM covers a row with one chunk per lane of a warp");
+    return launch_row<VT, XT, YT, AT>(a, plan.stage, s);
+  }
+  if (plan.kind == 2 || plan.kind == 3) {
+    SCL_REQUIRE(plan.group == 32, kErrInvalidArgument, "the stream SpMM uses a whole warp per row block");
+    const int k = plan.kind, st = plan.stage;
+    if (plan.vec == kVec) return launch_stream<VT, XT, YT, AT, kVec>(a, k, st, s);
+    if constexpr (kVec8 > 1) {
+      if (plan.vec == kVec8) return launch_stream<VT, XT, YT, AT, (kVec8 > 1 ? kVec8 : 2)>(a, k, st, s);
+    }
+    if constexpr (kVec4 > 1) {
+      if (plan.vec == kVec4) return launch_stream<VT, XT, YT, AT, (kVec4 > 1 ? kVec4 : 2)>(a, k, st, s);
+    }
+    if constexpr (sizeof(XT) >= 4) {
+      if (plan.vec == 1) return launch_stream<VT, XT, YT, AT, 1>(a, k, st, s);
+    }
+    throw Error(kErrInvalidArgument, "unsupported lane chunk width for the stream SpMM");
+  }
+  if (plan.vec == kVec) return launch_g<VT, XT, YT, AT, kVec>(plan.group, a, s);
+  if (plan.vec == 1) return launch_g<VT, XT, YT, AT, 1>(plan.group, a, s);
+  // narrower chunks: one warp per row (no divergence between rows in a warp)
+  SCL_REQUIRE(plan.group == 32, kErrInvalidArgument, "4- and 8-byte lane chunks need a whole warp per row");
+  if constexpr (kVec8 > 1) {
+    if (plan.vec == kVec8) return launch_warp<VT, XT, YT, AT, (kVec8 > 1 ? kVec8 : 2)>(a, s);
+  }
+  if constexpr (kVec4 > 1) {
+    if (plan.vec == kVec4) return launch_warp<VT, XT, YT, AT, (kVec4 > 1 ? kVec4 : 2)>(a, s);
+  }
+  throw Error(kErrInvalidArgument, "unsupported lane chunk width");
 }
 
 }  // namespace
@@ -220,6 +884,21 @@ SpmmPlan default_spmm_plan(int64_t F, DType xtype, const void* X, const void* Y,
   SpmmPlan p;
   const int xs = (int)dtype_size(xtype);
   const int ys = (int)dtype_size(ytype);
+  // Rows of 128, 256 or 512 bytes: one warp per row, one 4/8/16-byte chunk per
+  // lane — no divergence between rows sharing a warp, one load per entry.
+  const int64_t rb = F * xs;
+  if (rb == 128 || rb == 256 || rb == 512) {
+    const int lane_bytes = (int)(rb / 32);
+    const int v = lane_bytes / xs;
+    if (v >= 1 && (reinterpret_cast<uintptr_t>(X) % lane_bytes) == 0 &&
+        (reinterpret_cast<uintptr_t>(Y) % (uintptr_t)(v * ys)) == 0) {
+      p.group = 32;
+      p.vec = v;
+      p.kind = 4;
+      p.stage = 8;
+      return p;
+    }
+  }
   const int vec = 16 / xs;
   const bool aligned = ((reinterpret_cast<uintptr_t>(X) & 15u) == 0) && ((reinterpret_cast<uintptr_t>(Y) & 15u) == 0) &&
                        ((F * xs) % 16 == 0) && ((F * ys) % 8 == 0) && (F % vec == 0);
@@ -228,6 +907,12 @@ SpmmPlan default_spmm_plan(int64_t F, DType xtype, const void* X, const void* Y,
   int g = 1;
   while (g < lanes && g < 32) g <<= 1;
   p.group = g;
+  // the cp.async pipeline hides gather latency without register cost; it needs
+  // 16-byte lane chunks and at least 4 lanes per row
+  if (p.vec > 1 && p.group >= 4) {
+    p.kind = 1;
+    p.stage = p.group >= 8 ? 8 : 4;
+  }
   return p;
 }
 
@@ -235,11 +920,17 @@ void spmm_with_plan(const SpmmArgs& a, const SpmmPlan& plan, cudaStream_t s) {
   if (a.n_rows <= 0 || a.F <= 0) return;
   SCL_REQUIRE(plan.group >= 1 && plan.group <= 32 && (plan.group & (plan.group - 1)) == 0, kErrInvalidArgument,
               "lane-group size must be a power of two in [1, 32]");
+  SCL_REQUIRE(plan.kind == 0 || plan.kind == 2 || plan.kind == 3 || plan.kind == 4 ||
+                  (plan.kind == 1 && plan.vec > 1 && plan.group >= 4),
+              kErrInvalidArgument, "the pipelined SpMM needs 16-byte lane chunks and a lane group of at least 4");
   if (plan.vec > 1) {
-    const int xs = (int)dtype_size(a.xtype);
-    SCL_REQUIRE(plan.vec == 16 / xs && a.F % plan.vec == 0 && (reinterpret_cast<uintptr_t>(a.X) & 15u) == 0 &&
-                    (reinterpret_cast<uintptr_t>(a.Y) & 15u) == 0,
+    const int xs = (int)dtype_size(a.xtype), ys = (int)dtype_size(a.ytype);
+    const int xb = plan.vec * xs, yb = plan.vec * ys;
+    SCL_REQUIRE((xb == 4 || xb == 8 || xb == 16) && a.F % plan.vec == 0 &&
+                    reinterpret_cast<uintptr_t>(a.X) % xb == 0 && reinterpret_cast<uintptr_t>(a.Y) % yb == 0,
                 kErrInvalidArgument, "vector SpMM plan does not fit this feature block");
+    SCL_REQUIRE(xb == 16 || plan.group == 32, kErrInvalidArgument,
+                "4- and 8-byte lane chunks need a whole warp per row");
   }
   const DType v = a.vtype, x = a.xtype, y = a.ytype;
   if (v == kF32 && x == kF32 && y == kF32) return launch_typed<float, float, float, float>(a, plan, s);

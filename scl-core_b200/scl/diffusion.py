@@ -58,6 +58,12 @@ def set_degree_mode(mat_or_lib, mode: int) -> None:
     check_error(lib.scl_diffusion_gpu_set_degree_mode(int(mode)), "set_degree_mode", lib)
 
 
+def set_reorder(mat_or_lib, mode: int) -> None:
+    """-1 = automatic (default), 0 = off, 1 = always; results are identical either way."""
+    lib = getattr(mat_or_lib, "lib", mat_or_lib)
+    check_error(lib.scl_diffusion_gpu_set_reorder(int(mode)), "set_reorder", lib)
+
+
 def attach(mat: CsrMatrix) -> None:
     check_error(mat.lib.scl_diffusion_gpu_attach(mat.handle), "attach", mat.lib)
 

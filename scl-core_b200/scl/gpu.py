@@ -119,6 +119,27 @@ class GpuGraph:
         self.storage = code
         return self
 
+    def reorder(self, mode: int = 1, stream=None) -> "GpuGraph":
+        """Group rows by connected component for the diffusion (results unchanged)."""
+        check_error(self._lib.scl_gpu_graph_reorder(self._h, int(mode), _stream_ptr(stream)), "reorder", self._lib)
+        return self
+
+    def set_plan(self, n_features: int, group: int, vec: int = 1, kind: int = 0, stage: int = 8) -> "GpuGraph":
+        """Launch shape used by diffuse() at this width and storage dtype (group <= 0: default)."""
+        check_error(self._lib.scl_gpu_graph_set_plan(self._h, int(n_features), int(group), int(vec), int(kind),
+                                                     int(stage)), "set_plan", self._lib)
+        return self
+
+    def reorder_info(self):
+        """(perm new->old as int32 array, component-labelling rounds)."""
+        n = self.shape[0]
+        perm = np.empty(n, np.int32)
+        rounds = ctypes.c_int()
+        check_error(self._lib.scl_gpu_graph_reorder_info(self._h, ctypes.c_void_p(perm.ctypes.data),
+                                                         ctypes.byref(rounds), _stream_ptr()), "reorder_info",
+                    self._lib)
+        return perm, rounds.value
+
     def export(self, master_dtype=np.float32):
         """(indptr int64, indices int32, values) as host NumPy arrays."""
         n, _, nnz = self.shape
@@ -144,10 +165,11 @@ class GpuGraph:
                                               F, int(n_steps), _stream_ptr(stream)), "diffuse", self._lib)
         return out
 
-    def spmm(self, X, out, group: int = 0, vec: int = 1, stream=None):
+    def spmm(self, X, out, group: int = 0, vec: int = 1, kind: int = 0, stage: int = 8, stream=None):
+        """One Y = P X in the original row order with an explicit launch shape (group <= 0: default)."""
         F = X.shape[1]
         check_error(self._lib.scl_gpu_spmm(self._h, _ptr(X), _ptr(out), dtype_code(out.dtype), F, int(group), int(vec),
-                                           _stream_ptr(stream)), "spmm", self._lib)
+                                           int(kind), int(stage), _stream_ptr(stream)), "spmm", self._lib)
         return out
 
     # ---- lifecycle -------------------------------------------------------------------------

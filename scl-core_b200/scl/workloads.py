@@ -1,0 +1,72 @@
+"""Synthetic diffusion workloads on the device (benchmark and profiling cases).
+
+    python -m scl.workloads spmm --cells 200000 --k 30 --features 64 --steps 3 [--storage bf16] [--no-reorder]
+
+builds the seeded mixture graph on the current GPU (kNN with torch as an input
+generator, then this library's weights / symmetrisation / normalisation /
+reordering) and runs `steps` diffusion steps through scl_gpu_diffuse — the
+case the ncu captures under profiles/ were taken on.
+"""
+from __future__ import annotations
+
+import argparse
+import time
+
+
+def build_graph(n_cells: int, k: int, device="cuda", seed: int = 0, reorder: bool = True, stream=None):
+    """(GpuGraph, knn_idx, knn_dist, timings dict) for the seeded mixture."""
+    import torch
+
+    from . import synthetic
+    from .gpu import GpuGraph
+
+    t0 = time.time()
+    pts = synthetic.mixture(n_cells, seed=seed)
+    ki, kd = synthetic.knn_device(pts, k, device=device, block=2048)
+    torch.cuda.synchronize()
+    t_knn = time.time() - t0
+    s = stream if stream is not None else torch.cuda.current_stream()
+    e0, e1, e2 = (torch.cuda.Event(enable_timing=True) for _ in range(3))
+    e0.record(s)
+    g = GpuGraph.from_knn(ki, kd, stream=s)
+    g.normalize(symmetric=False, stream=s)
+    e1.record(s)
+    if reorder:
+        g.reorder(1, stream=s)
+    e2.record(s)
+    e2.synchronize()
+    return g, ki, kd, {"knn_s": t_knn, "build_ms": e0.elapsed_time(e1), "reorder_ms": e1.elapsed_time(e2)}
+
+
+def _main():
+    import torch
+
+    ap = argparse.ArgumentParser()
+    ap.add_argument("case", choices=["spmm"])
+    ap.add_argument("--cells", type=int, default=200_000)
+    ap.add_argument("--k", type=int, default=30)
+    ap.add_argument("--features", type=int, default=64)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--storage", default="f32", choices=["f32", "bf16", "f16"])
+    ap.add_argument("--no-reorder", action="store_true")
+    ap.add_argument("--plan", default="", help="group,vec,kind,stage launch shape for diffuse (default: built-in)")
+    a = ap.parse_args()
+    g, _, _, tm = build_graph(a.cells, a.k, reorder=not a.no_reorder)
+    if a.storage != "f32":
+        g.set_storage(torch.bfloat16 if a.storage == "bf16" else torch.float16)
+    if a.plan:
+        grp, vec, kind, stage = (int(x) for x in a.plan.split(","))
+        g.set_plan(a.features, grp, vec, kind, stage)
+    X = torch.randn((a.cells, a.features), device="cuda")
+    if a.storage != "f32":
+        X = X.to(torch.bfloat16 if a.storage == "bf16" else torch.float16)
+    Y = g.diffuse(X, a.steps)
+    torch.cuda.synchronize()
+    n, _, nnz = g.shape
+    print(f"cells={n} nnz={nnz} features={a.features} steps={a.steps} storage={a.storage} "
+          f"reorder={not a.no_reorder} build_ms={tm['build_ms']:.2f} reorder_ms={tm['reorder_ms']:.2f} "
+          f"checksum={float(Y.float().sum()):.6e}")
+
+
+if __name__ == "__main__":
+    _main()

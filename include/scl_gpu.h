@@ -103,6 +103,31 @@ SCL_EXPORT scl_error_t scl_gpu_graph_reorder_info(scl_gpu_graph_t graph, int32_t
 SCL_EXPORT scl_error_t scl_gpu_spmm(scl_gpu_graph_t graph, const void* X, void* Y, scl_dtype_t y_dtype,
                                     int64_t n_features, int group, int vec, int kind, int stage, void* stream);
 
+/* Diffusion that allocates no device memory. No counterpart in scl-core.
+ *
+ * For callers that cannot allocate GPU memory while they run: a framework
+ * that owns the whole device-memory budget through its own arena and forbids
+ * outside cudaMalloc, a serving loop that must neither block nor fail on an
+ * allocation after start-up, or code that must not let cudaMalloc/cudaFree
+ * synchronise the device. Computes Y = P^n_steps X (FP32, row-major
+ * n_rows x n_features, the same bits as scl_gpu_diffuse) for a device CSR
+ * transition matrix P given as indptr (int64, n_rows + 1), indices (int32,
+ * each in [0, n_rows)) and values (f32). X and Y are caller-owned device
+ * buffers and must be different; the one intermediate iterate lives in a
+ * fixed 32 MiB scratch array compiled into the library, which every GPU that
+ * loads the library holds until the process exits.
+ *
+ * Limit: n_rows * n_features <= 8,388,608, else SCL_ERROR_INVALID_ARGUMENT
+ * and nothing is launched. The first call on each device looks up the scratch
+ * array's device address (cudaGetSymbolAddress); make that first call before
+ * any stream capture. All calls share the one array and it keeps the last
+ * call's contents (every element is overwritten before it is read, so no
+ * clearing is needed); calls that overlap on the GPU — other streams, other
+ * threads — race on it. Asynchronous on `stream`. */
+SCL_EXPORT scl_error_t scl_gpu_diffuse_noalloc(const int64_t* indptr, const int32_t* indices, const float* values,
+                                               int64_t n_rows, const float* X, float* Y, int64_t n_features,
+                                               int64_t n_steps, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

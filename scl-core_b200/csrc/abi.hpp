@@ -8,6 +8,7 @@
 #include <memory>
 #include <vector>
 
+#include "abi_error.hpp"
 #include "engine.hpp"
 #include "scl_core.h"
 #include "scl_sparse.h"
@@ -19,11 +20,6 @@ using Index = scl_index_t;
 
 constexpr sclgpu::DType kRealDType = sizeof(Real) == 8 ? sclgpu::kF64 : sclgpu::kF32;
 constexpr sclgpu::DType kIndexDType = sizeof(Index) == 8 ? sclgpu::kI64 : sclgpu::kI32;
-
-void set_last_error(scl_error_t code, const char* message) noexcept;
-void clear_last_error() noexcept;
-// Maps the active exception to an error code and records its message.
-scl_error_t handle_exception() noexcept;
 
 // ---- host sparse container ---------------------------------------------------
 // Pointer-per-row storage (scl/core/sparse.hpp:152-170): row i of the primary
@@ -73,29 +69,3 @@ void allocate_blocks(scl_sparse_matrix& m, const std::vector<Index>& lens, Block
 std::vector<int64_t> offsets_of(const scl_sparse_matrix& m);
 }  // namespace sclabi
 
-#define SCL_API_CHECK_NULL(ptr, msg)                                    \
-  do {                                                                  \
-    if ((ptr) == nullptr) {                                             \
-      ::sclabi::set_last_error(SCL_ERROR_NULL_POINTER, (msg));          \
-      return SCL_ERROR_NULL_POINTER;                                    \
-    }                                                                   \
-  } while (0)
-
-#define SCL_API_CHECK(cond, code, msg)                                  \
-  do {                                                                  \
-    if (!(cond)) {                                                      \
-      ::sclabi::set_last_error((code), (msg));                          \
-      return (code);                                                    \
-    }                                                                   \
-  } while (0)
-
-#define SCL_API_TRY try {
-#define SCL_API_CATCH \
-  }                   \
-  catch (...) { return ::sclabi::handle_exception(); }
-
-#define SCL_API_RETURN_OK          \
-  do {                             \
-    ::sclabi::clear_last_error();  \
-    return SCL_OK;                 \
-  } while (0)

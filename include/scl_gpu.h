@@ -97,11 +97,99 @@ SCL_EXPORT scl_error_t scl_gpu_graph_reorder_info(scl_gpu_graph_t graph, int32_t
 /* One Y = P X (original row order) with an explicit launch shape: group lanes
  * per row in {1,2,4,8,16,32}; vec = 16 bytes / element size, or 1; kind 0 =
  * register-gather kernel, 1 = cp.async shared-memory pipeline (vec > 1,
- * group >= 4) with `stage` in {4, 8, 16} entries per stage. group <= 0 picks
- * the default shape. X and Y must be in the storage dtype (Y may also be F32).
- * Every shape computes the same bits. */
+ * group >= 4) with `stage` in {4, 8, 16} entries per stage; 2/3 = row-block
+ * stream (register / cp.async); 4 = warp per row with a compile-time pitch
+ * (stage = gathers per batch 8/16/32); 5 = bf16/f16 storage, warp per row
+ * with one 16-byte chunk per lane, group = row bytes / 16 (8 or 16), so one
+ * load gathers 32/group entries that feed 32/group interleaved fma chains
+ * summed pairwise at the row end (stage = gathers per lane per batch: 2/4/8
+ * for 128-byte rows, 4/8/16 for 256-byte rows); 6 = kind 5 with the
+ * mixed-precision fma. group <= 0 picks the default shape. X and Y must be in
+ * the storage dtype (Y may also be F32). Every shape of kinds 0-4 computes the
+ * same bits (the sequential fma chain); kinds 5 and 6 compute the same bits as
+ * each other (the interleaved chains). */
 SCL_EXPORT scl_error_t scl_gpu_spmm(scl_gpu_graph_t graph, const void* X, void* Y, scl_dtype_t y_dtype,
                                     int64_t n_features, int group, int vec, int kind, int stage, void* stream);
+
+/* ---- gradients (no counterpart in scl-core, which has no backward pass) ----
+ * For L(X_T) with X_T = P^T X_0 and P = normalise(W) (scl_gpu_graph_normalize):
+ * dL/dX_0 = G_0 with G_s = P^T G_{s+1}, G_T = dL/dX_T, and
+ * dL/dW per stored entry through the SDDMM gP_ij = sum_s <G_{s+1}[i], X_s[j]>
+ * and the row / symmetric normalisation (FP64 degrees). All dense blocks are
+ * row-major n x n_features in the graph's master dtype (f32 or f64) on the
+ * device; the storage dtype must be the master dtype. */
+
+/* Replace the graph's values (its pre-normalisation weights W, nnz entries in
+ * the graph's CSR order, f32 or f64, host or device). The graph becomes
+ * un-normalised; call scl_gpu_graph_normalize next. */
+SCL_EXPORT scl_error_t scl_gpu_graph_set_weights(scl_gpu_graph_t graph, const void* values, scl_dtype_t dtype,
+                                                 int on_device, void* stream);
+
+/* Y = P^n_steps X0 (original row order, X0 != Y) keeping checkpoints for
+ * scl_gpu_diffuse_backward: X_s for s = every, 2*every, ... < n_steps, i.e.
+ * (n_steps - 1) / every blocks of n x n_features written to `checkpoints`
+ * (NULL allowed when that count is 0). Same bits as scl_gpu_diffuse. */
+SCL_EXPORT scl_error_t scl_gpu_diffuse_checkpointed(scl_gpu_graph_t graph, const void* X0, void* Y,
+                                                    int64_t n_features, int64_t n_steps, int64_t every,
+                                                    void* checkpoints, void* stream);
+
+/* Backward of scl_gpu_diffuse_checkpointed with the same X0, checkpoints,
+ * n_steps and every: given dY = dL/dX_T, writes dX0 = dL/dX_0 and, when dW is
+ * non-NULL, dW = dL/dW (nnz entries, graph CSR order; dL/dP when the graph was
+ * not normalised). Each checkpoint segment is recomputed with the forward
+ * SpMM; each backward step is one fused kernel over the CSC view of P (built
+ * once per graph) that gathers G_{s+1} rows once for both the transpose-SpMM
+ * and the per-entry SDDMM. */
+SCL_EXPORT scl_error_t scl_gpu_diffuse_backward(scl_gpu_graph_t graph, const void* X0, const void* checkpoints,
+                                                const void* dY, int64_t n_features, int64_t n_steps, int64_t every,
+                                                void* dX0, void* dW, void* stream);
+
+/* ---- batched diffusion (no counterpart in scl-core, which diffuses one graph
+ * per call: scl/binding/c_api/diffusion.h:28-35) ----
+ * Many independent graphs of uneven size, each with its own dense block, all
+ * n_steps steps in ONE persistent kernel launch replayed from a CUDA graph.
+ * The graphs (normalised, f32 values and storage, on the current device) are
+ * copied into one block-diagonal CSR at creation; the dense blocks are the
+ * graphs' blocks stacked row-wise: graph b's rows start at row_offsets[b] of a
+ * (row_offsets[n_graphs]) x n_features f32 block. Each graph's result is
+ * bit-identical to scl_gpu_diffuse of that graph alone. A work item waits for
+ * its graph's previous step with an iteration limit (about a second); a wait
+ * that gives up sets the batch status (scl_gpu_batch_status) to
+ * SCL_ERROR_CONVERGENCE and the launch returns early. */
+typedef struct scl_gpu_batch scl_gpu_batch;
+typedef scl_gpu_batch* scl_gpu_batch_t;
+
+SCL_EXPORT scl_error_t scl_gpu_batch_create(scl_gpu_batch_t* out, int64_t n_graphs, const scl_gpu_graph_t* graphs,
+                                            int64_t n_features, int64_t n_steps, void* stream);
+SCL_EXPORT scl_error_t scl_gpu_batch_destroy(scl_gpu_batch_t* batch);
+/* row_offsets: host int64 [n_graphs + 1] (may be NULL); nnz_total and n_tiles may be NULL. */
+SCL_EXPORT scl_error_t scl_gpu_batch_layout(scl_gpu_batch_t batch, int64_t* row_offsets, int64_t* nnz_total,
+                                            int64_t* n_tiles);
+/* Explicit schedule: about tile_nnz stored entries per tile, unroll (4 or 8)
+ * gathers in flight per lane, blocks_per_sm resident CTAs (0 = occupancy
+ * limit). Drops the captured CUDA graph. */
+SCL_EXPORT scl_error_t scl_gpu_batch_set_schedule(scl_gpu_batch_t batch, int64_t tile_nnz, int unroll,
+                                                  int blocks_per_sm, void* stream);
+/* Autotuner: times every candidate schedule (tile size x unroll x CTAs per
+ * SM) on these blocks, `reps` launches each, and keeps the fastest.
+ * Synchronises `stream`; Y is overwritten. */
+SCL_EXPORT scl_error_t scl_gpu_batch_autotune(scl_gpu_batch_t batch, const float* X0, float* Y, int reps,
+                                              void* stream);
+SCL_EXPORT scl_error_t scl_gpu_batch_schedule(scl_gpu_batch_t batch, int64_t* tile_nnz, int* unroll, int* grid,
+                                              int* lanes_per_row, double* tuned_ms);
+/* Y = P_b^n_steps X0_b for every graph b (X0 != Y). The first call captures
+ * the memset + kernel into a CUDA graph; later calls replay it (updating the
+ * block pointers when they change). Asynchronous on `stream`. */
+SCL_EXPORT scl_error_t scl_gpu_batch_solve(scl_gpu_batch_t batch, const float* X0, float* Y, void* stream);
+/* Synchronises `stream`, returns the status of the launches since the last
+ * call (0 = ok, SCL_ERROR_CONVERGENCE = a wait gave up; item = its work item)
+ * and clears it. */
+SCL_EXPORT scl_error_t scl_gpu_batch_status(scl_gpu_batch_t batch, int* code, int* item, void* stream);
+/* Failure-path test hook: while graph >= 0, that graph's step waits need one
+ * more finished tile than exists, so they give up after their time limit and
+ * the next scl_gpu_batch_status reports SCL_ERROR_CONVERGENCE; -1 turns it off.
+ * Results of a stalled launch are undefined. */
+SCL_EXPORT scl_error_t scl_gpu_batch_inject_stall(scl_gpu_batch_t batch, int graph);
 
 /* Diffusion that allocates no device memory. No counterpart in scl-core.
  *

@@ -254,6 +254,50 @@ void oracle_diffuse_lowp(int64_t n, const int64_t* indptr, const int64_t* indice
   free(v); free(a); free(b);
 }
 
+/* Interleaved-chain form of the 16-bit storage diffusion. The B200 kernel for
+ * bf16/f16 storage gathers Q entries per load instruction (Q = 32 lanes /
+ * lanes per row): chain q (0 <= q < Q) is the sequential fma over the row's
+ * entries q, q+Q, q+2Q, ... in stored order, and the chains are summed
+ * pairwise over the bits of q from the lowest: Q=2 -> c0+c1,
+ * Q=4 -> (c0+c1)+(c2+c3). Q=1 is oracle_diffuse_lowp. Same rounding of the
+ * stored values and iterates as oracle_diffuse_lowp. */
+static void spmm_f32_chains(int64_t n, const int64_t* indptr, const int64_t* indices,
+                            const float* v, const float* X, float* Y, int64_t F, int Q) {
+  float c[32];
+  for (int64_t i = 0; i < n; ++i) {
+    for (int64_t col = 0; col < F; ++col) {
+      for (int q = 0; q < Q; ++q) c[q] = 0.0f;
+      for (int64_t p = indptr[i]; p < indptr[i + 1]; ++p) {
+        const int q = (int)((p - indptr[i]) % Q);
+        c[q] = fmaf(v[p], X[indices[p] * F + col], c[q]);
+      }
+      for (int w = 1; w < Q; w <<= 1)
+        for (int q = 0; q < Q; q += 2 * w) c[q] = c[q] + c[q + w];
+      Y[i * F + col] = c[0];
+    }
+  }
+}
+
+void oracle_diffuse_lowp_chains(int64_t n, const int64_t* indptr, const int64_t* indices,
+                                const float* values_f32, const float* X0_f32, float* Y_out,
+                                int64_t F, int64_t steps, int kind, int final_f32, int chains) {
+  const int64_t nnz = indptr[n];
+  float* v = (float*)malloc(sizeof(float) * (size_t)(nnz > 0 ? nnz : 1));
+  float* a = (float*)malloc(sizeof(float) * (size_t)(n * F > 0 ? n * F : 1));
+  float* b = (float*)malloc(sizeof(float) * (size_t)(n * F > 0 ? n * F : 1));
+  for (int64_t p = 0; p < nnz; ++p) v[p] = lowp_round(values_f32[p], kind);
+  for (int64_t q = 0; q < n * F; ++q) a[q] = lowp_round(X0_f32[q], kind);
+  for (int64_t s = 0; s < steps; ++s) {
+    spmm_f32_chains(n, indptr, indices, v, a, b, F, chains);
+    const int last = (s == steps - 1);
+    if (!(last && final_f32))
+      for (int64_t q = 0; q < n * F; ++q) b[q] = lowp_round(b[q], kind);
+    float* t = a; a = b; b = t;
+  }
+  memcpy(Y_out, a, sizeof(float) * (size_t)(n * F));
+  free(v); free(a); free(b);
+}
+
 /* ===================================================================== */
 /* Graph build: Gaussian weights (kernel.hpp:403-453 sigma = max of the     */
 /* first k stored distances, floored at MIN_BANDWIDTH; w = exp(-(d/s)^2)).  */

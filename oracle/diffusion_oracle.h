@@ -70,6 +70,11 @@ void oracle_diffuse_matrix_f64(int64_t n, const int64_t* indptr, const int64_t* 
 void oracle_diffuse_lowp(int64_t n, const int64_t* indptr, const int64_t* indices,
                          const float* values_f32, const float* X0_f32, float* Y_out,
                          int64_t F, int64_t steps, int kind, int final_f32);
+/* Same with Q interleaved fma chains per row summed pairwise (the entry order
+ * of the B200 kernel for 16-bit storage). */
+void oracle_diffuse_lowp_chains(int64_t n, const int64_t* indptr, const int64_t* indices,
+                                const float* values_f32, const float* X0_f32, float* Y_out,
+                                int64_t F, int64_t steps, int kind, int final_f32, int chains);
 
 /* RNE conversions used above, exposed for tests. */
 uint16_t oracle_f32_to_bf16(float x);

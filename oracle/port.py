@@ -32,6 +32,7 @@ _SIGS = {
     "oracle_diffuse_matrix_f32": ([_i64, _p, _p, _p, _p, _i64, _i64], None),
     "oracle_diffuse_matrix_f64": ([_i64, _p, _p, _p, _p, _i64, _i64], None),
     "oracle_diffuse_lowp": ([_i64, _p, _p, _p, _p, _p, _i64, _i64, _int, _int], None),
+    "oracle_diffuse_lowp_chains": ([_i64, _p, _p, _p, _p, _p, _i64, _i64, _int, _int, _int], None),
     "oracle_f32_to_bf16": ([ctypes.c_float], ctypes.c_uint16),
     "oracle_bf16_to_f32": ([ctypes.c_uint16], ctypes.c_float),
     "oracle_f32_to_f16": ([ctypes.c_float], ctypes.c_uint16),
@@ -131,6 +132,20 @@ def diffuse_lowp(indptr, indices, values_f32, X0_f32, steps, kind, final_f32=Tru
     Y = np.empty((n, F), np.float32)
     lib().oracle_diffuse_lowp(n, _ptr(indptr), _ptr(indices), _ptr(v), _ptr(X0), _ptr(Y), F, steps,
                               int(kind), int(final_f32))
+    return Y
+
+
+def diffuse_lowp_chains(indptr, indices, values_f32, X0_f32, steps, kind, chains, final_f32=True):
+    """16-bit storage diffusion with `chains` interleaved fma chains per row
+    (oracle_diffuse_lowp_chains)."""
+    indptr, indices = _csr(indptr, indices)
+    n = indptr.size - 1
+    v = np.ascontiguousarray(values_f32, np.float32)
+    X0 = np.ascontiguousarray(X0_f32, np.float32)
+    F = X0.shape[1]
+    Y = np.empty((n, F), np.float32)
+    lib().oracle_diffuse_lowp_chains(n, _ptr(indptr), _ptr(indices), _ptr(v), _ptr(X0), _ptr(Y), F, steps,
+                                     int(kind), int(final_f32), int(chains))
     return Y
 
 

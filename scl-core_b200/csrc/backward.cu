@@ -1,0 +1,436 @@
+// Backward pass of the diffusion X_T = P^T X_0, P = normalise(W), for a loss
+// L(X_T) whose gradient dL/dX_T the caller supplies.
+//
+//   G_T = dL/dX_T;   G_s = P^T G_{s+1};   dL/dX_0 = G_0
+//   gP_ij = sum_s <G_{s+1}[i,:], X_s[j,:]>        (SDDMM over the stored entries)
+//   row:  dW_ij = (gP_ij - u_i) / d_i,              u_i = sum_c gP_ic P_ic
+//   sym:  dW_ij = gP_ij a_i a_j - (u_i + v_i)/(2 d_i), v_i = sum_r gP_ri P_ri, a = d^-1/2
+//   rows with d_i <= 1e-15 were zeroed by the forward and get dW = 0.
+//
+// No scl-core counterpart (scl-core has no gradients); the forward it
+// differentiates is scl/kernel/diffusion.hpp:492-603 (transition) and 638-664
+// (diffuse_matrix). The FP64 restatement the tests check against is
+// oracle_adjoint_f64 in the oracle.
+//
+// Kernels:
+//   k_adj_step  one fused step over the CSC view of P (the CSR of P^T, built
+//               once per graph by transpose_map): a warp owns row i of P^T,
+//               keeps X_s[i] in registers, and for every stored entry (j, i) of
+//               P gathers G_{s+1}[j] ONCE for both uses — the fma chain of
+//               G_s[i] and the dot <G_{s+1}[j], X_s[i]> that is gP's term for
+//               that entry. The 32 per-lane partial dots of a chunk of 32
+//               entries are summed by a transposed butterfly (31 shuffles per
+//               32 entries, lane l ends with entry l's total), and lane l adds
+//               it to gPt[chunk + l] — a coalesced read-modify-write in CSC
+//               order that no other warp touches (no atomics).
+//   k_norm_*    normalisation backward in FP64 (degrees kept by normalize).
+// Checkpointing: the forward stores X_s for s = every, 2*every, ... < T; the
+// backward recomputes each segment from its checkpoint with the forward SpMM
+// (the same kernel, so the same bits) and walks it in reverse.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <vector>
+
+#include "engine.hpp"
+
+namespace sclgpu {
+namespace {
+
+constexpr double kMinProbB = 1e-15;  // diffusion.hpp:41 config::MIN_PROB
+
+inline unsigned nblk(int64_t items, int per) {
+  return (unsigned)std::max<int64_t>(1, (items + per - 1) / per);
+}
+
+template <int BYTES> struct Raw;
+template <> struct Raw<4> { using type = unsigned int; };
+template <> struct Raw<8> { using type = uint2; };
+template <> struct Raw<16> { using type = uint4; };
+
+template <class T, int VEC>
+__device__ __forceinline__ void load_vec(const T* __restrict__ p, T (&out)[VEC]) {
+  if constexpr (VEC == 1) {
+    out[0] = __ldg(p);
+  } else {
+    using R = typename Raw<VEC * (int)sizeof(T)>::type;
+    const R raw = __ldg(reinterpret_cast<const R*>(p));
+    const T* e = reinterpret_cast<const T*>(&raw);
+#pragma unroll
+    for (int i = 0; i < VEC; ++i) out[i] = e[i];
+  }
+}
+
+template <class T, int VEC>
+__device__ __forceinline__ void store_vec(T* __restrict__ p, const T (&in)[VEC]) {
+  if constexpr (VEC == 1) {
+    p[0] = in[0];
+  } else {
+    using R = typename Raw<VEC * (int)sizeof(T)>::type;
+    R raw;
+    T* e = reinterpret_cast<T*>(&raw);
+#pragma unroll
+    for (int i = 0; i < VEC; ++i) e[i] = in[i];
+    *reinterpret_cast<R*>(p) = raw;
+  }
+}
+
+__device__ __forceinline__ float fma_t(float a, float b, float c) { return __fmaf_rn(a, b, c); }
+__device__ __forceinline__ double fma_t(double a, double b, double c) { return __fma_rn(a, b, c); }
+
+// Sum across the warp of 32 per-lane arrays: on return lane l holds
+// sum over lanes of p[l]. Five butterfly rounds; in each a lane keeps the half
+// of its live entries selected by its lane bit and sends the other half.
+template <class T>
+__device__ __forceinline__ T transpose_reduce32(T (&p)[32], int lane) {
+#pragma unroll
+  for (int h = 16; h >= 1; h >>= 1) {
+    const bool hi = (lane & h) != 0;
+#pragma unroll
+    for (int k = 0; k < h; ++k) {
+      const T send = hi ? p[k] : p[k + h];
+      const T keep = hi ? p[k + h] : p[k];
+      p[k] = keep + __shfl_xor_sync(0xffffffffu, send, h);
+    }
+  }
+  return p[0];
+}
+
+// One backward step. Warp per row i of P^T (persistent grid-stride); lane l
+// owns columns [c0 + l*VEC, c0 + l*VEC + VEC) of each column block of
+// 32*VEC columns (VEC > 1 requires F % VEC == 0 and aligned rows).
+// G0[i] = sum_q Pt[q] * G1[tidx[q]] in stored order (sequential fma chain);
+// gPt[q] += <G1[tidx[q]], Xs[i]> when gPt is non-null.
+template <class T, int VEC, int U>
+__global__ void __launch_bounds__(256)
+k_adj_step(const int64_t* __restrict__ tptr, const int32_t* __restrict__ tidx, const T* __restrict__ tval,
+           const T* __restrict__ G1, const T* __restrict__ Xs, T* __restrict__ G0, T* __restrict__ gPt, int64_t n,
+           int64_t F) {
+  static_assert(32 % U == 0, "batch must divide 32");
+  const int lane = threadIdx.x & 31;
+  const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
+  constexpr int CPB = 32 * VEC;  // columns per block
+  for (int64_t row = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; row < n; row += nw) {
+    const int64_t start = tptr[row], end = tptr[row + 1];
+    for (int64_t c0 = 0; c0 < F; c0 += CPB) {
+      const int64_t col = c0 + (int64_t)lane * VEC;
+      const bool active = col < F;
+      T xi[VEC], acc[VEC];
+#pragma unroll
+      for (int i = 0; i < VEC; ++i) {
+        xi[i] = T(0);
+        acc[i] = T(0);
+      }
+      if (active) load_vec<T, VEC>(Xs + row * F + col, xi);
+      const T* __restrict__ Gc = G1 + (active ? col : 0);
+      for (int64_t base = start; base < end; base += 32) {
+        const int64_t m = base + lane;
+        int32_t j_l = 0;
+        T v_l = T(0);
+        if (m < end) {
+          j_l = __ldcs(tidx + m);
+          v_l = __ldcs(tval + m);
+        }
+        const int cnt = (int)((end - base) < 32 ? (end - base) : 32);
+        T p[32];
+#pragma unroll
+        for (int t = 0; t < 32; ++t) p[t] = T(0);
+#pragma unroll
+        for (int t = 0; t < 32; t += U) {
+          if (t < cnt) {
+            T g[U][VEC];
+#pragma unroll
+            for (int u = 0; u < U; ++u) {
+              const int32_t jj = __shfl_sync(0xffffffffu, j_l, t + u);
+              if (t + u < cnt && active) {
+                load_vec<T, VEC>(Gc + (int64_t)jj * F, g[u]);
+              } else {
+#pragma unroll
+                for (int i = 0; i < VEC; ++i) g[u][i] = T(0);
+              }
+            }
+#pragma unroll
+            for (int u = 0; u < U; ++u) {
+              const T vv = __shfl_sync(0xffffffffu, v_l, t + u);
+              if (t + u < cnt) {
+                T d = g[u][0] * xi[0];
+#pragma unroll
+                for (int i = 1; i < VEC; ++i) d = fma_t(g[u][i], xi[i], d);
+                p[t + u] = d;
+#pragma unroll
+                for (int i = 0; i < VEC; ++i) acc[i] = fma_t(vv, g[u][i], acc[i]);
+              }
+            }
+          }
+        }
+        if (gPt != nullptr) {
+          const T tot = transpose_reduce32<T>(p, lane);
+          if (lane < cnt) gPt[m] += tot;
+        }
+      }
+      if (active) store_vec<T, VEC>(G0 + row * F + col, acc);
+    }
+  }
+}
+
+template <class T>
+__global__ void k_scatter_entries(const T* __restrict__ src, const int32_t* __restrict__ map, int64_t nnz,
+                                  T* __restrict__ dst) {
+  for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < nnz; q += (int64_t)gridDim.x * blockDim.x)
+    dst[map[q]] = src[q];
+}
+
+template <class T>
+__global__ void k_gather_by_map(const T* __restrict__ src, const int32_t* __restrict__ map, int64_t nnz,
+                                T* __restrict__ dst) {
+  for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < nnz; q += (int64_t)gridDim.x * blockDim.x)
+    dst[q] = src[map[q]];
+}
+
+// out[i] = sum over row i of a[p] * b[p] in FP64 (warp per row).
+template <class T>
+__global__ void k_row_dot(const int64_t* __restrict__ ptr, const T* __restrict__ a, const T* __restrict__ b,
+                          int64_t n, double* __restrict__ out) {
+  const int64_t row = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (row >= n) return;
+  double s = 0.0;
+  for (int64_t p = ptr[row] + lane, e = ptr[row + 1]; p < e; p += 32) s += (double)a[p] * (double)b[p];
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+  if (lane == 0) out[row] = s;
+}
+
+template <class T>
+__global__ void k_norm_bwd(const int64_t* __restrict__ ptr, const int32_t* __restrict__ idx,
+                           const T* __restrict__ gP, const double* __restrict__ deg, const double* __restrict__ u,
+                           const double* __restrict__ v, int64_t n, int symmetric, T* __restrict__ dW) {
+  const int64_t row = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (row >= n) return;
+  const double di = deg[row];
+  const bool live = di > kMinProbB;
+  const double ai = live ? 1.0 / sqrt(di) : 0.0;
+  const double shift = live ? (symmetric ? (u[row] + v[row]) / (2.0 * di) : u[row]) : 0.0;
+  for (int64_t p = ptr[row] + lane, e = ptr[row + 1]; p < e; p += 32) {
+    double r = 0.0;
+    if (live) {
+      if (symmetric) {
+        const double dj = deg[idx[p]];
+        const double aj = dj > kMinProbB ? 1.0 / sqrt(dj) : 0.0;
+        r = (double)gP[p] * ai * aj - shift;
+      } else {
+        r = ((double)gP[p] - shift) / di;
+      }
+    }
+    dW[p] = (T)r;
+  }
+}
+
+template <class T, int VEC, int U>
+void launch_adj(const CsrView& t, const T* G1, const T* Xs, T* G0, T* gPt, int64_t F, cudaStream_t s) {
+  auto kern = k_adj_step<T, VEC, U>;
+  int dev = 0, per_sm = 0;
+  SCL_CUDA(cudaGetDevice(&dev));
+  SCL_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, 256, 0));
+  const int64_t need = (t.n_rows * 32 + 255) / 256;
+  const int64_t grid = std::max<int64_t>(1, std::min<int64_t>(need, (int64_t)std::max(per_sm, 1) * sm_count(dev)));
+  kern<<<(unsigned)grid, 256, 0, s>>>(t.indptr, t.indices, static_cast<const T*>(t.values), G1, Xs, G0, gPt,
+                                      t.n_rows, F);
+  SCL_CUDA(cudaGetLastError());
+}
+
+template <class T>
+void adj_step(const CsrView& t, const T* G1, const T* Xs, T* G0, T* gPt, int64_t F, cudaStream_t s) {
+  constexpr int kV16 = 16 / (int)sizeof(T);
+  const auto al = [&](const void* p, int b) { return (reinterpret_cast<uintptr_t>(p) % (uintptr_t)b) == 0; };
+  // one 16-byte chunk per lane when the row fits one column block of the warp
+  if (F % kV16 == 0 && F <= 32 * kV16 && F > 16 * kV16 && al(G1, 16) && al(Xs, 16) && al(G0, 16))
+    return launch_adj<T, kV16, 8>(t, G1, Xs, G0, gPt, F, s);
+  if constexpr (kV16 / 2 > 1) {
+    constexpr int kV8 = kV16 / 2;
+    if (F % kV8 == 0 && F <= 32 * kV8 && F > 16 * kV8 && al(G1, 8) && al(Xs, 8) && al(G0, 8))
+      return launch_adj<T, kV8, 8>(t, G1, Xs, G0, gPt, F, s);
+  }
+  return launch_adj<T, 1, 8>(t, G1, Xs, G0, gPt, F, s);
+}
+
+}  // namespace
+
+// ---- CSC view ---------------------------------------------------------------------
+void build_adjoint(const DeviceCSR& g, Adjoint& a, cudaStream_t s) {
+  transpose_map(g, a.t, a.tmap, s);
+  a.values_ok = false;
+}
+
+void adjoint_values(const void* vals, DType t, Adjoint& a, cudaStream_t s) {
+  SCL_REQUIRE(t == kF32 || t == kF64, kErrTypeMismatch, "the backward pass needs f32 or f64 values");
+  const int64_t nnz = a.t.nnz;
+  if (!a.t.values.p || a.t.vtype != t) a.t.values = DevBuf(std::max<int64_t>(nnz, 1) * dtype_size(t), s);
+  a.t.vtype = t;
+  if (nnz > 0) {
+    const unsigned b = std::min<unsigned>(nblk(nnz, 256), 148u * 16u);
+    if (t == kF32)
+      k_gather_by_map<float><<<b, 256, 0, s>>>(static_cast<const float*>(vals), a.tmap.as<int32_t>(), nnz,
+                                                a.t.values.as<float>());
+    else
+      k_gather_by_map<double><<<b, 256, 0, s>>>(static_cast<const double*>(vals), a.tmap.as<int32_t>(), nnz,
+                                                 a.t.values.as<double>());
+    SCL_CUDA(cudaGetLastError());
+  }
+  a.values_ok = true;
+}
+
+// ---- checkpointed forward -------------------------------------------------------------
+int64_t checkpoint_slots(int64_t steps, int64_t every) { return steps > 0 ? (steps - 1) / every : 0; }
+
+void diffuse_checkpointed(const CsrView& g, const void* X0, void* Y, DType t, int64_t F, int64_t steps,
+                          int64_t every, void* ckpt, cudaStream_t s) {
+  SCL_REQUIRE(t == kF32 || t == kF64, kErrTypeMismatch, "checkpointed diffusion needs f32 or f64 values");
+  SCL_REQUIRE(g.vtype == t, kErrTypeMismatch, "graph values and the iterate must have the same dtype");
+  SCL_REQUIRE(g.n_rows == g.n_cols, kErrDimensionMismatch, "diffusion with checkpoints needs a square matrix");
+  SCL_REQUIRE(every >= 1, kErrInvalidArgument, "checkpoint interval must be >= 1");
+  const int64_t n = g.n_rows;
+  const size_t blk = (size_t)n * (size_t)F * dtype_size(t);
+  if (steps <= 0) {
+    if (X0 != Y) SCL_CUDA(cudaMemcpyAsync(Y, X0, blk, cudaMemcpyDeviceToDevice, s));
+    return;
+  }
+  SCL_REQUIRE(X0 != Y, kErrInvalidArgument, "checkpointed diffusion needs distinct input and output blocks");
+  DevBuf A, B;
+  SpmmArgs a{};
+  a.indptr = g.indptr;
+  a.indices = g.indices;
+  a.values = g.values;
+  a.vtype = t;
+  a.n_rows = n;
+  a.F = F;
+  a.xtype = t;
+  a.ytype = t;
+  const void* src = X0;
+  for (int64_t st = 0; st < steps; ++st) {
+    const int64_t made = st + 1;  // index of the iterate this step produces
+    void* dst;
+    if (made == steps) {
+      dst = Y;
+    } else if (made % every == 0) {
+      dst = static_cast<char*>(ckpt) + (size_t)(made / every - 1) * blk;
+    } else {
+      if (!A.p) A = DevBuf(blk, s);
+      if (src == A.p) {
+        if (!B.p) B = DevBuf(blk, s);
+        dst = B.p;
+      } else {
+        dst = A.p;
+      }
+    }
+    a.X = src;
+    a.Y = dst;
+    spmm(a, s);
+    src = dst;
+  }
+}
+
+// ---- backward ---------------------------------------------------------------------------
+template <class T>
+static void backward_typed(const CsrView& g, const Adjoint& adj, const T* X0, const T* ckpt, const T* dY,
+                           int64_t F, int64_t steps, int64_t every, T* dX0, T* gPt, cudaStream_t s) {
+  const int64_t n = g.n_rows;
+  const size_t blk = (size_t)n * (size_t)F * sizeof(T);
+  const CsrView tv = adj.t.view();
+  if (gPt) SCL_CUDA(cudaMemsetAsync(gPt, 0, std::max<int64_t>(g.nnz, 1) * sizeof(T), s));
+  if (steps <= 0) {
+    SCL_CUDA(cudaMemcpyAsync(dX0, dY, blk, cudaMemcpyDeviceToDevice, s));
+    return;
+  }
+  const int64_t seg = std::min<int64_t>(every, steps);
+  // segment iterates X_c .. X_{c+seg-1}: slot 0 aliases the checkpoint
+  std::vector<DevBuf> xs(seg);
+  for (int64_t k = 1; k < seg; ++k) xs[k] = DevBuf(blk, s);
+  DevBuf Ga(blk, s), Gb(blk, s);
+  const T* Gcur = dY;
+  SpmmArgs a{};
+  a.indptr = g.indptr;
+  a.indices = g.indices;
+  a.values = g.values;
+  a.vtype = g.vtype;
+  a.n_rows = n;
+  a.F = F;
+  a.xtype = g.vtype;
+  a.ytype = g.vtype;
+  const int64_t last_c = ((steps - 1) / every) * every;
+  for (int64_t c = last_c; c >= 0; c -= every) {
+    const int64_t e = std::min<int64_t>(c + every, steps);
+    const T* base = (c == 0) ? X0 : ckpt + (size_t)(c / every - 1) * (size_t)n * (size_t)F;
+    std::vector<const T*> X(e - c);
+    X[0] = base;
+    for (int64_t st = c; st < e - 1; ++st) {  // recompute X_{c+1} .. X_{e-1}
+      a.X = X[st - c];
+      a.Y = xs[st - c + 1].p;
+      spmm(a, s);
+      X[st - c + 1] = xs[st - c + 1].as<T>();
+    }
+    for (int64_t st = e - 1; st >= c; --st) {
+      T* Gnext = (st == 0) ? dX0 : ((Gcur == Ga.as<T>()) ? Gb.as<T>() : Ga.as<T>());
+      adj_step<T>(tv, Gcur, X[st - c], Gnext, gPt, F, s);
+      Gcur = Gnext;
+    }
+  }
+}
+
+void diffuse_backward(const CsrView& g, const Adjoint& adj, const void* X0, const void* ckpt, const void* dY,
+                      DType t, int64_t F, int64_t steps, int64_t every, void* dX0, void* gPt, cudaStream_t s) {
+  SCL_REQUIRE(t == kF32 || t == kF64, kErrTypeMismatch, "the backward pass needs f32 or f64 values");
+  SCL_REQUIRE(g.vtype == t && adj.values_ok && adj.t.vtype == t, kErrInternal, "adjoint view is stale");
+  SCL_REQUIRE(every >= 1, kErrInvalidArgument, "checkpoint interval must be >= 1");
+  if (t == kF32)
+    backward_typed<float>(g, adj, static_cast<const float*>(X0), static_cast<const float*>(ckpt),
+                          static_cast<const float*>(dY), F, steps, every, static_cast<float*>(dX0),
+                          static_cast<float*>(gPt), s);
+  else
+    backward_typed<double>(g, adj, static_cast<const double*>(X0), static_cast<const double*>(ckpt),
+                           static_cast<const double*>(dY), F, steps, every, static_cast<double*>(dX0),
+                           static_cast<double*>(gPt), s);
+}
+
+template <class T>
+static void norm_bwd_typed(const CsrView& P, const Adjoint& adj, const T* gPt, const double* degrees, int symmetric,
+                           T* dW, cudaStream_t s) {
+  const int64_t n = P.n_rows, nnz = P.nnz;
+  if (nnz == 0) return;
+  DevBuf gP(nnz * sizeof(T), s), u(std::max<int64_t>(n, 1) * 8, s), v(std::max<int64_t>(n, 1) * 8, s);
+  const unsigned b = std::min<unsigned>(nblk(nnz, 256), 148u * 16u);
+  k_scatter_entries<T><<<b, 256, 0, s>>>(gPt, adj.tmap.as<int32_t>(), nnz, gP.as<T>());
+  k_row_dot<T><<<nblk(n * 32, 256), 256, 0, s>>>(P.indptr, gP.as<T>(), static_cast<const T*>(P.values), n,
+                                                 u.as<double>());
+  if (symmetric)
+    k_row_dot<T><<<nblk(n * 32, 256), 256, 0, s>>>(adj.t.indptr.as<int64_t>(), gPt, adj.t.values.as<T>(), n,
+                                                   v.as<double>());
+  k_norm_bwd<T><<<nblk(n * 32, 256), 256, 0, s>>>(P.indptr, P.indices, gP.as<T>(), degrees, u.as<double>(),
+                                                  v.as<double>(), n, symmetric, dW);
+  SCL_CUDA(cudaGetLastError());
+}
+
+void normalize_backward(const CsrView& P, const Adjoint& adj, const void* gPt, const double* degrees, int symmetric,
+                        void* dW, cudaStream_t s) {
+  SCL_REQUIRE(P.vtype == adj.t.vtype, kErrInternal, "adjoint view is stale");
+  if (P.vtype == kF32)
+    norm_bwd_typed<float>(P, adj, static_cast<const float*>(gPt), degrees, symmetric, static_cast<float*>(dW), s);
+  else
+    norm_bwd_typed<double>(P, adj, static_cast<const double*>(gPt), degrees, symmetric, static_cast<double*>(dW), s);
+}
+
+void scatter_adjoint_entries(const Adjoint& adj, const void* gPt, DType t, void* gP, cudaStream_t s) {
+  const int64_t nnz = adj.t.nnz;
+  if (nnz == 0) return;
+  const unsigned b = std::min<unsigned>(nblk(nnz, 256), 148u * 16u);
+  if (t == kF32)
+    k_scatter_entries<float><<<b, 256, 0, s>>>(static_cast<const float*>(gPt), adj.tmap.as<int32_t>(), nnz,
+                                               static_cast<float*>(gP));
+  else
+    k_scatter_entries<double><<<b, 256, 0, s>>>(static_cast<const double*>(gPt), adj.tmap.as<int32_t>(), nnz,
+                                                static_cast<double*>(gP));
+  SCL_CUDA(cudaGetLastError());
+}
+
+}  // namespace sclgpu

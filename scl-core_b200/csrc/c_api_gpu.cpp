@@ -1,6 +1,7 @@
 // Device-pointer extension C ABI (scl_gpu.h). No scl-core counterpart: these
 // entry points keep the graph resident on the GPU and take raw device buffers
 // and a caller stream, for the autograd wrapper and device-side callers.
+#include <algorithm>
 #include <cstring>
 #include <map>
 #include <utility>
@@ -10,6 +11,11 @@
 #include "scl_gpu.h"
 
 using namespace sclgpu;
+
+struct scl_gpu_batch {
+  int device = -1;
+  BatchSolver solver;
+};
 
 struct scl_gpu_graph {
   int device = -1;
@@ -25,6 +31,17 @@ struct scl_gpu_graph {
   std::unique_ptr<Reordered> reo;
   // launch shapes chosen per (n_features, storage dtype): set_plan / autotune
   std::map<std::pair<int64_t, int>, SpmmPlan> plans;
+  // CSC view of P for the backward pass (structure built on first use)
+  std::unique_ptr<Adjoint> adj;
+  // bumped whenever the master values change; the adjoint view caches the
+  // version its values were gathered at
+  uint64_t values_version = 1;
+  uint64_t adj_version = 0;
+
+  void values_changed() {
+    ++values_version;
+    if (reo) reo->values_ok = false;
+  }
 
   const SpmmPlan* plan_for(int64_t F) const {
     auto it = plans.find({F, (int)store_type});
@@ -154,7 +171,7 @@ SCL_EXPORT scl_error_t scl_gpu_graph_normalize(scl_gpu_graph_t graph, int symmet
   normalize(g, symmetric != 0, degree_mode, graph->degrees.as<double>(), s);
   graph->symmetric = symmetric != 0;
   graph->normalized = true;
-  if (graph->reo) graph->reo->values_ok = false;
+  graph->values_changed();
   if (graph->store_type != g.vtype) {
     graph->store_vals = DevBuf(std::max<int64_t>(g.nnz, 1) * dtype_size(graph->store_type), s);
     convert_values(g.values.p, g.vtype, graph->store_vals.p, graph->store_type, g.nnz, s);
@@ -262,7 +279,11 @@ SCL_EXPORT scl_error_t scl_gpu_graph_set_plan(scl_gpu_graph_t graph, int64_t n_f
                     (kind == 2 && group == 32 && (stage == 8 || stage == 16)) ||
                     (kind == 3 && group == 32 && (stage == 16 || stage == 32) && bytes >= 4) ||
                     (kind == 4 && group == 32 && (stage == 8 || stage == 16 || stage == 32) &&
-                     n_features == 32 * vec && (bytes == 4 || bytes == 8 || bytes == 16)),
+                     n_features == 32 * vec && (bytes == 4 || bytes == 8 || bytes == 16)) ||
+                    ((kind == 5 || kind == 6) && dtype_size(graph->store_type) == 2 && bytes == 16 &&
+                     n_features == (int64_t)group * vec &&
+                     ((group == 8 && (stage == 2 || stage == 4 || stage == 8)) ||
+                      (group == 16 && (stage == 4 || stage == 8 || stage == 16)))),
                 SCL_ERROR_INVALID_ARGUMENT, "invalid kernel kind / stage for this shape");
     SpmmPlan p;
     p.group = group;
@@ -319,6 +340,214 @@ SCL_EXPORT scl_error_t scl_gpu_spmm(scl_gpu_graph_t graph, const void* X, void* 
     plan.stage = stage;
   }
   spmm_with_plan(a, plan, as_stream(stream));
+  SCL_API_RETURN_OK;
+  SCL_API_CATCH
+}
+
+SCL_EXPORT scl_error_t scl_gpu_graph_set_weights(scl_gpu_graph_t graph, const void* values, scl_dtype_t dtype,
+                                                 int on_device, void* stream) {
+  SCL_API_CHECK_NULL(graph, "Graph is null");
+  SCL_API_CHECK(graph->g.nnz == 0 || values != nullptr, SCL_ERROR_NULL_POINTER, "Value array pointer is null");
+  SCL_API_TRY
+  ensure_device(graph);
+  const DType t = checked_dtype(dtype);
+  SCL_REQUIRE(t == kF32 || t == kF64, SCL_ERROR_TYPE_MISMATCH, "weights must be f32 or f64");
+  cudaStream_t s = as_stream(stream);
+  DeviceCSR& g = graph->g;
+  if (g.nnz > 0) {
+    DevBuf tmp(g.nnz * dtype_size(t), s);
+    SCL_CUDA(cudaMemcpyAsync(tmp.p, values, g.nnz * dtype_size(t),
+                             on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, s));
+    convert_values(tmp.p, t, g.values.p, g.vtype, g.nnz, s);
+    if (!on_device) SCL_CUDA(cudaStreamSynchronize(s));
+  }
+  graph->normalized = false;
+  graph->weights.reset();
+  graph->degrees.reset();
+  graph->values_changed();
+  if (graph->store_type != g.vtype) {
+    graph->store_vals = DevBuf(std::max<int64_t>(g.nnz, 1) * dtype_size(graph->store_type), s);
+    convert_values(g.values.p, g.vtype, graph->store_vals.p, graph->store_type, g.nnz, s);
+  }
+  SCL_API_RETURN_OK;
+  SCL_API_CATCH
+}
+
+SCL_EXPORT scl_error_t scl_gpu_diffuse_checkpointed(scl_gpu_graph_t graph, const void* X0, void* Y,
+                                                    int64_t n_features, int64_t n_steps, int64_t every,
+                                                    void* checkpoints, void* stream) {
+  SCL_API_CHECK_NULL(graph, "Graph is null");
+  SCL_API_CHECK_NULL(X0, "Matrix X is null");
+  SCL_API_CHECK_NULL(Y, "Matrix Y is null");
+  SCL_API_CHECK(n_features > 0 && n_steps >= 0 && every >= 1, SCL_ERROR_INVALID_ARGUMENT,
+                "Dimensions must be positive");
+  SCL_API_CHECK(checkpoint_slots(n_steps, every) == 0 || checkpoints != nullptr, SCL_ERROR_NULL_POINTER,
+                "Checkpoint buffer is null");
+  SCL_API_TRY
+  ensure_device(graph);
+  SCL_REQUIRE(graph->store_type == graph->g.vtype, SCL_ERROR_TYPE_MISMATCH,
+              "checkpointed diffusion runs in the graph's f32/f64 values; reset the storage dtype first");
+  diffuse_checkpointed(graph->g.view(), X0, Y, graph->g.vtype, n_features, n_steps, every, checkpoints,
+                       as_stream(stream));
+  SCL_API_RETURN_OK;
+  SCL_API_CATCH
+}
+
+SCL_EXPORT scl_error_t scl_gpu_diffuse_backward(scl_gpu_graph_t graph, const void* X0, const void* checkpoints,
+                                                const void* dY, int64_t n_features, int64_t n_steps, int64_t every,
+                                                void* dX0, void* dW, void* stream) {
+  SCL_API_CHECK_NULL(graph, "Graph is null");
+  SCL_API_CHECK_NULL(X0, "Matrix X is null");
+  SCL_API_CHECK_NULL(dY, "Gradient dY is null");
+  SCL_API_CHECK_NULL(dX0, "Gradient output dX0 is null");
+  SCL_API_CHECK(n_features > 0 && n_steps >= 0 && every >= 1, SCL_ERROR_INVALID_ARGUMENT,
+                "Dimensions must be positive");
+  SCL_API_CHECK(checkpoint_slots(n_steps, every) == 0 || checkpoints != nullptr, SCL_ERROR_NULL_POINTER,
+                "Checkpoint buffer is null");
+  SCL_API_TRY
+  ensure_device(graph);
+  DeviceCSR& g = graph->g;
+  SCL_REQUIRE(graph->store_type == g.vtype, SCL_ERROR_TYPE_MISMATCH,
+              "the backward pass runs in the graph's f32/f64 values; reset the storage dtype first");
+  SCL_REQUIRE(g.n_rows == g.n_cols, SCL_ERROR_DIMENSION_MISMATCH, "the backward pass needs a square matrix");
+  cudaStream_t s = as_stream(stream);
+  if (!graph->adj) {
+    auto a = std::make_unique<Adjoint>();
+    build_adjoint(g, *a, s);
+    graph->adj = std::move(a);
+    graph->adj_version = 0;
+  }
+  if (graph->adj_version != graph->values_version || !graph->adj->values_ok) {
+    adjoint_values(g.values.p, g.vtype, *graph->adj, s);
+    graph->adj_version = graph->values_version;
+  }
+  const CsrView v = g.view();
+  DevBuf gPt;
+  if (dW != nullptr && n_steps > 0) gPt = DevBuf(std::max<int64_t>(g.nnz, 1) * dtype_size(g.vtype), s);
+  diffuse_backward(v, *graph->adj, X0, checkpoints, dY, g.vtype, n_features, n_steps, every, dX0, gPt.p, s);
+  if (dW != nullptr) {
+    if (n_steps <= 0 || g.nnz == 0) {
+      if (g.nnz > 0) SCL_CUDA(cudaMemsetAsync(dW, 0, g.nnz * dtype_size(g.vtype), s));
+    } else if (graph->normalized) {
+      normalize_backward(v, *graph->adj, gPt.p, graph->degrees.as<double>(), graph->symmetric, dW, s);
+    } else {
+      scatter_adjoint_entries(*graph->adj, gPt.p, g.vtype, dW, s);
+    }
+  }
+  SCL_API_RETURN_OK;
+  SCL_API_CATCH
+}
+
+SCL_EXPORT scl_error_t scl_gpu_batch_create(scl_gpu_batch_t* out, int64_t n_graphs, const scl_gpu_graph_t* graphs,
+                                            int64_t n_features, int64_t n_steps, void* stream) {
+  SCL_API_CHECK_NULL(out, "Output pointer is null");
+  SCL_API_CHECK_NULL(graphs, "Graph array is null");
+  SCL_API_CHECK(n_graphs > 0 && n_features > 0 && n_steps > 0, SCL_ERROR_INVALID_ARGUMENT,
+                "Dimensions must be positive");
+  SCL_API_TRY
+  cudaStream_t s = as_stream(stream);
+  std::vector<CsrView> views;
+  views.reserve(n_graphs);
+  for (int64_t b = 0; b < n_graphs; ++b) {
+    SCL_REQUIRE(graphs[b] != nullptr, SCL_ERROR_NULL_POINTER, "Graph is null");
+    ensure_device(graphs[b]);
+    SCL_REQUIRE(graphs[b]->store_type == kF32 && graphs[b]->g.vtype == kF32, SCL_ERROR_TYPE_MISMATCH,
+                "batched diffusion needs f32 graphs with f32 storage");
+    views.push_back(graphs[b]->g.view());
+  }
+  auto h = std::make_unique<scl_gpu_batch>();
+  h->device = current_device();
+  h->solver.init(views, n_features, n_steps, s);
+  *out = h.release();
+  SCL_API_RETURN_OK;
+  SCL_API_CATCH
+}
+
+SCL_EXPORT scl_error_t scl_gpu_batch_destroy(scl_gpu_batch_t* batch) {
+  if (batch == nullptr || *batch == nullptr) SCL_API_RETURN_OK;
+  SCL_API_TRY
+  delete *batch;
+  *batch = nullptr;
+  SCL_API_RETURN_OK;
+  SCL_API_CATCH
+}
+
+SCL_EXPORT scl_error_t scl_gpu_batch_layout(scl_gpu_batch_t batch, int64_t* row_offsets, int64_t* nnz_total,
+                                            int64_t* n_tiles) {
+  SCL_API_CHECK_NULL(batch, "Batch is null");
+  SCL_API_TRY
+  const auto& ro = batch->solver.row_offsets();
+  if (row_offsets) std::copy(ro.begin(), ro.end(), row_offsets);
+  if (nnz_total) *nnz_total = batch->solver.nnz_total();
+  if (n_tiles) *n_tiles = batch->solver.n_tiles();
+  SCL_API_RETURN_OK;
+  SCL_API_CATCH
+}
+
+SCL_EXPORT scl_error_t scl_gpu_batch_set_schedule(scl_gpu_batch_t batch, int64_t tile_nnz, int unroll,
+                                                  int blocks_per_sm, void* stream) {
+  SCL_API_CHECK_NULL(batch, "Batch is null");
+  SCL_API_TRY
+  SCL_REQUIRE(batch->device == current_device(), SCL_ERROR_INVALID_ARGUMENT,
+              "batch lives on another device than the current one");
+  batch->solver.set_schedule(tile_nnz, unroll, blocks_per_sm, as_stream(stream));
+  SCL_API_RETURN_OK;
+  SCL_API_CATCH
+}
+
+SCL_EXPORT scl_error_t scl_gpu_batch_autotune(scl_gpu_batch_t batch, const float* X0, float* Y, int reps,
+                                              void* stream) {
+  SCL_API_CHECK_NULL(batch, "Batch is null");
+  SCL_API_CHECK_NULL(X0, "Matrix X is null");
+  SCL_API_CHECK_NULL(Y, "Matrix Y is null");
+  SCL_API_TRY
+  SCL_REQUIRE(batch->device == current_device(), SCL_ERROR_INVALID_ARGUMENT,
+              "batch lives on another device than the current one");
+  SCL_REQUIRE(X0 != Y, SCL_ERROR_INVALID_ARGUMENT, "batched diffusion needs distinct input and output blocks");
+  batch->solver.autotune(X0, Y, std::max(1, reps), as_stream(stream));
+  SCL_API_RETURN_OK;
+  SCL_API_CATCH
+}
+
+SCL_EXPORT scl_error_t scl_gpu_batch_schedule(scl_gpu_batch_t batch, int64_t* tile_nnz, int* unroll, int* grid,
+                                              int* lanes_per_row, double* tuned_ms) {
+  SCL_API_CHECK_NULL(batch, "Batch is null");
+  const BatchSolver& b = batch->solver;
+  if (tile_nnz) *tile_nnz = b.tile_nnz();
+  if (unroll) *unroll = b.unroll();
+  if (grid) *grid = b.grid();
+  if (lanes_per_row) *lanes_per_row = b.group();
+  if (tuned_ms) *tuned_ms = b.tuned_ms();
+  SCL_API_RETURN_OK;
+}
+
+SCL_EXPORT scl_error_t scl_gpu_batch_solve(scl_gpu_batch_t batch, const float* X0, float* Y, void* stream) {
+  SCL_API_CHECK_NULL(batch, "Batch is null");
+  SCL_API_CHECK_NULL(X0, "Matrix X is null");
+  SCL_API_CHECK_NULL(Y, "Matrix Y is null");
+  SCL_API_TRY
+  SCL_REQUIRE(batch->device == current_device(), SCL_ERROR_INVALID_ARGUMENT,
+              "batch lives on another device than the current one");
+  batch->solver.solve(X0, Y, as_stream(stream));
+  SCL_API_RETURN_OK;
+  SCL_API_CATCH
+}
+
+SCL_EXPORT scl_error_t scl_gpu_batch_inject_stall(scl_gpu_batch_t batch, int graph) {
+  SCL_API_CHECK_NULL(batch, "Batch is null");
+  SCL_API_TRY
+  batch->solver.inject_stall(graph);
+  SCL_API_RETURN_OK;
+  SCL_API_CATCH
+}
+
+SCL_EXPORT scl_error_t scl_gpu_batch_status(scl_gpu_batch_t batch, int* code, int* item, void* stream) {
+  SCL_API_CHECK_NULL(batch, "Batch is null");
+  SCL_API_TRY
+  int32_t it = 0;
+  const int32_t c = batch->solver.status(as_stream(stream), &it);
+  if (code) *code = c;
+  if (item) *item = it;
   SCL_API_RETURN_OK;
   SCL_API_CATCH
 }

@@ -10,6 +10,7 @@
 #include <cstdint>
 #include <stdexcept>
 #include <string>
+#include <vector>
 
 #include <cuda_runtime.h>
 
@@ -219,5 +220,94 @@ void exclusive_scan_i64(const int64_t* in, int64_t* out, int64_t count, cudaStre
 // Transpose structure: for CSR g (n_rows x n_cols) build the CSR of g^T and the
 // map tmap[q] = position in g of the entry that lands at q in g^T.
 void transpose_map(const DeviceCSR& g, DeviceCSR& gt, DevBuf& tmap, cudaStream_t s);
+
+// ---- backward pass ----------------------------------------------------------------
+// CSC view of P (the CSR of P^T) for the adjoint: structure built once per
+// graph, values gathered from P's current values through tmap.
+struct Adjoint {
+  DeviceCSR t;    // P^T: indptr int64[n+1], indices int32[nnz], values vtype[nnz]
+  DevBuf tmap;    // int32[nnz]: entry q of P^T is entry tmap[q] of P
+  bool values_ok = false;
+};
+void build_adjoint(const DeviceCSR& g, Adjoint& a, cudaStream_t s);
+void adjoint_values(const void* vals, DType t, Adjoint& a, cudaStream_t s);
+
+// Checkpoint slots the forward fills: X_s for s = every, 2*every, ... < steps.
+int64_t checkpoint_slots(int64_t steps, int64_t every);
+// Y = P^steps X0 (f32 or f64, original row order), storing the checkpoints in
+// ckpt (checkpoint_slots(steps, every) blocks of n x F). X0 != Y.
+void diffuse_checkpointed(const CsrView& g, const void* X0, void* Y, DType t, int64_t F, int64_t steps,
+                          int64_t every, void* ckpt, cudaStream_t s);
+// Given dY = dL/dX_T: dX0 = dL/dX_0 and, when gPt is non-null, the SDDMM
+// gradient dL/dP accumulated in P^T's (CSC) entry order.
+void diffuse_backward(const CsrView& g, const Adjoint& adj, const void* X0, const void* ckpt, const void* dY,
+                      DType t, int64_t F, int64_t steps, int64_t every, void* dX0, void* gPt, cudaStream_t s);
+// dW (CSR order of P) from dL/dP in CSC order, through the row or symmetric
+// normalisation with the FP64 degrees kept by normalize().
+void normalize_backward(const CsrView& P, const Adjoint& adj, const void* gPt, const double* degrees, int symmetric,
+                        void* dW, cudaStream_t s);
+// dL/dP in CSR order from its CSC-order accumulator.
+void scatter_adjoint_entries(const Adjoint& adj, const void* gPt, DType t, void* gP, cudaStream_t s);
+
+}  // namespace sclgpu
+
+namespace sclgpu {
+
+// ---- batched diffusion -------------------------------------------------------------
+// Many independent f32 graphs, all diffusion steps in one persistent kernel
+// launch replayed from a CUDA graph (batch.cu). The graphs' structure and
+// values are copied into one block-diagonal CSR at init.
+class BatchSolver {
+ public:
+  BatchSolver() = default;
+  BatchSolver(const BatchSolver&) = delete;
+  BatchSolver& operator=(const BatchSolver&) = delete;
+  ~BatchSolver();
+
+  void init(const std::vector<CsrView>& graphs, int64_t F, int64_t steps, cudaStream_t s);
+  // tile_nnz: stored entries per tile; unroll: gathers in flight (4 or 8);
+  // blocks_per_sm: resident CTAs per SM (0 = occupancy limit)
+  void set_schedule(int64_t tile_nnz, int unroll, int blocks_per_sm, cudaStream_t s);
+  // times every candidate schedule on (X0, Y) and keeps the fastest
+  void autotune(const float* X0, float* Y, int reps, cudaStream_t s);
+  // Y = P_b^steps X0_b for every graph b, one CUDA-graph launch (asynchronous)
+  void solve(const float* X0, float* Y, cudaStream_t s);
+  // plain launch of the same kernel (no graph), for timing candidates
+  void launch_direct(const float* X0, float* Y, cudaStream_t s);
+  // syncs s; returns the kernel's status word (0 ok) and clears it
+  int32_t status(cudaStream_t s, int32_t* item);
+  // test hook: graph `graph`'s waits can never complete (-1 = off), so they run
+  // into their time limit and report an error
+  void inject_stall(int graph);
+
+  int64_t n_graphs() const { return n_graphs_; }
+  int64_t n_total() const { return n_total_; }
+  int64_t nnz_total() const { return nnz_total_; }
+  int64_t n_tiles() const { return n_tiles_; }
+  int64_t tile_nnz() const { return tile_nnz_; }
+  int unroll() const { return unroll_; }
+  int grid() const { return grid_; }
+  int group() const { return group_; }
+  int vec() const { return vec_; }
+  double tuned_ms() const { return tuned_ms_; }
+  const std::vector<int64_t>& row_offsets() const { return row_off_; }
+
+ private:
+  void build_tiles(int64_t tile_nnz, cudaStream_t s);
+  void invalidate_graph();
+  void* params_for(const float* X0, float* Y, void* storage) const;
+  double time_solve(const float* X0, float* Y, int reps, cudaStream_t s);
+
+  int64_t F_ = 0, steps_ = 0, n_graphs_ = 0, n_total_ = 0, nnz_total_ = 0, n_tiles_ = 0, tile_nnz_ = 0;
+  int unroll_ = 8, grid_ = 1, group_ = 1, vec_ = 1, blocks_per_sm_ = 0, stall_graph_ = -1;
+  double tuned_ms_ = 0.0;
+  std::vector<int64_t> row_off_, nnz_off_, h_indptr_;
+  DevBuf indptr_, indices_, values_, tiles_, tile_graph_, graph_tiles_, counters_, status_, scratch_;
+  cudaGraph_t graph_ = nullptr;
+  cudaGraphExec_t exec_ = nullptr;
+  cudaGraphNode_t knode_ = nullptr;
+  const float* cap_x0_ = nullptr;
+  float* cap_y_ = nullptr;
+};
 
 }  // namespace sclgpu

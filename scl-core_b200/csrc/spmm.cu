@@ -677,6 +677,156 @@ k_spmm_row(const int64_t* __restrict__ indptr, const int32_t* __restrict__ indic
   }
 }
 
+// ---- split-chain warp-per-row kernel (16-bit storage) --------------------------------
+// One warp per row as in k_spmm_row, but every lane loads 16 bytes: a row of
+// ROWB bytes takes L = ROWB/16 lanes, so one 128-bit load instruction of the
+// warp gathers Q = 32/L entries at once — quarter q of the warp (lanes
+// [qL, qL+L)) takes entries q, q+Q, q+2Q, ... of the row and keeps its own
+// sequential fma chain over them. At the row end the Q chains are summed
+// pairwise by shuffles over the lane bits L, 2L, ... (Q=2: c0+c1; Q=4:
+// (c0+c1)+(c2+c3)), the order the oracle's chain restatement uses. Pairs are
+// staged 32 at a time in a per-warp shared-memory double buffer, the next
+// chunk (or the next row's first chunk) and the next row's bounds are fetched
+// one step ahead, exactly as in k_spmm_row. MIXED forms the products with
+// fma.rn.f32.{bf16,f16} straight from the stored operands (exact product, one
+// rounding: the bits of widening both to f32 first).
+template <class T>
+__device__ __forceinline__ float fma_mixed(unsigned short a, unsigned short b, float c);
+template <>
+__device__ __forceinline__ float fma_mixed<__nv_bfloat16>(unsigned short a, unsigned short b, float c) {
+  asm("fma.rn.f32.bf16 %0, %1, %2, %0;" : "+f"(c) : "h"(a), "h"(b));
+  return c;
+}
+template <>
+__device__ __forceinline__ float fma_mixed<__half>(unsigned short a, unsigned short b, float c) {
+  asm("fma.rn.f32.f16 %0, %1, %2, %0;" : "+f"(c) : "h"(a), "h"(b));
+  return c;
+}
+
+template <class VT, class XT, class YT, int ROWB, int U, bool MIXED>
+__global__ void __launch_bounds__(kSpmmThreads, (U <= 2) ? 4 : ((U <= 8) ? 3 : 2))
+k_spmm_split(const int64_t* __restrict__ indptr, const int32_t* __restrict__ indices, const VT* __restrict__ values,
+             const XT* __restrict__ X, YT* __restrict__ Y, const int32_t* __restrict__ row_map, int64_t n_rows) {
+  static_assert(sizeof(XT) == 2 && sizeof(VT) == 2, "the split-chain kernel is for 16-bit storage");
+  constexpr int L = ROWB / 16;        // lanes per gathered row
+  constexpr int Q = 32 / L;           // entries per load instruction (chains)
+  constexpr int VEC = 8;              // 16-bit elements per lane
+  constexpr int WARPS = kSpmmThreads / 32;
+  constexpr int STEP = U * Q;         // entries per batch
+  static_assert(L == 8 || L == 16, "row pitch must be 128 or 256 bytes");
+  static_assert(32 % STEP == 0, "a chunk of 32 entries holds whole batches");
+  __shared__ __align__(16) int32_t s_j[WARPS][2][32];
+  __shared__ __align__(16) unsigned short s_v[WARPS][2][32];
+  const int lane = threadIdx.x & 31;
+  const int w = threadIdx.x >> 5;
+  const int q = lane / L;             // chain of this lane
+  const int lq = lane & (L - 1);      // 16-byte chunk of the row
+  const int64_t nw = ((int64_t)gridDim.x * kSpmmThreads) >> 5;
+  int64_t row = ((int64_t)blockIdx.x * kSpmmThreads + threadIdx.x) >> 5;
+  if (row >= n_rows) return;
+  const char* __restrict__ Xb = reinterpret_cast<const char*>(X) + lq * 16;
+  int64_t s_cur = indptr[row], e_cur = indptr[row + 1];
+  int64_t s_nx = 0, e_nx = 0;
+  if (row + nw < n_rows) {
+    s_nx = indptr[row + nw];
+    e_nx = indptr[row + nw + 1];
+  }
+  auto fetch = [&](int64_t pos, int64_t end, int32_t& j, unsigned short& v) {
+    j = 0;
+    v = 0;
+    if (pos < end) {
+      j = __ldcs(indices + pos);
+      v = __ldcs(reinterpret_cast<const unsigned short*>(values) + pos);
+    }
+  };
+  int buf = 0;
+  {
+    int32_t j;
+    unsigned short v;
+    fetch(s_cur + lane, e_cur, j, v);
+    s_j[w][0][lane] = j;
+    s_v[w][0][lane] = v;
+    __syncwarp();
+  }
+  for (; row < n_rows; row += nw) {
+    const int64_t nn = row + 2 * nw;
+    int64_t s_nn = 0, e_nn = 0;
+    if (nn < n_rows) {
+      s_nn = indptr[nn];
+      e_nn = indptr[nn + 1];
+    }
+    float acc[VEC];
+#pragma unroll
+    for (int i = 0; i < VEC; ++i) acc[i] = 0.0f;
+    const int len = (int)(e_cur - s_cur);
+    for (int base = 0; base < len; base += 32) {
+      int32_t j_n;
+      unsigned short v_n;
+      if (base + 32 < len) fetch(s_cur + base + 32 + lane, e_cur, j_n, v_n);
+      else fetch(s_nx + lane, e_nx, j_n, v_n);
+      const int cnt = (len - base) < 32 ? (len - base) : 32;
+      const int32_t* __restrict__ jb = s_j[w][buf];
+      const unsigned short* __restrict__ vb = s_v[w][buf];
+#pragma unroll
+      for (int t = 0; t < 32; t += STEP) {
+        if (t >= cnt) break;
+        uint4 xr[U];
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+          const int e = t + u * Q + q;
+          if (e < cnt) {
+            const int32_t j = jb[e];
+            xr[u] = __ldg(reinterpret_cast<const uint4*>(Xb + (size_t)(uint32_t)j * ROWB));
+          }
+        }
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+          const int e = t + u * Q + q;
+          if (e < cnt) {
+            const unsigned short vbits = vb[e];
+            const unsigned short* ex = reinterpret_cast<const unsigned short*>(&xr[u]);
+            if constexpr (MIXED) {
+#pragma unroll
+              for (int i = 0; i < VEC; ++i) acc[i] = fma_mixed<XT>(vbits, ex[i], acc[i]);
+            } else {
+              const float vf = tof<VT>(*reinterpret_cast<const VT*>(&vbits));
+#pragma unroll
+              for (int i = 0; i < VEC; ++i)
+                acc[i] = __fmaf_rn(vf, tof<XT>(*reinterpret_cast<const XT*>(&ex[i])), acc[i]);
+            }
+          }
+        }
+      }
+      s_j[w][buf ^ 1][lane] = j_n;
+      s_v[w][buf ^ 1][lane] = v_n;
+      __syncwarp();
+      buf ^= 1;
+    }
+    if (len == 0) {
+      int32_t j;
+      unsigned short v;
+      fetch(s_nx + lane, e_nx, j, v);
+      s_j[w][buf][lane] = j;
+      s_v[w][buf][lane] = v;
+      __syncwarp();
+    }
+    // sum the Q chains: lane bits L, 2L, ... from the lowest
+#pragma unroll
+    for (int o = L; o < 32; o <<= 1) {
+#pragma unroll
+      for (int i = 0; i < VEC; ++i) acc[i] = acc[i] + __shfl_xor_sync(0xffffffffu, acc[i], o);
+    }
+    if (q == 0) {
+      const int64_t orow = row_map ? (int64_t)row_map[row] : row;
+      VecStore<YT, VEC>::store(Y + orow * (ROWB / 2) + lq * VEC, acc);
+    }
+    s_cur = s_nx;
+    e_cur = e_nx;
+    s_nx = s_nn;
+    e_nx = e_nn;
+  }
+}
+
 // Persistent grid size: resident blocks per SM (from the occupancy
 // calculator) times the SM count, capped by the blocks the rows need.
 template <class K>
@@ -810,6 +960,34 @@ void launch_row(const SpmmArgs& a, int U, cudaStream_t s) {
   throw Error(kErrInvalidArgument, "the fixed-pitch SpMM needs 128-, 256- or 512-byte rows");
 }
 
+// kinds 5/6: split-chain kernel for 16-bit storage (6 = mixed-precision fma);
+// stage = gathers per lane per batch (U * chains must divide 32)
+template <class VT, class XT, class YT, int ROWB, int U, bool MIXED>
+void launch_split_ru(const SpmmArgs& a, cudaStream_t s) {
+  auto kern = k_spmm_split<VT, XT, YT, ROWB, U, MIXED>;
+  const dim3 grid(persistent_blocks(kern, 0, a.n_rows, 32));
+  kern<<<grid, kSpmmThreads, 0, s>>>(a.indptr, a.indices, static_cast<const VT*>(a.values),
+                                     static_cast<const XT*>(a.X), static_cast<YT*>(a.Y), a.row_map, a.n_rows);
+  SCL_CUDA(cudaGetLastError());
+}
+
+template <class VT, class XT, class YT, bool MIXED>
+void launch_split(const SpmmArgs& a, int U, cudaStream_t s) {
+  const int64_t rowb = a.F * (int64_t)sizeof(XT);
+  if (rowb == 128) {  // 4 chains: U in {2, 4, 8}
+    if (U == 2) return launch_split_ru<VT, XT, YT, 128, 2, MIXED>(a, s);
+    if (U == 4) return launch_split_ru<VT, XT, YT, 128, 4, MIXED>(a, s);
+    if (U == 8) return launch_split_ru<VT, XT, YT, 128, 8, MIXED>(a, s);
+  } else if (rowb == 256) {  // 2 chains: U in {4, 8, 16}
+    if (U == 4) return launch_split_ru<VT, XT, YT, 256, 4, MIXED>(a, s);
+    if (U == 8) return launch_split_ru<VT, XT, YT, 256, 8, MIXED>(a, s);
+    if (U == 16) return launch_split_ru<VT, XT, YT, 256, 16, MIXED>(a, s);
+  } else {
+    throw Error(kErrInvalidArgument, "the split-chain SpMM needs 128- or 256-byte rows");
+  }
+  throw Error(kErrInvalidArgument, "split-chain SpMM batch must be 2/4/8 (128-byte rows) or 4/8/16 (256-byte rows)");
+}
+
 // kind 2: register stream (stage = U in {8, 16}); kind 3: cp.async stream
 // pipeline (stage = entries per stage in {16, 32}).
 template <class VT, class XT, class YT, class AT, int VEC>
@@ -849,6 +1027,15 @@ void launch_typed(const SpmmArgs& a, const SpmmPlan& plan, cudaStream_t s) {
                 kErrInvalidArgument, "the fixed-pitch SpMM covers a row with one chunk per lane of a warp");
     return launch_row<VT, XT, YT, AT>(a, plan.stage, s);
   }
+  if (plan.kind == 5 || plan.kind == 6) {
+    SCL_REQUIRE(plan.vec == kVec && (int64_t)plan.group * kVec == a.F, kErrInvalidArgument,
+                "the split-chain SpMM covers a row with one 16-byte chunk per lane of a group");
+    if constexpr (sizeof(XT) == 2 && sizeof(VT) == 2 && sizeof(AT) == 4) {
+      if (plan.kind == 6) return launch_split<VT, XT, YT, true>(a, plan.stage, s);
+      return launch_split<VT, XT, YT, false>(a, plan.stage, s);
+    }
+    throw Error(kErrInvalidArgument, "the split-chain SpMM is for bf16 or f16 storage");
+  }
   if (plan.kind == 2 || plan.kind == 3) {
     SCL_REQUIRE(plan.group == 32, kErrInvalidArgument, "the stream SpMM uses a whole warp per row block");
     const int k = plan.kind, st = plan.stage;
@@ -887,6 +1074,16 @@ SpmmPlan default_spmm_plan(int64_t F, DType xtype, const void* X, const void* Y,
   // Rows of 128, 256 or 512 bytes: one warp per row, one 4/8/16-byte chunk per
   // lane — no divergence between rows sharing a warp, one load per entry.
   const int64_t rb = F * xs;
+  if (xs == 2 && (rb == 128 || rb == 256) && (reinterpret_cast<uintptr_t>(X) & 15u) == 0 &&
+      (reinterpret_cast<uintptr_t>(Y) % (uintptr_t)(8 * ys)) == 0) {
+    // 16-bit storage: one 16-byte chunk per lane, 4 (128-byte rows) or 2
+    // (256-byte rows) entries per load instruction, mixed-precision fma
+    p.group = (int)(rb / 16);
+    p.vec = 8;
+    p.kind = 6;
+    p.stage = (rb == 128) ? 4 : 8;
+    return p;
+  }
   if (rb == 128 || rb == 256 || rb == 512) {
     const int lane_bytes = (int)(rb / 32);
     const int v = lane_bytes / xs;
@@ -920,8 +1117,8 @@ void spmm_with_plan(const SpmmArgs& a, const SpmmPlan& plan, cudaStream_t s) {
   if (a.n_rows <= 0 || a.F <= 0) return;
   SCL_REQUIRE(plan.group >= 1 && plan.group <= 32 && (plan.group & (plan.group - 1)) == 0, kErrInvalidArgument,
               "lane-group size must be a power of two in [1, 32]");
-  SCL_REQUIRE(plan.kind == 0 || plan.kind == 2 || plan.kind == 3 || plan.kind == 4 ||
-                  (plan.kind == 1 && plan.vec > 1 && plan.group >= 4),
+  SCL_REQUIRE(plan.kind == 0 || plan.kind == 2 || plan.kind == 3 || plan.kind == 4 || plan.kind == 5 ||
+                  plan.kind == 6 || (plan.kind == 1 && plan.vec > 1 && plan.group >= 4),
               kErrInvalidArgument, "the pipelined SpMM needs 16-byte lane chunks and a lane group of at least 4");
   if (plan.vec > 1) {
     const int xs = (int)dtype_size(a.xtype), ys = (int)dtype_size(a.ytype);

@@ -165,6 +165,53 @@ class GpuGraph:
                                               F, int(n_steps), _stream_ptr(stream)), "diffuse", self._lib)
         return out
 
+    def set_weights(self, values, stream=None) -> "GpuGraph":
+        """Replace the pre-normalisation weights (nnz entries in CSR order; host
+        NumPy array or CUDA tensor, f32/f64). The graph is un-normalised after."""
+        if isinstance(values, np.ndarray):
+            values = np.ascontiguousarray(values)
+            code = F32 if values.dtype == np.float32 else F64
+            rc = self._lib.scl_gpu_graph_set_weights(self._h, ctypes.c_void_p(values.ctypes.data), code, 0,
+                                                     _stream_ptr(stream))
+        else:
+            values = values.contiguous()
+            rc = self._lib.scl_gpu_graph_set_weights(self._h, _ptr(values), dtype_code(values.dtype), 1,
+                                                     _stream_ptr(stream))
+        check_error(rc, "set_weights", self._lib)
+        return self
+
+    @staticmethod
+    def checkpoint_slots(n_steps: int, every: int) -> int:
+        return (n_steps - 1) // every if (n_steps > 0 and every >= 1) else 0
+
+    def diffuse_checkpointed(self, X0, n_steps: int, every: int, out=None, checkpoints=None, stream=None):
+        """(Y, checkpoints): Y = P^n_steps X0 keeping X_every, X_2every, ... for diffuse_backward."""
+        torch = _torch()
+        X0 = X0.contiguous()
+        n, F = X0.shape
+        Y = out if out is not None else torch.empty_like(X0)
+        k = self.checkpoint_slots(n_steps, every)
+        if checkpoints is None:
+            checkpoints = torch.empty((max(k, 0), n, F), dtype=X0.dtype, device=X0.device)
+        cp = _ptr(checkpoints) if k > 0 else ctypes.c_void_p(0)
+        check_error(self._lib.scl_gpu_diffuse_checkpointed(self._h, _ptr(X0), _ptr(Y), F, int(n_steps), int(every), cp,
+                                                           _stream_ptr(stream)), "diffuse_checkpointed", self._lib)
+        return Y, checkpoints
+
+    def diffuse_backward(self, X0, checkpoints, dY, n_steps: int, every: int, need_dW: bool = True, stream=None):
+        """(dX0, dW or None) for the diffusion run by diffuse_checkpointed."""
+        torch = _torch()
+        X0, dY = X0.contiguous(), dY.contiguous()
+        n, F = X0.shape
+        dX0 = torch.empty_like(X0)
+        dW = torch.empty(self.shape[2], dtype=X0.dtype, device=X0.device) if need_dW else None
+        k = self.checkpoint_slots(n_steps, every)
+        cp = _ptr(checkpoints) if k > 0 else ctypes.c_void_p(0)
+        check_error(self._lib.scl_gpu_diffuse_backward(self._h, _ptr(X0), cp, _ptr(dY), F, int(n_steps), int(every),
+                                                       _ptr(dX0), _ptr(dW) if dW is not None else ctypes.c_void_p(0),
+                                                       _stream_ptr(stream)), "diffuse_backward", self._lib)
+        return dX0, dW
+
     def spmm(self, X, out, group: int = 0, vec: int = 1, kind: int = 0, stage: int = 8, stream=None):
         """One Y = P X in the original row order with an explicit launch shape (group <= 0: default)."""
         F = X.shape[1]
@@ -176,6 +223,87 @@ class GpuGraph:
     def close(self):
         if self._h is not None and self._h.value:
             self._lib.scl_gpu_graph_destroy(ctypes.byref(self._h))
+        self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class GpuBatch:
+    """Many independent graphs diffused together in one persistent, CUDA-graph
+    replayed launch (scl_gpu_batch_*). Blocks are the graphs' n_b x F blocks
+    stacked row-wise; `row_offsets[b]` is graph b's first row."""
+
+    def __init__(self, graphs, n_features: int, n_steps: int, stream=None):
+        if not graphs:
+            raise ValueError("a batch needs at least one graph")
+        self._lib = graphs[0].lib
+        self._graphs = list(graphs)  # keep the handles alive (the batch holds copies, not references)
+        arr = (ctypes.c_void_p * len(graphs))(*[g.handle.value for g in graphs])
+        h = ctypes.c_void_p()
+        check_error(self._lib.scl_gpu_batch_create(ctypes.byref(h), len(graphs), ctypes.cast(arr, ctypes.c_void_p),
+                                                   int(n_features), int(n_steps), _stream_ptr(stream)),
+                    "batch_create", self._lib)
+        self._h = h
+        self.n_features, self.n_steps = int(n_features), int(n_steps)
+        offs = np.empty(len(graphs) + 1, np.int64)
+        nnz, tiles = ctypes.c_int64(), ctypes.c_int64()
+        check_error(self._lib.scl_gpu_batch_layout(self._h, ctypes.c_void_p(offs.ctypes.data), ctypes.byref(nnz),
+                                                   ctypes.byref(tiles)), "batch_layout", self._lib)
+        self.row_offsets = offs
+        self.nnz_total = nnz.value
+
+    @property
+    def n_rows(self) -> int:
+        return int(self.row_offsets[-1])
+
+    def schedule(self) -> dict:
+        t, u, gr, lpr, ms = ctypes.c_int64(), ctypes.c_int(), ctypes.c_int(), ctypes.c_int(), ctypes.c_double()
+        check_error(self._lib.scl_gpu_batch_schedule(self._h, ctypes.byref(t), ctypes.byref(u), ctypes.byref(gr),
+                                                     ctypes.byref(lpr), ctypes.byref(ms)), "batch_schedule", self._lib)
+        offs = np.empty(len(self._graphs) + 1, np.int64)
+        tiles = ctypes.c_int64()
+        check_error(self._lib.scl_gpu_batch_layout(self._h, ctypes.c_void_p(offs.ctypes.data), None,
+                                                   ctypes.byref(tiles)), "batch_layout", self._lib)
+        return {"tile_nnz": t.value, "unroll": u.value, "grid": gr.value, "lanes_per_row": lpr.value,
+                "tuned_ms": ms.value, "tiles_per_step": tiles.value}
+
+    def set_schedule(self, tile_nnz: int, unroll: int = 8, blocks_per_sm: int = 0, stream=None) -> "GpuBatch":
+        check_error(self._lib.scl_gpu_batch_set_schedule(self._h, int(tile_nnz), int(unroll), int(blocks_per_sm),
+                                                         _stream_ptr(stream)), "batch_set_schedule", self._lib)
+        return self
+
+    def autotune(self, X0, Y, reps: int = 3, stream=None) -> dict:
+        check_error(self._lib.scl_gpu_batch_autotune(self._h, _ptr(X0), _ptr(Y), int(reps), _stream_ptr(stream)),
+                    "batch_autotune", self._lib)
+        return self.schedule()
+
+    def solve(self, X0, out=None, stream=None):
+        torch = _torch()
+        X0 = X0.contiguous()
+        Y = out if out is not None else torch.empty_like(X0)
+        check_error(self._lib.scl_gpu_batch_solve(self._h, _ptr(X0), _ptr(Y), _stream_ptr(stream)), "batch_solve",
+                    self._lib)
+        return Y
+
+    def status(self, stream=None):
+        """(code, item): synchronises the stream; 0 = every wait completed."""
+        c, i = ctypes.c_int(), ctypes.c_int()
+        check_error(self._lib.scl_gpu_batch_status(self._h, ctypes.byref(c), ctypes.byref(i), _stream_ptr(stream)),
+                    "batch_status", self._lib)
+        return c.value, i.value
+
+    def inject_stall(self, graph: int) -> "GpuBatch":
+        """Failure-path test hook: graph `graph`'s waits never complete (-1 = off)."""
+        check_error(self._lib.scl_gpu_batch_inject_stall(self._h, int(graph)), "batch_inject_stall", self._lib)
+        return self
+
+    def close(self):
+        if self._h is not None and self._h.value:
+            self._lib.scl_gpu_batch_destroy(ctypes.byref(self._h))
         self._h = None
 
     def __del__(self):

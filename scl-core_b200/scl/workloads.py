@@ -24,6 +24,7 @@ def build_graph(n_cells: int, k: int, device="cuda", seed: int = 0, reorder: boo
     pts = synthetic.mixture(n_cells, seed=seed)
     ki, kd = synthetic.knn_device(pts, k, device=device, block=2048)
     torch.cuda.synchronize()
+    torch.cuda.empty_cache()  # the kNN blocks' distance tiles (GBs) are not needed any more
     t_knn = time.time() - t0
     s = stream if stream is not None else torch.cuda.current_stream()
     e0, e1, e2 = (torch.cuda.Event(enable_timing=True) for _ in range(3))

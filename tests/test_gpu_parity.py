@@ -262,10 +262,16 @@ def test_low_precision_storage_bit_exact(graph_3k, kind):
     g.set_storage(tdt)
     X0 = np.random.default_rng(9).standard_normal((n, 64)).astype(np.float32)
     Xd = torch.from_numpy(X0).cuda()
+    # 64 16-bit columns = 128-byte rows: the split-chain kernel with 4 interleaved chains
     for final_f32 in (True, False):
         Y = g.diffuse(Xd, 4, out_dtype=torch.float32 if final_f32 else tdt).float().cpu().numpy()
-        Yo = port.diffuse_lowp(ip, ind, P, X0, 4, port.BF16 if kind == "bf16" else port.F16, final_f32)
+        Yo = port.diffuse_lowp_chains(ip, ind, P, X0, 4, port.BF16 if kind == "bf16" else port.F16, 4, final_f32)
         np.testing.assert_array_equal(bits(Y), bits(Yo))
+    # a width the sequential kernels handle (48 columns = 96-byte rows)
+    X1 = np.random.default_rng(10).standard_normal((n, 48)).astype(np.float32)
+    Y1 = g.diffuse(torch.from_numpy(X1).cuda(), 3, out_dtype=torch.float32).cpu().numpy()
+    Yo1 = port.diffuse_lowp(ip, ind, P, X1, 3, port.BF16 if kind == "bf16" else port.F16, True)
+    np.testing.assert_array_equal(bits(Y1), bits(Yo1))
 
 
 @pytest.mark.parametrize("group", [1, 2, 4, 8, 16, 32])
@@ -365,3 +371,37 @@ def test_reordered_drop_in_is_bit_identical():
         scl.diffusion.detach(m)
         np.testing.assert_array_equal(bits(X), bits(want))
     scl.diffusion.set_reorder(m, -1)
+
+
+# ---- split-chain kernel (16-bit storage, 16-byte lanes) ------------------------------
+@pytest.mark.parametrize("storage,F", [("bf16", 64), ("bf16", 128), ("f16", 64), ("f16", 128)])
+def test_split_chain_shapes_are_exact(graph_3k, storage, F):
+    """Every split-chain launch shape (one 16-byte chunk per lane, 32/group
+    entries per load feeding as many interleaved fma chains; batches of gathers;
+    plain or mixed-precision fma) gives the bits of the oracle's chain
+    restatement."""
+    import torch
+
+    _, _, ip, ind, W = graph_3k
+    n = ip.size - 1
+    P = port.transition(ip, ind, W.astype(np.float32), False, True)
+    g = scl.gpu.GpuGraph.from_csr(ip, ind.astype(np.int32), P, (n, n))
+    tdt = torch.bfloat16 if storage == "bf16" else torch.float16
+    kind_code = port.BF16 if storage == "bf16" else port.F16
+    try:
+        g.set_storage(tdt)
+        X0 = np.random.default_rng(F).standard_normal((n, F)).astype(np.float32)
+        Xd = torch.from_numpy(X0).cuda().to(tdt)
+        group = F * 2 // 16
+        chains = 32 // group
+        ref1 = port.diffuse_lowp_chains(ip, ind, P, Xd.float().cpu().numpy(), 1, kind_code, chains, True)
+        stages = (2, 4, 8) if group == 8 else (4, 8, 16)
+        for kind in (5, 6):
+            for stage in stages:
+                Y = torch.empty((n, F), dtype=torch.float32, device="cuda")
+                g.spmm(Xd, Y, group=group, vec=8, kind=kind, stage=stage)
+                np.testing.assert_array_equal(bits(Y.cpu().numpy()), bits(ref1))
+        Yd = g.diffuse(Xd, 3, out_dtype=torch.float32).cpu().numpy()
+        np.testing.assert_array_equal(bits(Yd), bits(port.diffuse_lowp_chains(ip, ind, P, X0, 3, kind_code, chains)))
+    finally:
+        g.close()

@@ -156,6 +156,118 @@ def cpu_reference_diffusion(ip, ind, P, n, F, target_s=12.0, max_steps=N_STEPS):
     return gbs, steps, dt, cores, R.path.name
 
 
+def profiled_traffic(name):
+    """DRAM bytes per launch recorded from an ncu capture in profiles/<name>.md
+    (`dram_bytes_per_launch: N`), or None."""
+    p = ROOT / "profiles" / f"{name}.md"
+    if not p.exists():
+        return None
+    for line in p.read_text().splitlines():
+        if line.startswith("dram_bytes_per_launch:"):
+            return int(line.split(":", 1)[1])
+    return None
+
+
+def event_ms(torch, fn, stream, reps, warmup, flush_buf=None):
+    """Median CUDA-event time of fn() on `stream` (L2 flushed before each rep when flush_buf is given)."""
+    for _ in range(warmup):
+        fn()
+    torch.cuda.synchronize()
+    ts = []
+    for _ in range(reps):
+        if flush_buf is not None:
+            flush_l2(torch, flush_buf)
+        a = torch.cuda.Event(enable_timing=True)
+        b = torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        fn()
+        b.record(stream)
+        b.synchronize()
+        ts.append(a.elapsed_time(b))
+    return float(np.median(ts))
+
+
+def bench_backward(torch, scl, device, stream, reps, warmup, flush):
+    """Differentiation form: 200,000 cells, k=30, X0 200,000 x 32 FP32, 8 steps,
+    L = sum((X_8 - Y)^2), checkpoint every 4. Forward = the checkpointed
+    diffusion; forward+backward adds the loss gradient and the backward pass
+    (dL/dX0 and dL/dW through the row normalisation)."""
+    import scl.autograd  # noqa: F401
+
+    n, k, F, T, every = 200_000, 30, 32, 8, 4
+    pts = scl.synthetic.mixture(n, seed=0)
+    ki, kd = scl.synthetic.knn_device(pts, k, device=device, block=4096)
+    torch.cuda.synchronize()
+    torch.cuda.empty_cache()
+    g = scl.gpu.GpuGraph.from_knn(ki, kd, stream=stream)
+    g.normalize(symmetric=False, stream=stream)
+    del ki, kd
+    gen = torch.Generator(device=device).manual_seed(7)
+    X0 = torch.randn((n, F), device=device, generator=gen)
+    Yt = torch.randn((n, F), device=device, generator=gen)
+    ck = torch.empty((g.checkpoint_slots(T, every), n, F), device=device)
+    XT = torch.empty_like(X0)
+
+    def fwd():
+        g.diffuse_checkpointed(X0, T, every, out=XT, checkpoints=ck, stream=stream)
+
+    def fwd_bwd():
+        g.diffuse_checkpointed(X0, T, every, out=XT, checkpoints=ck, stream=stream)
+        dY = 2.0 * (XT - Yt)
+        g.diffuse_backward(X0, ck, dY, T, every, need_dW=True, stream=stream)
+
+    t_f = event_ms(torch, fwd, stream, reps, warmup, flush)
+    t_fb = event_ms(torch, fwd_bwd, stream, reps, warmup, flush)
+    nnz = g.shape[2]
+    g.close()
+    return {"workload": "200k cells k=30 32 cols 8 steps, checkpoint every 4, L=sum((X_8-Y)^2), dL/dX0 + dL/dW",
+            "cells": n, "nnz": nnz, "fwd_ms": round(t_f, 4), "fwd_bwd_ms": round(t_fb, 4),
+            "fwd_bwd_over_fwd": round(t_fb / t_f, 3)}
+
+
+def bench_batched(torch, scl, device, stream, reps, warmup):
+    """Batched form: 64 graphs, cell counts log-uniform in [2,000, 100,000]
+    (seed 0), each its own 10-component mixture, k=15, row-normalised FP32,
+    16-column blocks, 8 steps: one persistent CUDA-graph launch (autotuned
+    schedule) against 64 sequential scl_gpu_diffuse calls."""
+    rng = np.random.default_rng(0)
+    sizes = np.exp(rng.uniform(np.log(2000), np.log(100_000), 64)).astype(int)
+    graphs = []
+    for b, n in enumerate(sizes):
+        pts = scl.synthetic.mixture(int(n), seed=100 + b)
+        ki, kd = scl.synthetic.knn_device(pts, 15, device=device, block=8192)
+        g = scl.gpu.GpuGraph.from_knn(ki, kd, stream=stream)
+        g.normalize(symmetric=False, stream=stream)
+        graphs.append(g)
+    torch.cuda.synchronize()
+    torch.cuda.empty_cache()
+    F, T = 16, 8
+    batch = scl.gpu.GpuBatch(graphs, F, T, stream=stream)
+    X0 = torch.randn((batch.n_rows, F), device=device, generator=torch.Generator(device=device).manual_seed(3))
+    Y = torch.empty_like(X0)
+    sched = batch.autotune(X0, Y, reps=3, stream=stream)
+    t_b = event_ms(torch, lambda: batch.solve(X0, out=Y, stream=stream), stream, reps, warmup)
+    code, _ = batch.status(stream)
+    offs = batch.row_offsets
+    Ys = torch.empty_like(X0)
+    views = [(X0[offs[i]:offs[i + 1]], Ys[offs[i]:offs[i + 1]]) for i in range(len(graphs))]
+
+    def seq():
+        for g, (xi, yi) in zip(graphs, views):
+            g.diffuse(xi, T, out=yi, stream=stream)
+
+    t_s = event_ms(torch, seq, stream, reps, warmup)
+    same = bool(torch.equal(Y, Ys))
+    nnz = batch.nnz_total
+    batch.close()
+    for g in graphs:
+        g.close()
+    return {"workload": "64 graphs, cells log-uniform [2k, 100k], k=15, 16 cols, 8 steps, FP32",
+            "graphs": 64, "cells_total": int(offs[-1]), "nnz_total": int(nnz),
+            "batched_ms": round(t_b, 4), "sequential_ms": round(t_s, 4), "speedup": round(t_s / t_b, 3),
+            "bit_identical_to_sequential": same, "status": code, "schedule": sched}
+
+
 def cpu_model():
     try:
         for line in open("/proc/cpuinfo"):
@@ -174,6 +286,9 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-forms", action="store_true", help="skip the BF16/FP16 forms")
+    ap.add_argument("--no-backward", action="store_true", help="skip the forward+backward configuration")
+    ap.add_argument("--no-batched", action="store_true", help="skip the batched configuration")
     args = ap.parse_args()
     warmup = max(3, args.warmup)
 
@@ -281,7 +396,7 @@ def main():
     # ---- FP64 reference on the device for the precision forms --------------------------
     ip, ind, Pm = g.export()
     forms = {}
-    if rank == 0:
+    if rank == 0 and not args.no_forms:
         g64 = scl.gpu.GpuGraph.from_knn(ki, kd, variant="f64_i64")  # same W, FP64 normalisation below
         ip64, ind64, W32 = g64.export()
         g64.close()
@@ -317,6 +432,14 @@ def main():
         g.set_storage(torch.float32, stream=stream)
         g64.close()
         del Y64
+
+    # ---- differentiation and batched forms (each rank runs its own replica) ---------------
+    fwd_bwd = None
+    if not args.no_backward:
+        fwd_bwd = bench_backward(torch, scl, device, stream, args.steps, warmup, flush)
+    batched = None
+    if not args.no_batched:
+        batched = bench_batched(torch, scl, device, stream, args.steps, warmup)
 
     # ---- end to end through the drop-in C ABI with pinned host buffers --------------------
     e2e = None
@@ -372,13 +495,17 @@ def main():
                        "cells": n, "k": K_NN, "features": F, "diffusion_steps": T, "nnz": nnz,
                        "bytes_per_spmm_step": B32, "l2": "flushed (256 MiB write) before every timed step",
                        "parallelism": f"replicas x{world}"},
-            "gpu_launches": args.steps * T,
+            "gpu_launches": args.steps * (T + 1),
             "roofline": {"bound": "hbm", "achieved": round(achieved, 2), "peak": peak, "unit": "GB/s",
-                         "frac": round(achieved / peak, 4), "traffic": None, "peak_kind": peak_kind,
-                         "kernel": "k_spmm_row<float,float,float,float,256,8,true>",
+                         "frac": round(achieved / peak, 4), "traffic": profiled_traffic("spmm_row_f32_500k"),
+                         "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum per launch, "
+                                           "profiles/spmm_row_f32_500k.md", "peak_kind": peak_kind,
+                         "kernel": "k_spmm_row<float,float,float,float,256,16,true>",
                          "per_launch_ms": round(per_launch_ms, 5)},
             "forms": forms,
-            "fwd_bwd_ms": None,
+            "fwd_bwd_ms": fwd_bwd["fwd_bwd_ms"] if fwd_bwd else None,
+            "fwd_bwd": fwd_bwd,
+            "batched": batched,
             "graph_build_ms": round(build_ms, 3),
             "reorder_ms": round(reorder_ms, 3),
             "reorder_cc_rounds": cc_rounds,

@@ -104,10 +104,12 @@ SCL_EXPORT scl_error_t scl_gpu_graph_reorder_info(scl_gpu_graph_t graph, int32_t
  * load gathers 32/group entries that feed 32/group interleaved fma chains
  * summed pairwise at the row end (stage = gathers per lane per batch: 2/4/8
  * for 128-byte rows, 4/8/16 for 256-byte rows); 6 = kind 5 with the
- * mixed-precision fma. group <= 0 picks the default shape. X and Y must be in
- * the storage dtype (Y may also be F32). Every shape of kinds 0-4 computes the
- * same bits (the sequential fma chain); kinds 5 and 6 compute the same bits as
- * each other (the interleaved chains). */
+ * mixed-precision fma; 7 = flat entry stream over tasks of 16 consecutive
+ * rows with kind 4's lane layout (stage = gathers per batch 8/16/32; batches
+ * stay full across row ends). group <= 0 picks the default shape. X and Y must be in
+ * the storage dtype (Y may also be F32). Every shape of kinds 0-4 and 7
+ * computes the same bits (the sequential fma chain); kinds 5 and 6 compute the
+ * same bits as each other (the interleaved chains). */
 SCL_EXPORT scl_error_t scl_gpu_spmm(scl_gpu_graph_t graph, const void* X, void* Y, scl_dtype_t y_dtype,
                                     int64_t n_features, int group, int vec, int kind, int stage, void* stream);
 
@@ -127,22 +129,25 @@ SCL_EXPORT scl_error_t scl_gpu_graph_set_weights(scl_gpu_graph_t graph, const vo
 
 /* Y = P^n_steps X0 (original row order, X0 != Y) keeping checkpoints for
  * scl_gpu_diffuse_backward: X_s for s = every, 2*every, ... < n_steps, i.e.
- * (n_steps - 1) / every blocks of n x n_features written to `checkpoints`
- * (NULL allowed when that count is 0). Same bits as scl_gpu_diffuse. */
+ * nc = (n_steps - 1) / every blocks of n x n_features written to
+ * `checkpoints`, and with keep_last != 0 also the iterates of the last segment
+ * after its checkpoint (n_steps - 1 - nc * every more blocks, which the
+ * backward then does not recompute). NULL allowed when no block is kept.
+ * Same bits as scl_gpu_diffuse. */
 SCL_EXPORT scl_error_t scl_gpu_diffuse_checkpointed(scl_gpu_graph_t graph, const void* X0, void* Y,
                                                     int64_t n_features, int64_t n_steps, int64_t every,
-                                                    void* checkpoints, void* stream);
+                                                    int keep_last, void* checkpoints, void* stream);
 
 /* Backward of scl_gpu_diffuse_checkpointed with the same X0, checkpoints,
- * n_steps and every: given dY = dL/dX_T, writes dX0 = dL/dX_0 and, when dW is
- * non-NULL, dW = dL/dW (nnz entries, graph CSR order; dL/dP when the graph was
- * not normalised). Each checkpoint segment is recomputed with the forward
- * SpMM; each backward step is one fused kernel over the CSC view of P (built
- * once per graph) that gathers G_{s+1} rows once for both the transpose-SpMM
- * and the per-entry SDDMM. */
+ * n_steps, every and keep_last: given dY = dL/dX_T, writes dX0 = dL/dX_0 and,
+ * when dW is non-NULL, dW = dL/dW (nnz entries, graph CSR order; dL/dP when
+ * the graph was not normalised). Iterates that were not kept are recomputed
+ * from their segment's checkpoint with the forward SpMM; each backward step is
+ * one fused kernel over the CSC view of P (built once per graph) that gathers
+ * G_{s+1} rows once for both the transpose-SpMM and the per-entry SDDMM. */
 SCL_EXPORT scl_error_t scl_gpu_diffuse_backward(scl_gpu_graph_t graph, const void* X0, const void* checkpoints,
                                                 const void* dY, int64_t n_features, int64_t n_steps, int64_t every,
-                                                void* dX0, void* dW, void* stream);
+                                                int keep_last, void* dX0, void* dW, void* stream);
 
 /* ---- batched diffusion (no counterpart in scl-core, which diffuses one graph
  * per call: scl/binding/c_api/diffusion.h:28-35) ----

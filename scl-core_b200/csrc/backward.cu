@@ -24,9 +24,14 @@
 //               it to gPt[chunk + l] — a coalesced read-modify-write in CSC
 //               order that no other warp touches (no atomics).
 //   k_norm_*    normalisation backward in FP64 (degrees kept by normalize).
-// Checkpointing: the forward stores X_s for s = every, 2*every, ... < T; the
-// backward recomputes each segment from its checkpoint with the forward SpMM
-// (the same kernel, so the same bits) and walks it in reverse.
+//   k_adj_quarter  the same step for rows of 1, 2 or 4 blocks of eight 16-byte
+//               chunks: one load instruction gathers 4 entries (4 interleaved
+//               chains of G_s[i], summed pairwise at the row end), partial
+//               dots reduced within a quarter-warp (7 shuffles per 8 entries).
+// Checkpointing: the forward stores X_s for s = every, 2*every, ... < T (and,
+// with keep_last, the last segment's iterates); the backward recomputes every
+// other iterate of a segment from its checkpoint with the forward SpMM (the
+// same kernel, so the same bits) and walks the segment in reverse.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -173,6 +178,113 @@ k_adj_step(const int64_t* __restrict__ tptr, const int32_t* __restrict__ tidx, c
   }
 }
 
+// Quarter-warp form of the step for rows of NCB x 8 x (16 / sizeof(T))
+// elements: 8 lanes cover a column block with one 16-byte chunk each, so one
+// 128-bit load instruction gathers 4 entries (quarter q of the warp takes the
+// chunk's entries q, q+4, ..., q+28). Quarter q keeps its own fma chain of
+// G_s[i] over its entries; the 4 chains are summed (c0+c1)+(c2+c3) at the row
+// end. The 8 per-lane partial dots of a lane's entries are summed inside the
+// quarter by a transposed butterfly over lane bits 4, 2, 1 (7 shuffles for 8
+// entries); lane l of quarter q then adds entry 4*l + q of the chunk to gPt.
+// Summation order differs from the sequential chain only by the chain split.
+template <int H, class T>
+__device__ __forceinline__ void tr_round(T (&p)[8], int lq) {
+  const bool hi = (lq & H) != 0;
+#pragma unroll
+  for (int k = 0; k < H; ++k) {
+    const T send = hi ? p[k] : p[k + H];
+    const T keep = hi ? p[k + H] : p[k];
+    p[k] = keep + __shfl_xor_sync(0xffffffffu, send, H);
+  }
+}
+
+template <class T, int NCB, int U>
+__global__ void __launch_bounds__(256, (NCB == 1 && sizeof(T) == 4) ? 3 : 2)
+k_adj_quarter(const int64_t* __restrict__ tptr, const int32_t* __restrict__ tidx, const T* __restrict__ tval,
+              const T* __restrict__ G1, const T* __restrict__ Xs, T* __restrict__ G0, T* __restrict__ gPt,
+              int64_t n) {
+  constexpr int VEC = 16 / (int)sizeof(T);
+  constexpr int CB = 8 * VEC;      // columns per block
+  constexpr int F = NCB * CB;
+  constexpr int NB = 8 / U;        // batches per chunk of 32 entries
+  static_assert(U == 4 || U == 8, "batch of 4 or 8 gathers per lane");
+  const int lane = threadIdx.x & 31;
+  const int q = lane >> 3, lq = lane & 7;
+  const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
+  for (int64_t row = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; row < n; row += nw) {
+    const int64_t start = tptr[row], end = tptr[row + 1];
+    T xi[NCB][VEC], acc[NCB][VEC];
+#pragma unroll
+    for (int c = 0; c < NCB; ++c) {
+      load_vec<T, VEC>(Xs + row * F + c * CB + lq * VEC, xi[c]);
+#pragma unroll
+      for (int i = 0; i < VEC; ++i) acc[c][i] = T(0);
+    }
+    for (int64_t base = start; base < end; base += 32) {
+      const int64_t m = base + lane;
+      int32_t j_l = 0;
+      T v_l = T(0);
+      if (m < end) {
+        j_l = __ldcs(tidx + m);
+        v_l = __ldcs(tval + m);
+      }
+      const int cnt = (int)((end - base) < 32 ? (end - base) : 32);
+      T p[8];
+#pragma unroll
+      for (int u = 0; u < 8; ++u) p[u] = T(0);
+#pragma unroll
+      for (int b = 0; b < NB; ++b) {
+        if (b * U * 4 < cnt) {
+#pragma unroll
+          for (int c = 0; c < NCB; ++c) {
+            T g[U][VEC];
+#pragma unroll
+            for (int u = 0; u < U; ++u) {
+              const int e = (b * U + u) * 4 + q;
+              const int32_t jj = __shfl_sync(0xffffffffu, j_l, e);
+              if (e < cnt) {
+                load_vec<T, VEC>(G1 + (int64_t)jj * F + c * CB + lq * VEC, g[u]);
+              } else {
+#pragma unroll
+                for (int i = 0; i < VEC; ++i) g[u][i] = T(0);
+              }
+            }
+#pragma unroll
+            for (int u = 0; u < U; ++u) {
+              const int e = (b * U + u) * 4 + q;
+              const T vv = __shfl_sync(0xffffffffu, v_l, e);
+              T d = p[b * U + u];
+#pragma unroll
+              for (int i = 0; i < VEC; ++i) d = fma_t(g[u][i], xi[c][i], d);
+              p[b * U + u] = d;
+              if (e < cnt) {
+#pragma unroll
+                for (int i = 0; i < VEC; ++i) acc[c][i] = fma_t(vv, g[u][i], acc[c][i]);
+              }
+            }
+          }
+        }
+      }
+      if (gPt != nullptr) {
+        tr_round<4>(p, lq);
+        tr_round<2>(p, lq);
+        tr_round<1>(p, lq);
+        const int e = lq * 4 + q;
+        if (e < cnt) gPt[base + e] += p[0];
+      }
+    }
+#pragma unroll
+    for (int c = 0; c < NCB; ++c) {
+#pragma unroll
+      for (int i = 0; i < VEC; ++i) {
+        acc[c][i] = acc[c][i] + __shfl_xor_sync(0xffffffffu, acc[c][i], 8);
+        acc[c][i] = acc[c][i] + __shfl_xor_sync(0xffffffffu, acc[c][i], 16);
+      }
+      if (q == 0) store_vec<T, VEC>(G0 + row * F + c * CB + lq * VEC, acc[c]);
+    }
+  }
+}
+
 template <class T>
 __global__ void k_scatter_entries(const T* __restrict__ src, const int32_t* __restrict__ map, int64_t nnz,
                                   T* __restrict__ dst) {
@@ -240,10 +352,29 @@ void launch_adj(const CsrView& t, const T* G1, const T* Xs, T* G0, T* gPt, int64
   SCL_CUDA(cudaGetLastError());
 }
 
+template <class T, int NCB, int U>
+void launch_adj_quarter(const CsrView& t, const T* G1, const T* Xs, T* G0, T* gPt, cudaStream_t s) {
+  auto kern = k_adj_quarter<T, NCB, U>;
+  int dev = 0, per_sm = 0;
+  SCL_CUDA(cudaGetDevice(&dev));
+  SCL_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, 256, 0));
+  const int64_t need = (t.n_rows * 32 + 255) / 256;
+  const int64_t grid = std::max<int64_t>(1, std::min<int64_t>(need, (int64_t)std::max(per_sm, 1) * sm_count(dev)));
+  kern<<<(unsigned)grid, 256, 0, s>>>(t.indptr, t.indices, static_cast<const T*>(t.values), G1, Xs, G0, gPt,
+                                      t.n_rows);
+  SCL_CUDA(cudaGetLastError());
+}
+
 template <class T>
 void adj_step(const CsrView& t, const T* G1, const T* Xs, T* G0, T* gPt, int64_t F, cudaStream_t s) {
   constexpr int kV16 = 16 / (int)sizeof(T);
   const auto al = [&](const void* p, int b) { return (reinterpret_cast<uintptr_t>(p) % (uintptr_t)b) == 0; };
+  // quarter-warp kernel: rows of 1, 2 or 4 blocks of 8 sixteen-byte chunks
+  if (al(G1, 16) && al(Xs, 16) && al(G0, 16)) {
+    if (F == 8 * kV16) return launch_adj_quarter<T, 1, 8>(t, G1, Xs, G0, gPt, s);
+    if (F == 16 * kV16) return launch_adj_quarter<T, 2, 4>(t, G1, Xs, G0, gPt, s);
+    if (F == 32 * kV16) return launch_adj_quarter<T, 4, 4>(t, G1, Xs, G0, gPt, s);
+  }
   // one 16-byte chunk per lane when the row fits one column block of the warp
   if (F % kV16 == 0 && F <= 32 * kV16 && F > 16 * kV16 && al(G1, 16) && al(Xs, 16) && al(G0, 16))
     return launch_adj<T, kV16, 8>(t, G1, Xs, G0, gPt, F, s);
@@ -282,10 +413,28 @@ void adjoint_values(const void* vals, DType t, Adjoint& a, cudaStream_t s) {
 }
 
 // ---- checkpointed forward -------------------------------------------------------------
-int64_t checkpoint_slots(int64_t steps, int64_t every) { return steps > 0 ? (steps - 1) / every : 0; }
+// Slot layout: [0, nc) hold X_every, X_2every, ..., X_{nc*every} with
+// nc = (steps-1)/every; with keep_last, slots [nc, nc + steps-1-nc*every) hold
+// the last segment's iterates X_{nc*every+1} .. X_{steps-1}, which the
+// backward then needs not recompute.
+int64_t checkpoint_slots(int64_t steps, int64_t every, bool keep_last) {
+  if (steps <= 0 || every < 1) return 0;
+  const int64_t nc = (steps - 1) / every;
+  return nc + (keep_last ? (steps - 1 - nc * every) : 0);
+}
+
+namespace {
+// slot of iterate X_m (1 <= m < steps) or -1 when it is not kept
+inline int64_t slot_of(int64_t m, int64_t steps, int64_t every, bool keep_last) {
+  const int64_t nc = (steps - 1) / every;
+  if (m % every == 0) return m / every - 1;
+  if (keep_last && m > nc * every) return nc + (m - nc * every - 1);
+  return -1;
+}
+}  // namespace
 
 void diffuse_checkpointed(const CsrView& g, const void* X0, void* Y, DType t, int64_t F, int64_t steps,
-                          int64_t every, void* ckpt, cudaStream_t s) {
+                          int64_t every, bool keep_last, void* ckpt, cudaStream_t s) {
   SCL_REQUIRE(t == kF32 || t == kF64, kErrTypeMismatch, "checkpointed diffusion needs f32 or f64 values");
   SCL_REQUIRE(g.vtype == t, kErrTypeMismatch, "graph values and the iterate must have the same dtype");
   SCL_REQUIRE(g.n_rows == g.n_cols, kErrDimensionMismatch, "diffusion with checkpoints needs a square matrix");
@@ -311,10 +460,11 @@ void diffuse_checkpointed(const CsrView& g, const void* X0, void* Y, DType t, in
   for (int64_t st = 0; st < steps; ++st) {
     const int64_t made = st + 1;  // index of the iterate this step produces
     void* dst;
+    const int64_t slot = (made < steps) ? slot_of(made, steps, every, keep_last) : -1;
     if (made == steps) {
       dst = Y;
-    } else if (made % every == 0) {
-      dst = static_cast<char*>(ckpt) + (size_t)(made / every - 1) * blk;
+    } else if (slot >= 0) {
+      dst = static_cast<char*>(ckpt) + (size_t)slot * blk;
     } else {
       if (!A.p) A = DevBuf(blk, s);
       if (src == A.p) {
@@ -334,9 +484,11 @@ void diffuse_checkpointed(const CsrView& g, const void* X0, void* Y, DType t, in
 // ---- backward ---------------------------------------------------------------------------
 template <class T>
 static void backward_typed(const CsrView& g, const Adjoint& adj, const T* X0, const T* ckpt, const T* dY,
-                           int64_t F, int64_t steps, int64_t every, T* dX0, T* gPt, cudaStream_t s) {
+                           int64_t F, int64_t steps, int64_t every, bool keep_last, T* dX0, T* gPt,
+                           cudaStream_t s) {
   const int64_t n = g.n_rows;
   const size_t blk = (size_t)n * (size_t)F * sizeof(T);
+  const size_t elems = (size_t)n * (size_t)F;
   const CsrView tv = adj.t.view();
   if (gPt) SCL_CUDA(cudaMemsetAsync(gPt, 0, std::max<int64_t>(g.nnz, 1) * sizeof(T), s));
   if (steps <= 0) {
@@ -344,9 +496,8 @@ static void backward_typed(const CsrView& g, const Adjoint& adj, const T* X0, co
     return;
   }
   const int64_t seg = std::min<int64_t>(every, steps);
-  // segment iterates X_c .. X_{c+seg-1}: slot 0 aliases the checkpoint
+  // recomputed iterates of a segment (slot 0 of a segment aliases its checkpoint)
   std::vector<DevBuf> xs(seg);
-  for (int64_t k = 1; k < seg; ++k) xs[k] = DevBuf(blk, s);
   DevBuf Ga(blk, s), Gb(blk, s);
   const T* Gcur = dY;
   SpmmArgs a{};
@@ -361,14 +512,20 @@ static void backward_typed(const CsrView& g, const Adjoint& adj, const T* X0, co
   const int64_t last_c = ((steps - 1) / every) * every;
   for (int64_t c = last_c; c >= 0; c -= every) {
     const int64_t e = std::min<int64_t>(c + every, steps);
-    const T* base = (c == 0) ? X0 : ckpt + (size_t)(c / every - 1) * (size_t)n * (size_t)F;
     std::vector<const T*> X(e - c);
-    X[0] = base;
-    for (int64_t st = c; st < e - 1; ++st) {  // recompute X_{c+1} .. X_{e-1}
-      a.X = X[st - c];
-      a.Y = xs[st - c + 1].p;
+    for (int64_t m = c; m < e; ++m) {
+      const int64_t slot = (m == 0) ? -1 : slot_of(m, steps, every, keep_last);
+      if (m == 0) X[0] = X0;
+      else if (slot >= 0) X[m - c] = ckpt + (size_t)slot * elems;
+      else X[m - c] = nullptr;
+    }
+    for (int64_t m = c + 1; m < e; ++m) {  // recompute what was not kept
+      if (X[m - c] != nullptr) continue;
+      if (!xs[m - c].p) xs[m - c] = DevBuf(blk, s);
+      a.X = X[m - c - 1];
+      a.Y = xs[m - c].p;
       spmm(a, s);
-      X[st - c + 1] = xs[st - c + 1].as<T>();
+      X[m - c] = xs[m - c].as<T>();
     }
     for (int64_t st = e - 1; st >= c; --st) {
       T* Gnext = (st == 0) ? dX0 : ((Gcur == Ga.as<T>()) ? Gb.as<T>() : Ga.as<T>());
@@ -379,17 +536,18 @@ static void backward_typed(const CsrView& g, const Adjoint& adj, const T* X0, co
 }
 
 void diffuse_backward(const CsrView& g, const Adjoint& adj, const void* X0, const void* ckpt, const void* dY,
-                      DType t, int64_t F, int64_t steps, int64_t every, void* dX0, void* gPt, cudaStream_t s) {
+                      DType t, int64_t F, int64_t steps, int64_t every, bool keep_last, void* dX0, void* gPt,
+                      cudaStream_t s) {
   SCL_REQUIRE(t == kF32 || t == kF64, kErrTypeMismatch, "the backward pass needs f32 or f64 values");
   SCL_REQUIRE(g.vtype == t && adj.values_ok && adj.t.vtype == t, kErrInternal, "adjoint view is stale");
   SCL_REQUIRE(every >= 1, kErrInvalidArgument, "checkpoint interval must be >= 1");
   if (t == kF32)
     backward_typed<float>(g, adj, static_cast<const float*>(X0), static_cast<const float*>(ckpt),
-                          static_cast<const float*>(dY), F, steps, every, static_cast<float*>(dX0),
+                          static_cast<const float*>(dY), F, steps, every, keep_last, static_cast<float*>(dX0),
                           static_cast<float*>(gPt), s);
   else
     backward_typed<double>(g, adj, static_cast<const double*>(X0), static_cast<const double*>(ckpt),
-                           static_cast<const double*>(dY), F, steps, every, static_cast<double*>(dX0),
+                           static_cast<const double*>(dY), F, steps, every, keep_last, static_cast<double*>(dX0),
                            static_cast<double*>(gPt), s);
 }
 

@@ -278,7 +278,7 @@ SCL_EXPORT scl_error_t scl_gpu_graph_set_plan(scl_gpu_graph_t graph, int64_t n_f
     SCL_REQUIRE(kind == 0 || (kind == 1 && bytes == 16 && group >= 4 && (stage == 4 || stage == 8 || stage == 16)) ||
                     (kind == 2 && group == 32 && (stage == 8 || stage == 16)) ||
                     (kind == 3 && group == 32 && (stage == 16 || stage == 32) && bytes >= 4) ||
-                    (kind == 4 && group == 32 && (stage == 8 || stage == 16 || stage == 32) &&
+                    ((kind == 4 || kind == 7) && group == 32 && (stage == 8 || stage == 16 || stage == 32) &&
                      n_features == 32 * vec && (bytes == 4 || bytes == 8 || bytes == 16)) ||
                     ((kind == 5 || kind == 6) && dtype_size(graph->store_type) == 2 && bytes == 16 &&
                      n_features == (int64_t)group * vec &&
@@ -375,35 +375,35 @@ SCL_EXPORT scl_error_t scl_gpu_graph_set_weights(scl_gpu_graph_t graph, const vo
 
 SCL_EXPORT scl_error_t scl_gpu_diffuse_checkpointed(scl_gpu_graph_t graph, const void* X0, void* Y,
                                                     int64_t n_features, int64_t n_steps, int64_t every,
-                                                    void* checkpoints, void* stream) {
+                                                    int keep_last, void* checkpoints, void* stream) {
   SCL_API_CHECK_NULL(graph, "Graph is null");
   SCL_API_CHECK_NULL(X0, "Matrix X is null");
   SCL_API_CHECK_NULL(Y, "Matrix Y is null");
   SCL_API_CHECK(n_features > 0 && n_steps >= 0 && every >= 1, SCL_ERROR_INVALID_ARGUMENT,
                 "Dimensions must be positive");
-  SCL_API_CHECK(checkpoint_slots(n_steps, every) == 0 || checkpoints != nullptr, SCL_ERROR_NULL_POINTER,
-                "Checkpoint buffer is null");
+  SCL_API_CHECK(checkpoint_slots(n_steps, every, keep_last != 0) == 0 || checkpoints != nullptr,
+                SCL_ERROR_NULL_POINTER, "Checkpoint buffer is null");
   SCL_API_TRY
   ensure_device(graph);
   SCL_REQUIRE(graph->store_type == graph->g.vtype, SCL_ERROR_TYPE_MISMATCH,
               "checkpointed diffusion runs in the graph's f32/f64 values; reset the storage dtype first");
-  diffuse_checkpointed(graph->g.view(), X0, Y, graph->g.vtype, n_features, n_steps, every, checkpoints,
-                       as_stream(stream));
+  diffuse_checkpointed(graph->g.view(), X0, Y, graph->g.vtype, n_features, n_steps, every, keep_last != 0,
+                       checkpoints, as_stream(stream));
   SCL_API_RETURN_OK;
   SCL_API_CATCH
 }
 
 SCL_EXPORT scl_error_t scl_gpu_diffuse_backward(scl_gpu_graph_t graph, const void* X0, const void* checkpoints,
                                                 const void* dY, int64_t n_features, int64_t n_steps, int64_t every,
-                                                void* dX0, void* dW, void* stream) {
+                                                int keep_last, void* dX0, void* dW, void* stream) {
   SCL_API_CHECK_NULL(graph, "Graph is null");
   SCL_API_CHECK_NULL(X0, "Matrix X is null");
   SCL_API_CHECK_NULL(dY, "Gradient dY is null");
   SCL_API_CHECK_NULL(dX0, "Gradient output dX0 is null");
   SCL_API_CHECK(n_features > 0 && n_steps >= 0 && every >= 1, SCL_ERROR_INVALID_ARGUMENT,
                 "Dimensions must be positive");
-  SCL_API_CHECK(checkpoint_slots(n_steps, every) == 0 || checkpoints != nullptr, SCL_ERROR_NULL_POINTER,
-                "Checkpoint buffer is null");
+  SCL_API_CHECK(checkpoint_slots(n_steps, every, keep_last != 0) == 0 || checkpoints != nullptr,
+                SCL_ERROR_NULL_POINTER, "Checkpoint buffer is null");
   SCL_API_TRY
   ensure_device(graph);
   DeviceCSR& g = graph->g;
@@ -424,7 +424,8 @@ SCL_EXPORT scl_error_t scl_gpu_diffuse_backward(scl_gpu_graph_t graph, const voi
   const CsrView v = g.view();
   DevBuf gPt;
   if (dW != nullptr && n_steps > 0) gPt = DevBuf(std::max<int64_t>(g.nnz, 1) * dtype_size(g.vtype), s);
-  diffuse_backward(v, *graph->adj, X0, checkpoints, dY, g.vtype, n_features, n_steps, every, dX0, gPt.p, s);
+  diffuse_backward(v, *graph->adj, X0, checkpoints, dY, g.vtype, n_features, n_steps, every, keep_last != 0, dX0,
+                   gPt.p, s);
   if (dW != nullptr) {
     if (n_steps <= 0 || g.nnz == 0) {
       if (g.nnz > 0) SCL_CUDA(cudaMemsetAsync(dW, 0, g.nnz * dtype_size(g.vtype), s));

@@ -232,16 +232,18 @@ struct Adjoint {
 void build_adjoint(const DeviceCSR& g, Adjoint& a, cudaStream_t s);
 void adjoint_values(const void* vals, DType t, Adjoint& a, cudaStream_t s);
 
-// Checkpoint slots the forward fills: X_s for s = every, 2*every, ... < steps.
-int64_t checkpoint_slots(int64_t steps, int64_t every);
+// Checkpoint slots the forward fills: X_s for s = every, 2*every, ... < steps,
+// plus (keep_last) the iterates of the last segment after its checkpoint.
+int64_t checkpoint_slots(int64_t steps, int64_t every, bool keep_last);
 // Y = P^steps X0 (f32 or f64, original row order), storing the checkpoints in
-// ckpt (checkpoint_slots(steps, every) blocks of n x F). X0 != Y.
+// ckpt (checkpoint_slots(...) blocks of n x F). X0 != Y.
 void diffuse_checkpointed(const CsrView& g, const void* X0, void* Y, DType t, int64_t F, int64_t steps,
-                          int64_t every, void* ckpt, cudaStream_t s);
+                          int64_t every, bool keep_last, void* ckpt, cudaStream_t s);
 // Given dY = dL/dX_T: dX0 = dL/dX_0 and, when gPt is non-null, the SDDMM
 // gradient dL/dP accumulated in P^T's (CSC) entry order.
 void diffuse_backward(const CsrView& g, const Adjoint& adj, const void* X0, const void* ckpt, const void* dY,
-                      DType t, int64_t F, int64_t steps, int64_t every, void* dX0, void* gPt, cudaStream_t s);
+                      DType t, int64_t F, int64_t steps, int64_t every, bool keep_last, void* dX0, void* gPt,
+                      cudaStream_t s);
 // dW (CSR order of P) from dL/dP in CSC order, through the row or symmetric
 // normalisation with the FP64 degrees kept by normalize().
 void normalize_backward(const CsrView& P, const Adjoint& adj, const void* gPt, const double* degrees, int symmetric,

@@ -677,6 +677,111 @@ k_spmm_row(const int64_t* __restrict__ indptr, const int32_t* __restrict__ indic
   }
 }
 
+// ---- flat-stream kernel: a warp walks the entries of a block of rows ---------------
+// A task is R consecutive rows; their entries [indptr[r0], indptr[r0+R]) are
+// one contiguous stream that the warp consumes in batches of U gathers, with
+// no regard for where rows begin or end — every batch but the stream's last is
+// full, so U loads are always in flight, whatever the row lengths. The lane
+// layout is k_spmm_row's (lane l owns bytes [l*LB, (l+1)*LB) of every
+// gathered row, compile-time pitch), and entries are consumed in stream order:
+// when the stream passes a row's end the row's accumulator is stored and
+// reset, so every output element is still the sequential fma chain over its
+// row's entries in stored order (bit-identical to the other variants). Row
+// bounds of the task live in shared memory; (index, value) pairs are staged
+// 32 at a time in a per-warp double buffer, the next chunk always in flight.
+template <class VT, class XT, class YT, class AT, int ROWB, int U, int R>
+__global__ void __launch_bounds__(kSpmmThreads, (U * ROWB <= 2048) ? 4 : ((U * ROWB <= 4096) ? 3 : 2))
+k_spmm_flow(const int64_t* __restrict__ indptr, const int32_t* __restrict__ indices, const VT* __restrict__ values,
+            const XT* __restrict__ X, YT* __restrict__ Y, const int32_t* __restrict__ row_map, int64_t n_rows) {
+  constexpr int LB = ROWB / 32;
+  constexpr int VEC = LB / (int)sizeof(XT);
+  constexpr int WARPS = kSpmmThreads / 32;
+  constexpr int ROWE = ROWB / (int)sizeof(XT);
+  static_assert(LB == 4 || LB == 8 || LB == 16, "row pitch must be 128, 256 or 512 bytes");
+  static_assert(U == 8 || U == 16 || U == 32, "batch must divide 32");
+  static_assert(R >= 1 && R <= 31, "a task holds at most 31 rows");
+  using Rw = typename RawVec<LB>::type;
+  __shared__ __align__(16) int32_t s_j[WARPS][2][32];
+  __shared__ __align__(16) AT s_v[WARPS][2][32];
+  __shared__ int64_t s_ptr[WARPS][32];
+  const int lane = threadIdx.x & 31;
+  const int w = threadIdx.x >> 5;
+  const int64_t n_tasks = (n_rows + R - 1) / R;
+  const int64_t nw = ((int64_t)gridDim.x * kSpmmThreads) >> 5;
+  const char* __restrict__ Xb = reinterpret_cast<const char*>(X) + lane * LB;
+  for (int64_t task = ((int64_t)blockIdx.x * kSpmmThreads + threadIdx.x) >> 5; task < n_tasks; task += nw) {
+    const int64_t r0 = task * R;
+    const int nr = (int)((n_rows - r0) < R ? (n_rows - r0) : R);
+    if (lane <= nr) s_ptr[w][lane] = indptr[r0 + lane];
+    __syncwarp();
+    const int64_t p0 = s_ptr[w][0], p1 = s_ptr[w][nr];
+    int ri = 0;                      // current row r0 + ri
+    int64_t row_end = s_ptr[w][1];
+    AT acc[VEC];
+#pragma unroll
+    for (int i = 0; i < VEC; ++i) acc[i] = AT(0);
+    auto flush = [&]() {
+      const int64_t r = r0 + ri;
+      const int64_t orow = row_map ? (int64_t)row_map[r] : r;
+      VecStore<YT, VEC>::store(Y + orow * ROWE + lane * VEC, acc);
+#pragma unroll
+      for (int i = 0; i < VEC; ++i) acc[i] = AT(0);
+      ++ri;
+      row_end = (ri < nr) ? s_ptr[w][ri + 1] : p1;
+    };
+    int buf = 0;
+    if (p0 + lane < p1) {
+      s_j[w][0][lane] = __ldcs(indices + p0 + lane);
+      s_v[w][0][lane] = to_acc<AT, VT>(__ldcs(values + p0 + lane));
+    }
+    __syncwarp();
+    for (int64_t c = p0; c < p1; c += 32) {
+      int32_t j_n = 0;
+      AT v_n = AT(0);
+      if (c + 32 + lane < p1) {
+        j_n = __ldcs(indices + c + 32 + lane);
+        v_n = to_acc<AT, VT>(__ldcs(values + c + 32 + lane));
+      }
+      const int cnt = (p1 - c) < 32 ? (int)(p1 - c) : 32;
+      const int32_t* __restrict__ jb = s_j[w][buf];
+      const AT* __restrict__ vb = s_v[w][buf];
+#pragma unroll
+      for (int t = 0; t < 32; t += U) {
+        if (t >= cnt) break;
+        Rw xr[U];
+        const bool full = (t + U <= cnt);
+#pragma unroll
+        for (int q = 0; q < U; q += 4) {
+          const int4 j4 = *reinterpret_cast<const int4*>(jb + t + q);
+          const int jj[4] = {j4.x, j4.y, j4.z, j4.w};
+#pragma unroll
+          for (int r = 0; r < 4; ++r) {
+            if (full || t + q + r < cnt)
+              xr[q + r] = __ldg(reinterpret_cast<const Rw*>(Xb + (size_t)(uint32_t)jj[r] * ROWB));
+          }
+        }
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+          if (full || t + u < cnt) {
+            const int64_t e = c + t + u;
+            while (e >= row_end) flush();  // rows that end before entry e (empty rows included)
+            const AT vv = vb[t + u];
+            const XT* ex = reinterpret_cast<const XT*>(&xr[u]);
+#pragma unroll
+            for (int i = 0; i < VEC; ++i) acc[i] = fma_acc(vv, to_acc<AT, XT>(ex[i]), acc[i]);
+          }
+        }
+      }
+      s_j[w][buf ^ 1][lane] = j_n;
+      s_v[w][buf ^ 1][lane] = v_n;
+      __syncwarp();
+      buf ^= 1;
+    }
+    while (ri < nr) flush();  // the row holding the last entry, then trailing empty rows
+    __syncwarp();
+  }
+}
+
 // ---- split-chain warp-per-row kernel (16-bit storage) --------------------------------
 // One warp per row as in k_spmm_row, but every lane loads 16 bytes: a row of
 // ROWB bytes takes L = ROWB/16 lanes, so one 128-bit load instruction of the
@@ -701,6 +806,37 @@ template <>
 __device__ __forceinline__ float fma_mixed<__half>(unsigned short a, unsigned short b, float c) {
   asm("fma.rn.f32.f16 %0, %1, %2, %0;" : "+f"(c) : "h"(a), "h"(b));
   return c;
+}
+
+// One batch of the split-chain kernel: lane quarter q gathers entries
+// t + u*Q + q (u < U) and adds them to its chain; only a row's last batch
+// tests each entry against the chunk count.
+template <bool FULL, int U, int Q, int ROWB, class VT, class XT, bool MIXED>
+__device__ __forceinline__ void split_batch(const char* __restrict__ Xb, const int32_t* __restrict__ jb,
+                                            const unsigned short* __restrict__ vb, int t, int q, int cnt,
+                                            float (&acc)[8]) {
+  uint4 xr[U];
+#pragma unroll
+  for (int u = 0; u < U; ++u) {
+    const int e = t + u * Q + q;
+    if (FULL || e < cnt) xr[u] = __ldg(reinterpret_cast<const uint4*>(Xb + (size_t)(uint32_t)jb[e] * (size_t)ROWB));
+  }
+#pragma unroll
+  for (int u = 0; u < U; ++u) {
+    const int e = t + u * Q + q;
+    if (FULL || e < cnt) {
+      const unsigned short vbits = vb[e];
+      const unsigned short* ex = reinterpret_cast<const unsigned short*>(&xr[u]);
+      if constexpr (MIXED) {
+#pragma unroll
+        for (int i = 0; i < 8; ++i) acc[i] = fma_mixed<XT>(vbits, ex[i], acc[i]);
+      } else {
+        const float vf = tof<VT>(*reinterpret_cast<const VT*>(&vbits));
+#pragma unroll
+        for (int i = 0; i < 8; ++i) acc[i] = __fmaf_rn(vf, tof<XT>(*reinterpret_cast<const XT*>(&ex[i])), acc[i]);
+      }
+    }
+  }
 }
 
 template <class VT, class XT, class YT, int ROWB, int U, bool MIXED>
@@ -767,36 +903,10 @@ k_spmm_split(const int64_t* __restrict__ indptr, const int32_t* __restrict__ ind
       const int cnt = (len - base) < 32 ? (len - base) : 32;
       const int32_t* __restrict__ jb = s_j[w][buf];
       const unsigned short* __restrict__ vb = s_v[w][buf];
-#pragma unroll
-      for (int t = 0; t < 32; t += STEP) {
-        if (t >= cnt) break;
-        uint4 xr[U];
-#pragma unroll
-        for (int u = 0; u < U; ++u) {
-          const int e = t + u * Q + q;
-          if (e < cnt) {
-            const int32_t j = jb[e];
-            xr[u] = __ldg(reinterpret_cast<const uint4*>(Xb + (size_t)(uint32_t)j * ROWB));
-          }
-        }
-#pragma unroll
-        for (int u = 0; u < U; ++u) {
-          const int e = t + u * Q + q;
-          if (e < cnt) {
-            const unsigned short vbits = vb[e];
-            const unsigned short* ex = reinterpret_cast<const unsigned short*>(&xr[u]);
-            if constexpr (MIXED) {
-#pragma unroll
-              for (int i = 0; i < VEC; ++i) acc[i] = fma_mixed<XT>(vbits, ex[i], acc[i]);
-            } else {
-              const float vf = tof<VT>(*reinterpret_cast<const VT*>(&vbits));
-#pragma unroll
-              for (int i = 0; i < VEC; ++i)
-                acc[i] = __fmaf_rn(vf, tof<XT>(*reinterpret_cast<const XT*>(&ex[i])), acc[i]);
-            }
-          }
-        }
-      }
+      int t = 0;
+#pragma unroll 1
+      for (; t + STEP <= cnt; t += STEP) split_batch<true, U, Q, ROWB, VT, XT, MIXED>(Xb, jb, vb, t, q, cnt, acc);
+      if (t < cnt) split_batch<false, U, Q, ROWB, VT, XT, MIXED>(Xb, jb, vb, t, q, cnt, acc);
       s_j[w][buf ^ 1][lane] = j_n;
       s_v[w][buf ^ 1][lane] = v_n;
       __syncwarp();
@@ -960,6 +1070,37 @@ void launch_row(const SpmmArgs& a, int U, cudaStream_t s) {
   throw Error(kErrInvalidArgument, "the fixed-pitch SpMM needs 128-, 256- or 512-byte rows");
 }
 
+// kind 7: flat-stream kernel over tasks of 16 consecutive rows; stage = gathers per batch
+template <class VT, class XT, class YT, class AT, int ROWB, int U>
+void launch_flow_u(const SpmmArgs& a, cudaStream_t s) {
+  constexpr int R = 16;
+  auto kern = k_spmm_flow<VT, XT, YT, AT, ROWB, U, R>;
+  const int64_t tasks = (a.n_rows + R - 1) / R;
+  const dim3 grid(persistent_blocks(kern, 0, tasks, 32));
+  kern<<<grid, kSpmmThreads, 0, s>>>(a.indptr, a.indices, static_cast<const VT*>(a.values),
+                                     static_cast<const XT*>(a.X), static_cast<YT*>(a.Y), a.row_map, a.n_rows);
+  SCL_CUDA(cudaGetLastError());
+}
+
+template <class VT, class XT, class YT, class AT>
+void launch_flow(const SpmmArgs& a, int U, cudaStream_t s) {
+  const int64_t rowb = a.F * (int64_t)sizeof(XT);
+#define SCL_FLOW_CASE(RB)                                                          \
+  if constexpr (RB / 32 >= (int)sizeof(XT)) {                                      \
+    if (rowb == RB) {                                                              \
+      if (U == 8) return launch_flow_u<VT, XT, YT, AT, RB, 8>(a, s);               \
+      if (U == 16) return launch_flow_u<VT, XT, YT, AT, RB, 16>(a, s);             \
+      if (U == 32) return launch_flow_u<VT, XT, YT, AT, RB, 32>(a, s);             \
+      throw Error(kErrInvalidArgument, "flat-stream SpMM batch must be 8, 16 or 32"); \
+    }                                                                              \
+  }
+  SCL_FLOW_CASE(128)
+  SCL_FLOW_CASE(256)
+  SCL_FLOW_CASE(512)
+#undef SCL_FLOW_CASE
+  throw Error(kErrInvalidArgument, "the flat-stream SpMM needs 128-, 256- or 512-byte rows");
+}
+
 // kinds 5/6: split-chain kernel for 16-bit storage (6 = mixed-precision fma);
 // stage = gathers per lane per batch (U * chains must divide 32)
 template <class VT, class XT, class YT, int ROWB, int U, bool MIXED>
@@ -1027,6 +1168,11 @@ void launch_typed(const SpmmArgs& a, const SpmmPlan& plan, cudaStream_t s) {
                 kErrInvalidArgument, "the fixed-pitch SpMM covers a row with one chunk per lane of a warp");
     return launch_row<VT, XT, YT, AT>(a, plan.stage, s);
   }
+  if (plan.kind == 7) {
+    SCL_REQUIRE(plan.group == 32 && plan.vec * 32 == a.F, kErrInvalidArgument,
+                "the flat-stream SpMM covers a row with one chunk per lane of a warp");
+    return launch_flow<VT, XT, YT, AT>(a, plan.stage, s);
+  }
   if (plan.kind == 5 || plan.kind == 6) {
     SCL_REQUIRE(plan.vec == kVec && (int64_t)plan.group * kVec == a.F, kErrInvalidArgument,
                 "the split-chain SpMM covers a row with one 16-byte chunk per lane of a group");
@@ -1092,7 +1238,7 @@ SpmmPlan default_spmm_plan(int64_t F, DType xtype, const void* X, const void* Y,
       p.group = 32;
       p.vec = v;
       p.kind = 4;
-      p.stage = 8;
+      p.stage = 16;  // 16 gathers in flight per lane (measured faster than 8 on B200)
       return p;
     }
   }
@@ -1118,7 +1264,7 @@ void spmm_with_plan(const SpmmArgs& a, const SpmmPlan& plan, cudaStream_t s) {
   SCL_REQUIRE(plan.group >= 1 && plan.group <= 32 && (plan.group & (plan.group - 1)) == 0, kErrInvalidArgument,
               "lane-group size must be a power of two in [1, 32]");
   SCL_REQUIRE(plan.kind == 0 || plan.kind == 2 || plan.kind == 3 || plan.kind == 4 || plan.kind == 5 ||
-                  plan.kind == 6 || (plan.kind == 1 && plan.vec > 1 && plan.group >= 4),
+                  plan.kind == 6 || plan.kind == 7 || (plan.kind == 1 && plan.vec > 1 && plan.group >= 4),
               kErrInvalidArgument, "the pipelined SpMM needs 16-byte lane chunks and a lane group of at least 4");
   if (plan.vec > 1) {
     const int xs = (int)dtype_size(a.xtype), ys = (int)dtype_size(a.ytype);

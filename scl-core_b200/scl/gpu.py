@@ -181,34 +181,43 @@ class GpuGraph:
         return self
 
     @staticmethod
-    def checkpoint_slots(n_steps: int, every: int) -> int:
-        return (n_steps - 1) // every if (n_steps > 0 and every >= 1) else 0
+    def checkpoint_slots(n_steps: int, every: int, keep_last: bool = True) -> int:
+        """Blocks diffuse_checkpointed keeps: X_every, X_2every, ... and, with
+        keep_last, the last segment's iterates after its checkpoint."""
+        if n_steps <= 0 or every < 1:
+            return 0
+        nc = (n_steps - 1) // every
+        return nc + ((n_steps - 1 - nc * every) if keep_last else 0)
 
-    def diffuse_checkpointed(self, X0, n_steps: int, every: int, out=None, checkpoints=None, stream=None):
-        """(Y, checkpoints): Y = P^n_steps X0 keeping X_every, X_2every, ... for diffuse_backward."""
+    def diffuse_checkpointed(self, X0, n_steps: int, every: int, out=None, checkpoints=None, keep_last: bool = True,
+                             stream=None):
+        """(Y, checkpoints): Y = P^n_steps X0 keeping the iterates diffuse_backward needs."""
         torch = _torch()
         X0 = X0.contiguous()
         n, F = X0.shape
         Y = out if out is not None else torch.empty_like(X0)
-        k = self.checkpoint_slots(n_steps, every)
+        k = self.checkpoint_slots(n_steps, every, keep_last)
         if checkpoints is None:
             checkpoints = torch.empty((max(k, 0), n, F), dtype=X0.dtype, device=X0.device)
         cp = _ptr(checkpoints) if k > 0 else ctypes.c_void_p(0)
-        check_error(self._lib.scl_gpu_diffuse_checkpointed(self._h, _ptr(X0), _ptr(Y), F, int(n_steps), int(every), cp,
-                                                           _stream_ptr(stream)), "diffuse_checkpointed", self._lib)
+        check_error(self._lib.scl_gpu_diffuse_checkpointed(self._h, _ptr(X0), _ptr(Y), F, int(n_steps), int(every),
+                                                           int(keep_last), cp, _stream_ptr(stream)),
+                    "diffuse_checkpointed", self._lib)
         return Y, checkpoints
 
-    def diffuse_backward(self, X0, checkpoints, dY, n_steps: int, every: int, need_dW: bool = True, stream=None):
-        """(dX0, dW or None) for the diffusion run by diffuse_checkpointed."""
+    def diffuse_backward(self, X0, checkpoints, dY, n_steps: int, every: int, need_dW: bool = True,
+                         keep_last: bool = True, stream=None):
+        """(dX0, dW or None) for the diffusion run by diffuse_checkpointed (same every / keep_last)."""
         torch = _torch()
         X0, dY = X0.contiguous(), dY.contiguous()
         n, F = X0.shape
         dX0 = torch.empty_like(X0)
         dW = torch.empty(self.shape[2], dtype=X0.dtype, device=X0.device) if need_dW else None
-        k = self.checkpoint_slots(n_steps, every)
+        k = self.checkpoint_slots(n_steps, every, keep_last)
         cp = _ptr(checkpoints) if k > 0 else ctypes.c_void_p(0)
         check_error(self._lib.scl_gpu_diffuse_backward(self._h, _ptr(X0), cp, _ptr(dY), F, int(n_steps), int(every),
-                                                       _ptr(dX0), _ptr(dW) if dW is not None else ctypes.c_void_p(0),
+                                                       int(keep_last), _ptr(dX0),
+                                                       _ptr(dW) if dW is not None else ctypes.c_void_p(0),
                                                        _stream_ptr(stream)), "diffuse_backward", self._lib)
         return dX0, dW
 

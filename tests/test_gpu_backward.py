@@ -24,12 +24,13 @@ def _dev_graph(ip, ind, W, n, dtype, symmetric):
     return g
 
 
-def _loss_grads_gpu(g, X0, Yt, T, every):
+def _loss_grads_gpu(g, X0, Yt, T, every, keep_last=True):
     X0d = torch.from_numpy(X0).cuda()
     Yd = torch.from_numpy(Yt).cuda()
-    XT, ck = g.diffuse_checkpointed(X0d, T, every)
+    XT, ck = g.diffuse_checkpointed(X0d, T, every, keep_last=keep_last)
+    assert ck.shape[0] == g.checkpoint_slots(T, every, keep_last)
     dY = 2.0 * (XT - Yd)
-    dX, dW = g.diffuse_backward(X0d, ck, dY, T, every)
+    dX, dW = g.diffuse_backward(X0d, ck, dY, T, every, keep_last=keep_last)
     return XT, dX.cpu().numpy(), dW.cpu().numpy()
 
 
@@ -62,8 +63,9 @@ def test_fp32_backward_matches_fp64_adjoint(graph_3k, F, symmetric):
     assert _rel_fro(dW, dW64) < 2e-5 and _max_rel(dW, dW64) < 2e-4
 
 
+@pytest.mark.parametrize("keep_last", [True, False])
 @pytest.mark.parametrize("every", [1, 3, 4, 8, 11])
-def test_checkpoint_interval_does_not_change_bits(graph_3k, every):
+def test_checkpoint_interval_does_not_change_bits(graph_3k, every, keep_last):
     _, _, ip, ind, W = graph_3k
     n = ip.size - 1
     rng = np.random.default_rng(3)
@@ -71,7 +73,7 @@ def test_checkpoint_interval_does_not_change_bits(graph_3k, every):
     Yt = rng.standard_normal((n, 32)).astype(np.float32)
     g = _dev_graph(ip, ind, W, n, np.float32, False)
     try:
-        XT, dX, dW = _loss_grads_gpu(g, X0, Yt, 8, every)
+        XT, dX, dW = _loss_grads_gpu(g, X0, Yt, 8, every, keep_last)
         XT1, dX1, dW1 = _loss_grads_gpu(g, X0, Yt, 8, 1)
         # forward with checkpoints = the plain diffusion, bit for bit
         Yp = g.diffuse(torch.from_numpy(X0).cuda(), 8)
@@ -126,7 +128,9 @@ def test_zero_degree_rows_get_zero_weight_gradient():
 
 def _fd_check(ip, ind, W, n, X0, Yt, T, symmetric, dX, dW, n_entries, seed):
     """Central differences (eps = 1e-3) of L = sum((P^T X0 - Y)^2) with the FP64
-    device forward, at n_entries random entries of X0 and of W."""
+    device forward, at n_entries random entries of X0 and of W. The difference
+    L(+) - L(-) is formed elementwise as sum((X+ - X-) * (X+ + X- - 2Y)), so no
+    large sums are subtracted."""
     g = _dev_graph(ip, ind, W, n, np.float64, symmetric)
     Wd = torch.from_numpy(W.astype(np.float64)).cuda()
     X0d = torch.from_numpy(X0.astype(np.float64)).cuda()
@@ -134,13 +138,13 @@ def _fd_check(ip, ind, W, n, X0, Yt, T, symmetric, dX, dW, n_entries, seed):
     eps = 1e-3
     rng = np.random.default_rng(seed)
 
-    def loss_w(Wv):
+    def out_w(Wv):
         g.set_weights(Wv)
         g.normalize(symmetric=symmetric)
-        return float(((g.diffuse(X0d, T) - Yd) ** 2).sum())
+        return g.diffuse(X0d, T)
 
-    def loss_x(Xv):
-        return float(((g.diffuse(Xv, T) - Yd) ** 2).sum())
+    def dl(Xp, Xm):
+        return float(((Xp - Xm) * (Xp + Xm - 2.0 * Yd)).sum()) / (2 * eps)
 
     try:
         qs = rng.choice(W.size, n_entries, replace=False)
@@ -149,8 +153,8 @@ def _fd_check(ip, ind, W, n, X0, Yt, T, symmetric, dX, dW, n_entries, seed):
             Wp, Wm = Wd.clone(), Wd.clone()
             Wp[q] += eps
             Wm[q] -= eps
-            fd_w.append((loss_w(Wp) - loss_w(Wm)) / (2 * eps))
-        loss_w(Wd)  # restore P
+            fd_w.append(dl(out_w(Wp), out_w(Wm)))
+        out_w(Wd)  # restore P
         cells = rng.choice(X0.size, n_entries, replace=False)
         fd_x = []
         for c in cells:
@@ -158,7 +162,7 @@ def _fd_check(ip, ind, W, n, X0, Yt, T, symmetric, dX, dW, n_entries, seed):
             Xp, Xm = X0d.clone(), X0d.clone()
             Xp[i, f] += eps
             Xm[i, f] -= eps
-            fd_x.append((loss_x(Xp) - loss_x(Xm)) / (2 * eps))
+            fd_x.append(dl(g.diffuse(Xp, T), g.diffuse(Xm, T)))
     finally:
         g.close()
     an_w, an_x = dW[qs], dX.reshape(-1)[cells]
@@ -250,3 +254,32 @@ def test_backward_argument_errors(graph_3k):
             g.diffuse_checkpointed(X0, 8, 4)
     finally:
         g.close()
+
+
+def test_differentiation_configuration_full_size():
+    """The differentiation configuration at full size: 200,000 cells, k=30,
+    X0 200,000 x 32 FP32, 8 steps, L = sum((X_8 - Y)^2), checkpoint every 4.
+    dL/dX0 and dL/dW against the FP64 adjoint restatement and against central
+    finite differences (eps = 1e-3, FP64 device forward) on 256 random entries
+    (128 of W, 128 of X0)."""
+    n, k, F, T, every = 200_000, 30, 32, 8, 4
+    pts = scl.synthetic.mixture(n, seed=0)
+    ki, kd = scl.synthetic.knn_device(pts, k, block=4096)
+    g = scl.gpu.GpuGraph.from_knn(ki, kd)
+    del ki, kd
+    ip, ind, W32 = g.export()
+    g.normalize(symmetric=False)
+    rng = np.random.default_rng(12)
+    X0 = rng.standard_normal((n, F)).astype(np.float32)
+    Yt = rng.standard_normal((n, F)).astype(np.float32)
+    try:
+        _, dX, dW = _loss_grads_gpu(g, X0, Yt, T, every)
+    finally:
+        g.close()
+    torch.cuda.empty_cache()
+    _, dX64, dW64 = port.adjoint(ip, ind, W32.astype(np.float64), X0.astype(np.float64), Yt.astype(np.float64), T)
+    assert _rel_fro(dX, dX64) < 2e-5 and _max_rel(dX, dX64) < 2e-4
+    assert _rel_fro(dW, dW64) < 2e-5 and _max_rel(dW, dW64) < 2e-4
+    ew, ex = _fd_check(ip, ind, W32.astype(np.float64), n, X0, Yt, T, False, dX.astype(np.float64),
+                       dW.astype(np.float64), 128, seed=9)
+    assert ew < 1e-4 and ex < 1e-4, (ew, ex)

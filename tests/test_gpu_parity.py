@@ -193,6 +193,22 @@ def test_skewed_and_empty_rows():
         X = X0.copy()
         scl.diffusion.diffuse_matrix(wrap(ip, ind, P.copy(), n), X, 3)
         np.testing.assert_array_equal(bits(X), bits(port.diffuse_matrix(ip, ind, P, X0, 3)))
+    # the fixed-pitch kernels on the same rows (runs of empty rows inside a
+    # row block, a hub row spanning many batches)
+    import torch
+
+    g = scl.gpu.GpuGraph.from_csr(ip, ind.astype(np.int32), P, (n, n))
+    try:
+        for F, vec in ((32, 1), (64, 2), (128, 4)):
+            X0 = rng.standard_normal((n, F)).astype(np.float32)
+            ref1 = port.spmm(ip, ind, P, X0)
+            Xd = torch.from_numpy(X0).cuda()
+            for kind, stage in ((4, 8), (4, 32), (7, 8), (7, 16), (7, 32)):
+                Y = torch.empty_like(Xd)
+                g.spmm(Xd, Y, group=32, vec=vec, kind=kind, stage=stage)
+                np.testing.assert_array_equal(bits(Y.cpu().numpy()), bits(ref1))
+    finally:
+        g.close()
 
 
 def test_index_out_of_range_is_reported():
@@ -290,6 +306,7 @@ def test_every_launch_shape_is_exact(graph_3k, group):
         shapes.append((2, 0, 8))  # whole warp per row, 8-byte lane chunks
         shapes += [(2, 2, 8), (2, 2, 16), (2, 3, 16), (2, 3, 32), (1, 3, 16)]  # row-block streams
         shapes += [(2, 4, 8), (2, 4, 16), (2, 4, 32)]  # fixed-pitch warp-per-row
+        shapes += [(2, 7, 8), (2, 7, 16), (2, 7, 32)]  # flat entry stream over row blocks
     for vec, kind, stage in shapes:
         Y = torch.empty_like(Xd)
         g.spmm(Xd, Y, group=group, vec=vec, kind=kind, stage=stage)

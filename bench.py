@@ -225,15 +225,21 @@ def bench_backward(torch, scl, device, stream, reps, warmup, flush):
             "fwd_bwd_over_fwd": round(t_fb / t_f, 3)}
 
 
-def bench_batched(torch, scl, device, stream, reps, warmup):
+def bench_batched(torch, scl, device, stream, reps, warmup, rank=0, world=1, dist=None):
     """Batched form: 64 graphs, cell counts log-uniform in [2,000, 100,000]
     (seed 0), each its own 10-component mixture, k=15, row-normalised FP32,
     16-column blocks, 8 steps: one persistent CUDA-graph launch (autotuned
-    schedule) against 64 sequential scl_gpu_diffuse calls."""
+    schedule) against 64 sequential scl_gpu_diffuse calls. With N ranks the
+    graphs are sharded by longest-processing-time on nnz*F*T (no collective
+    in the data path) and the times are the max over ranks."""
+    from scl import sharding
+
     rng = np.random.default_rng(0)
-    sizes = np.exp(rng.uniform(np.log(2000), np.log(100_000), 64)).astype(int)
+    sizes_all = np.exp(rng.uniform(np.log(2000), np.log(100_000), 64)).astype(int)
+    mine = sharding.shard_for_rank([float(n) for n in sizes_all], rank, world)
+    sizes = [(b, sizes_all[b]) for b in mine]
     graphs = []
-    for b, n in enumerate(sizes):
+    for b, n in sizes:
         pts = scl.synthetic.mixture(int(n), seed=100 + b)
         ki, kd = scl.synthetic.knn_device(pts, 15, device=device, block=8192)
         g = scl.gpu.GpuGraph.from_knn(ki, kd, stream=stream)
@@ -262,8 +268,13 @@ def bench_batched(torch, scl, device, stream, reps, warmup):
     batch.close()
     for g in graphs:
         g.close()
+    if dist is not None:
+        tt = torch.tensor([t_b, t_s], device=device)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        t_b, t_s = float(tt[0]), float(tt[1])
     return {"workload": "64 graphs, cells log-uniform [2k, 100k], k=15, 16 cols, 8 steps, FP32",
-            "graphs": 64, "cells_total": int(offs[-1]), "nnz_total": int(nnz),
+            "graphs": 64, "graphs_this_rank": len(mine), "cells_this_rank": int(offs[-1]),
+            "nnz_this_rank": int(nnz), "sharding": f"LPT over {world} rank(s), no data-path collective",
             "batched_ms": round(t_b, 4), "sequential_ms": round(t_s, 4), "speedup": round(t_s / t_b, 3),
             "bit_identical_to_sequential": same, "status": code, "schedule": sched}
 
@@ -367,6 +378,8 @@ def main():
     _, cc_rounds = g.reorder_info()
     n, _, nnz = g.shape
     F, T = N_FEAT, N_STEPS
+    tuned = g.autotune(F, reps=3, stream=stream)  # one-off: fastest bit-identical launch shape
+    floor_ms = g.gather_floor(F, reps=5, stream=stream)  # gathers only, same rows and order
     B32 = step_bytes(n, nnz, F)
     B16 = step_bytes(n, nnz, F, s_val=2, s_x=2)
     gen = torch.Generator(device=device).manual_seed(1 + rank)
@@ -439,7 +452,7 @@ def main():
         fwd_bwd = bench_backward(torch, scl, device, stream, args.steps, warmup, flush)
     batched = None
     if not args.no_batched:
-        batched = bench_batched(torch, scl, device, stream, args.steps, warmup)
+        batched = bench_batched(torch, scl, device, stream, args.steps, warmup, rank, world, dist)
 
     # ---- end to end through the drop-in C ABI with pinned host buffers --------------------
     e2e = None
@@ -500,8 +513,13 @@ def main():
                          "frac": round(achieved / peak, 4), "traffic": profiled_traffic("spmm_row_f32_500k"),
                          "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum per launch, "
                                            "profiles/spmm_row_f32_500k.md", "peak_kind": peak_kind,
-                         "kernel": "k_spmm_row<float,float,float,float,256,16,true>",
-                         "per_launch_ms": round(per_launch_ms, 5)},
+                         "kernel": f"SpMM plan kind {tuned['kind']} stage {tuned['stage']} "
+                                   "(kind 4 = k_spmm_row, kind 7 = k_spmm_flow)",
+                         "per_launch_ms": round(per_launch_ms, 5),
+                         "gather_floor_ms": round(floor_ms, 5),
+                         "frac_of_gather_floor": round(floor_ms / per_launch_ms, 4),
+                         "gather_floor_note": "time of a kernel that only gathers the same 26.1M 256-byte X rows "
+                                              "in the same order at full occupancy (scl_gpu_graph_gather_floor)"},
             "forms": forms,
             "fwd_bwd_ms": fwd_bwd["fwd_bwd_ms"] if fwd_bwd else None,
             "fwd_bwd": fwd_bwd,

@@ -90,6 +90,24 @@ SCL_EXPORT scl_error_t scl_gpu_graph_reorder(scl_gpu_graph_t graph, int mode, vo
 SCL_EXPORT scl_error_t scl_gpu_graph_set_plan(scl_gpu_graph_t graph, int64_t n_features, int group, int vec, int kind,
                                               int stage);
 
+/* Measurement aid (no counterpart in scl-core): median time in ms over `reps`
+ * of a kernel that only gathers one row of n_features elements of `dtype` per
+ * stored entry, in the order scl_gpu_diffuse visits the entries (the reordered
+ * structure when one is set), at full occupancy and with the L2 flushed before
+ * each repetition. It is the memory-system floor of one SpMM step on this
+ * graph (row pitch 128, 256 or 512 bytes). Synchronises `stream`. */
+SCL_EXPORT scl_error_t scl_gpu_graph_gather_floor(scl_gpu_graph_t graph, int64_t n_features, scl_dtype_t dtype,
+                                                  int reps, double* ms, void* stream);
+
+/* Autotuner: times every launch shape that computes the same bits as the
+ * default one for n_features columns in the current storage dtype (row pitch,
+ * gathers per batch, kernel family members), `reps` SpMM steps each on the
+ * structure scl_gpu_diffuse uses, and keeps the fastest as this graph's plan
+ * for that width (scl_gpu_graph_set_plan). Reports its kind, stage and median
+ * step time; any pointer may be NULL. Synchronises `stream`. */
+SCL_EXPORT scl_error_t scl_gpu_graph_autotune(scl_gpu_graph_t graph, int64_t n_features, int reps, int* kind,
+                                              int* stage, double* best_ms, void* stream);
+
 /* The reordering's permutation (perm[new] = old, host int32 [n_rows]) and the
  * number of component-labelling rounds it took; either pointer may be NULL. */
 SCL_EXPORT scl_error_t scl_gpu_graph_reorder_info(scl_gpu_graph_t graph, int32_t* perm, int* cc_rounds, void* stream);
@@ -106,10 +124,13 @@ SCL_EXPORT scl_error_t scl_gpu_graph_reorder_info(scl_gpu_graph_t graph, int32_t
  * for 128-byte rows, 4/8/16 for 256-byte rows); 6 = kind 5 with the
  * mixed-precision fma; 7 = flat entry stream over tasks of 16 consecutive
  * rows with kind 4's lane layout (stage = gathers per batch 8/16/32; batches
- * stay full across row ends). group <= 0 picks the default shape. X and Y must be in
+ * stay full across row ends); 9 = kind 5/6's layout and chains with the
+ * gathers copied by cp.async into shared memory, two chunks of 32 entries in
+ * flight per warp (stage 0 = plain fma, 1 = mixed-precision fma). group <= 0
+ * picks the default shape. X and Y must be in
  * the storage dtype (Y may also be F32). Every shape of kinds 0-4 and 7
- * computes the same bits (the sequential fma chain); kinds 5 and 6 compute the
- * same bits as each other (the interleaved chains). */
+ * computes the same bits (the sequential fma chain); kinds 5, 6 and 9 compute
+ * the same bits as each other (the interleaved chains). */
 SCL_EXPORT scl_error_t scl_gpu_spmm(scl_gpu_graph_t graph, const void* X, void* Y, scl_dtype_t y_dtype,
                                     int64_t n_features, int group, int vec, int kind, int stage, void* stream);
 

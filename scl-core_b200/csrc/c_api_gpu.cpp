@@ -280,6 +280,9 @@ SCL_EXPORT scl_error_t scl_gpu_graph_set_plan(scl_gpu_graph_t graph, int64_t n_f
                     (kind == 3 && group == 32 && (stage == 16 || stage == 32) && bytes >= 4) ||
                     ((kind == 4 || kind == 7) && group == 32 && (stage == 8 || stage == 16 || stage == 32) &&
                      n_features == 32 * vec && (bytes == 4 || bytes == 8 || bytes == 16)) ||
+                    (kind == 9 && dtype_size(graph->store_type) == 2 && bytes == 16 &&
+                     n_features == (int64_t)group * vec && (group == 8 || group == 16) &&
+                     (stage == 0 || stage == 1)) ||
                     ((kind == 5 || kind == 6) && dtype_size(graph->store_type) == 2 && bytes == 16 &&
                      n_features == (int64_t)group * vec &&
                      ((group == 8 && (stage == 2 || stage == 4 || stage == 8)) ||
@@ -549,6 +552,92 @@ SCL_EXPORT scl_error_t scl_gpu_batch_status(scl_gpu_batch_t batch, int* code, in
   const int32_t c = batch->solver.status(as_stream(stream), &it);
   if (code) *code = c;
   if (item) *item = it;
+  SCL_API_RETURN_OK;
+  SCL_API_CATCH
+}
+
+SCL_EXPORT scl_error_t scl_gpu_graph_gather_floor(scl_gpu_graph_t graph, int64_t n_features, scl_dtype_t dtype,
+                                                  int reps, double* ms, void* stream) {
+  SCL_API_CHECK_NULL(graph, "Graph is null");
+  SCL_API_CHECK_NULL(ms, "Output pointer is null");
+  SCL_API_CHECK(n_features > 0 && reps > 0, SCL_ERROR_INVALID_ARGUMENT, "Dimensions must be positive");
+  SCL_API_TRY
+  ensure_device(graph);
+  const DType t = checked_dtype(dtype);
+  SCL_REQUIRE(is_float_dtype(t), SCL_ERROR_TYPE_MISMATCH, "dtype must be a float dtype");
+  const int32_t* idx = graph->reo ? graph->reo->indices.as<int32_t>() : graph->g.indices.as<int32_t>();
+  *ms = gather_floor_ms(idx, graph->g.nnz, std::max(graph->g.n_rows, graph->g.n_cols),
+                        n_features * (int64_t)dtype_size(t), reps, as_stream(stream));
+  SCL_API_RETURN_OK;
+  SCL_API_CATCH
+}
+
+SCL_EXPORT scl_error_t scl_gpu_graph_autotune(scl_gpu_graph_t graph, int64_t n_features, int reps, int* kind,
+                                              int* stage, double* best_ms, void* stream) {
+  SCL_API_CHECK_NULL(graph, "Graph is null");
+  SCL_API_CHECK(n_features > 0, SCL_ERROR_INVALID_ARGUMENT, "Dimensions must be positive");
+  SCL_API_TRY
+  ensure_device(graph);
+  cudaStream_t s = as_stream(stream);
+  const DType t = graph->store_type;
+  const CsrView v = graph->storage_view();
+  SpmmArgs a{};
+  if (graph->reo) {  // time the structure scl_gpu_diffuse runs on
+    Reordered& r = *graph->reo;
+    if (!r.values_ok || r.vtype != t) reorder_values(v.values, v.vtype, r, s);
+    a.indptr = r.indptr.as<int64_t>();
+    a.indices = r.indices.as<int32_t>();
+    a.values = r.values.p;
+  } else {
+    a.indptr = v.indptr;
+    a.indices = v.indices;
+    a.values = v.values;
+  }
+  a.vtype = t;
+  a.n_rows = v.n_rows;
+  a.F = n_features;
+  a.xtype = t;
+  a.ytype = t;
+  const size_t blk = (size_t)std::max(v.n_rows, v.n_cols) * (size_t)n_features * dtype_size(t);
+  DevBuf X(blk, s), Y(blk, s);
+  SCL_CUDA(cudaMemsetAsync(X.p, 0, blk, s));
+  a.X = X.p;
+  a.Y = Y.p;
+  const std::vector<SpmmPlan> cands = candidate_plans(n_features, t, X.p, Y.p, t);
+  cudaEvent_t e0, e1;
+  SCL_CUDA(cudaEventCreate(&e0));
+  SCL_CUDA(cudaEventCreate(&e1));
+  double best = 1e300;
+  SpmmPlan best_plan = cands.front();
+  const int r = std::max(reps, 1);
+  try {
+    for (const SpmmPlan& p : cands) {
+      spmm_with_plan(a, p, s);  // warm-up (also validates the shape)
+      std::vector<float> ts(r);
+      for (int k = 0; k < r; ++k) {
+        SCL_CUDA(cudaEventRecord(e0, s));
+        spmm_with_plan(a, p, s);
+        SCL_CUDA(cudaEventRecord(e1, s));
+        SCL_CUDA(cudaEventSynchronize(e1));
+        SCL_CUDA(cudaEventElapsedTime(&ts[k], e0, e1));
+      }
+      std::sort(ts.begin(), ts.end());
+      if (ts[r / 2] < best) {
+        best = ts[r / 2];
+        best_plan = p;
+      }
+    }
+  } catch (...) {
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    throw;
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  graph->plans[{n_features, (int)t}] = best_plan;
+  if (kind) *kind = best_plan.kind;
+  if (stage) *stage = best_plan.stage;
+  if (best_ms) *best_ms = best;
   SCL_API_RETURN_OK;
   SCL_API_CATCH
 }

@@ -159,6 +159,9 @@ struct SpmmPlan {
   int stage = 8;
 };
 SpmmPlan default_spmm_plan(int64_t F, DType xtype, const void* X, const void* Y, DType ytype);
+// Launch shapes that compute the same bits as the default one for this width
+// and dtype (the default first): the autotuner's search space.
+std::vector<SpmmPlan> candidate_plans(int64_t F, DType xtype, const void* X, const void* Y, DType ytype);
 
 // One Y = P X. Each output element is the sequential fma chain over the row's
 // nonzeros in stored order (FP32 accumulation, FP64 when values/X are f64).
@@ -248,6 +251,11 @@ void diffuse_backward(const CsrView& g, const Adjoint& adj, const void* X0, cons
 // normalisation with the FP64 degrees kept by normalize().
 void normalize_backward(const CsrView& P, const Adjoint& adj, const void* gPt, const double* degrees, int symmetric,
                         void* dW, cudaStream_t s);
+// Median time (ms) over `reps` of gathering one row_bytes-wide row per entry of
+// idx[0..M) from an n_rows-row block — the memory-system floor of an SpMM step
+// that visits the same column sequence (probe.cu).
+double gather_floor_ms(const int32_t* idx, int64_t M, int64_t n_rows, int64_t row_bytes, int reps, cudaStream_t s);
+
 // dL/dP in CSR order from its CSC-order accumulator.
 void scatter_adjoint_entries(const Adjoint& adj, const void* gPt, DType t, void* gP, cudaStream_t s);
 

@@ -21,6 +21,7 @@
 
 #include <cstdio>
 
+#include "chunk_cursor.cuh"
 #include "engine.hpp"
 
 namespace sclgpu {
@@ -839,8 +840,14 @@ __device__ __forceinline__ void split_batch(const char* __restrict__ Xb, const i
   }
 }
 
+// Resident CTAs per SM of the split-chain kernel with 2 gathers per lane per
+// batch (the 128-byte-row default): a compile-time tuning constant.
+#ifndef SCL_SPLIT_MIN_BLOCKS_U2
+#define SCL_SPLIT_MIN_BLOCKS_U2 4
+#endif
+
 template <class VT, class XT, class YT, int ROWB, int U, bool MIXED>
-__global__ void __launch_bounds__(kSpmmThreads, (U <= 2) ? 4 : ((U <= 8) ? 3 : 2))
+__global__ void __launch_bounds__(kSpmmThreads, (U <= 2) ? SCL_SPLIT_MIN_BLOCKS_U2 : ((U <= 8) ? 3 : 2))
 k_spmm_split(const int64_t* __restrict__ indptr, const int32_t* __restrict__ indices, const VT* __restrict__ values,
              const XT* __restrict__ X, YT* __restrict__ Y, const int32_t* __restrict__ row_map, int64_t n_rows) {
   static_assert(sizeof(XT) == 2 && sizeof(VT) == 2, "the split-chain kernel is for 16-bit storage");
@@ -935,6 +942,127 @@ k_spmm_split(const int64_t* __restrict__ indptr, const int32_t* __restrict__ ind
     s_nx = s_nn;
     e_nx = e_nn;
   }
+}
+
+// ---- pipelined split-chain kernel (16-bit storage, gathers land in shared memory) ---
+// The lane layout and the chain order of k_spmm_split (quarter q of the warp
+// takes entries q, q+Q, ... of the row, one 16-byte chunk per lane), but the
+// gathered chunks are copied by cp.async straight into lane-private
+// shared-memory slots instead of registers: the next chunk of 32 entries per
+// warp is in flight while the current one is consumed, so deep batches cost no
+// registers. The warp walks its chunk stream (chunk_cursor.cuh) three deep:
+// (index, value) pairs of chunk k+2 load while chunk k+1's gathers are in
+// flight and chunk k is consumed. Each lane only reads slots it filled itself,
+// so the per-thread cp.async.wait_group is the only synchronisation. Same bits
+// as k_spmm_split.
+template <int ROWB>
+constexpr int split_pipe_warps() { return ROWB == 128 ? 8 : 4; }
+template <int ROWB>
+constexpr int split_pipe_smem() { return split_pipe_warps<ROWB>() * 2 * 32 * ROWB; }
+
+template <class VT, class XT, class YT, int ROWB, bool MIXED>
+__global__ void __launch_bounds__(32 * split_pipe_warps<ROWB>())
+k_spmm_split_pipe(const int64_t* __restrict__ indptr, const int32_t* __restrict__ indices,
+                  const VT* __restrict__ values, const XT* __restrict__ X, YT* __restrict__ Y,
+                  const int32_t* __restrict__ row_map, int64_t n_rows) {
+  static_assert(sizeof(XT) == 2 && sizeof(VT) == 2, "the split-chain kernel is for 16-bit storage");
+  constexpr int L = ROWB / 16;  // lanes per gathered row
+  constexpr int Q = 32 / L;     // chains (entries per load instruction)
+  constexpr int U = 32 / Q;     // copies per lane per chunk
+  constexpr int VEC = 8;
+  constexpr int NT = 32 * split_pipe_warps<ROWB>();
+  extern __shared__ uint4 smem_split[];
+  const int lane = threadIdx.x & 31;
+  const int w = threadIdx.x >> 5;
+  const int q = lane / L;
+  const int lq = lane & (L - 1);
+  uint4* __restrict__ my = smem_split + (size_t)w * 2 * U * 32 + lane;  // slot (st, u): my[(st * U + u) * 32]
+  const char* __restrict__ Xb = reinterpret_cast<const char*>(X) + lq * 16;
+  const unsigned short* __restrict__ vbits = reinterpret_cast<const unsigned short*>(values);
+  const int64_t nw = ((int64_t)gridDim.x * NT) >> 5;
+  const int64_t row0 = ((int64_t)blockIdx.x * NT + threadIdx.x) >> 5;
+  if (row0 >= n_rows) return;
+  ChunkCursor cur;
+  cur.init(indptr, row0, n_rows, nw);
+  Chunk C = cur.next(indptr);  // pairs loading
+  int32_t jC = 0;
+  unsigned vC = 0;
+  if (C.valid && lane < C.cnt) {
+    jC = __ldcs(indices + C.pos + lane);
+    vC = __ldcs(vbits + C.pos + lane);
+  }
+  Chunk B;  // gathers in flight
+  unsigned vB = 0;
+  int st = 0;
+  float acc[VEC];
+#pragma unroll
+  for (int i = 0; i < VEC; ++i) acc[i] = 0.0f;
+  while (B.valid || C.valid) {
+    Chunk D = cur.next(indptr);
+    int32_t jD = 0;
+    unsigned vD = 0;
+    if (D.valid && lane < D.cnt) {
+      jD = __ldcs(indices + D.pos + lane);
+      vD = __ldcs(vbits + D.pos + lane);
+    }
+    if (C.valid) {
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        const int e = u * Q + q;
+        const int32_t jj = __shfl_sync(0xffffffffu, jC, e);
+        if (e < C.cnt) {
+          const unsigned s = (unsigned)__cvta_generic_to_shared(my + (st * U + u) * 32);
+          asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s),
+                       "l"(Xb + (size_t)(uint32_t)jj * (size_t)ROWB) : "memory");
+        }
+      }
+    }
+    cp_async_commit_group();
+    if (B.valid) {
+      cp_async_wait_group<1>();
+      if (B.first) {
+#pragma unroll
+        for (int i = 0; i < VEC; ++i) acc[i] = 0.0f;
+      }
+      const uint4* __restrict__ sb = my + (st ^ 1) * U * 32;
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        const int e = u * Q + q;
+        const unsigned short vv = (unsigned short)__shfl_sync(0xffffffffu, vB, e);
+        if (e < B.cnt) {
+          const uint4 raw = sb[u * 32];
+          const unsigned short* ex = reinterpret_cast<const unsigned short*>(&raw);
+          if constexpr (MIXED) {
+#pragma unroll
+            for (int i = 0; i < VEC; ++i) acc[i] = fma_mixed<XT>(vv, ex[i], acc[i]);
+          } else {
+            const float vf = tof<VT>(*reinterpret_cast<const VT*>(&vv));
+#pragma unroll
+            for (int i = 0; i < VEC; ++i)
+              acc[i] = __fmaf_rn(vf, tof<XT>(*reinterpret_cast<const XT*>(&ex[i])), acc[i]);
+          }
+        }
+      }
+      if (B.last) {
+#pragma unroll
+        for (int o = L; o < 32; o <<= 1) {
+#pragma unroll
+          for (int i = 0; i < VEC; ++i) acc[i] = acc[i] + __shfl_xor_sync(0xffffffffu, acc[i], o);
+        }
+        if (q == 0) {
+          const int64_t orow = row_map ? (int64_t)row_map[B.row] : B.row;
+          VecStore<YT, VEC>::store(Y + orow * (ROWB / 2) + lq * VEC, acc);
+        }
+      }
+    }
+    B = C;
+    vB = vC;
+    C = D;
+    jC = jD;
+    vC = vD;
+    st ^= 1;
+  }
+  cp_async_wait_group<0>();
 }
 
 // Persistent grid size: resident blocks per SM (from the occupancy
@@ -1101,6 +1229,39 @@ void launch_flow(const SpmmArgs& a, int U, cudaStream_t s) {
   throw Error(kErrInvalidArgument, "the flat-stream SpMM needs 128-, 256- or 512-byte rows");
 }
 
+// kind 9: pipelined split-chain kernel (16-bit storage); stage: 0 = plain fma, 1 = mixed-precision fma
+template <class VT, class XT, class YT, int ROWB, bool MIXED>
+void launch_split_pipe_r(const SpmmArgs& a, cudaStream_t s) {
+  auto kern = k_spmm_split_pipe<VT, XT, YT, ROWB, MIXED>;
+  constexpr int smem = split_pipe_smem<ROWB>();
+  constexpr int nt = 32 * split_pipe_warps<ROWB>();
+  SCL_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+  SCL_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                (int)cudaSharedmemCarveoutMaxShared));
+  int dev = 0, per_sm = 0;
+  SCL_CUDA(cudaGetDevice(&dev));
+  SCL_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, nt, smem));
+  const int64_t need = (a.n_rows * 32 + nt - 1) / nt;
+  const int64_t grid = std::max<int64_t>(1, std::min<int64_t>(need, (int64_t)std::max(per_sm, 1) * sm_count(dev)));
+  kern<<<(unsigned)grid, nt, smem, s>>>(a.indptr, a.indices, static_cast<const VT*>(a.values),
+                                        static_cast<const XT*>(a.X), static_cast<YT*>(a.Y), a.row_map, a.n_rows);
+  SCL_CUDA(cudaGetLastError());
+}
+
+template <class VT, class XT, class YT>
+void launch_split_pipe(const SpmmArgs& a, int mixed, cudaStream_t s) {
+  const int64_t rowb = a.F * (int64_t)sizeof(XT);
+  if (rowb == 128) {
+    if (mixed) return launch_split_pipe_r<VT, XT, YT, 128, true>(a, s);
+    return launch_split_pipe_r<VT, XT, YT, 128, false>(a, s);
+  }
+  if (rowb == 256) {
+    if (mixed) return launch_split_pipe_r<VT, XT, YT, 256, true>(a, s);
+    return launch_split_pipe_r<VT, XT, YT, 256, false>(a, s);
+  }
+  throw Error(kErrInvalidArgument, "the pipelined split-chain SpMM needs 128- or 256-byte rows");
+}
+
 // kinds 5/6: split-chain kernel for 16-bit storage (6 = mixed-precision fma);
 // stage = gathers per lane per batch (U * chains must divide 32)
 template <class VT, class XT, class YT, int ROWB, int U, bool MIXED>
@@ -1173,6 +1334,14 @@ void launch_typed(const SpmmArgs& a, const SpmmPlan& plan, cudaStream_t s) {
                 "the flat-stream SpMM covers a row with one chunk per lane of a warp");
     return launch_flow<VT, XT, YT, AT>(a, plan.stage, s);
   }
+  if (plan.kind == 9) {
+    SCL_REQUIRE(plan.vec == kVec && (int64_t)plan.group * kVec == a.F && (plan.stage == 0 || plan.stage == 1),
+                kErrInvalidArgument, "the pipelined split-chain SpMM covers a row with one 16-byte chunk per lane");
+    if constexpr (sizeof(XT) == 2 && sizeof(VT) == 2 && sizeof(AT) == 4) {
+      return launch_split_pipe<VT, XT, YT>(a, plan.stage, s);
+    }
+    throw Error(kErrInvalidArgument, "the pipelined split-chain SpMM is for bf16 or f16 storage");
+  }
   if (plan.kind == 5 || plan.kind == 6) {
     SCL_REQUIRE(plan.vec == kVec && (int64_t)plan.group * kVec == a.F, kErrInvalidArgument,
                 "the split-chain SpMM covers a row with one 16-byte chunk per lane of a group");
@@ -1224,10 +1393,12 @@ SpmmPlan default_spmm_plan(int64_t F, DType xtype, const void* X, const void* Y,
       (reinterpret_cast<uintptr_t>(Y) % (uintptr_t)(8 * ys)) == 0) {
     // 16-bit storage: one 16-byte chunk per lane, 4 (128-byte rows) or 2
     // (256-byte rows) entries per load instruction, mixed-precision fma
+    // (measured at 500k cells: 128-byte rows fastest with 2 gathers per lane
+    // per batch; 256-byte rows with the cp.async pipeline)
     p.group = (int)(rb / 16);
     p.vec = 8;
-    p.kind = 6;
-    p.stage = (rb == 128) ? 4 : 8;
+    p.kind = (rb == 128) ? 6 : 9;
+    p.stage = (rb == 128) ? 2 : 1;
     return p;
   }
   if (rb == 128 || rb == 256 || rb == 512) {
@@ -1259,12 +1430,42 @@ SpmmPlan default_spmm_plan(int64_t F, DType xtype, const void* X, const void* Y,
   return p;
 }
 
+std::vector<SpmmPlan> candidate_plans(int64_t F, DType xtype, const void* X, const void* Y, DType ytype) {
+  const SpmmPlan d = default_spmm_plan(F, xtype, X, Y, ytype);
+  std::vector<SpmmPlan> c{d};
+  auto add = [&](int group, int vec, int kind, int stage) {
+    SpmmPlan p;
+    p.group = group;
+    p.vec = vec;
+    p.kind = kind;
+    p.stage = stage;
+    c.push_back(p);
+  };
+  if (d.kind == 5 || d.kind == 6 || d.kind == 9) {
+    // interleaved-chain family (16-bit storage): same bits for every member
+    const int rb = (int)(F * (int64_t)dtype_size(xtype));
+    const int group = rb / 16;
+    const int stages128[] = {2, 4, 8}, stages256[] = {4, 8, 16};
+    for (int st : (rb == 128 ? stages128 : stages256)) {
+      add(group, 8, 6, st);
+      add(group, 8, 5, st);
+    }
+    add(group, 8, 9, 1);
+  } else if (d.kind == 4) {
+    // sequential-chain family, fixed row pitch
+    for (int st : {8, 16, 32}) add(32, d.vec, 4, st);
+    for (int st : {8, 16}) add(32, d.vec, 7, st);
+  }
+  return c;
+}
+
 void spmm_with_plan(const SpmmArgs& a, const SpmmPlan& plan, cudaStream_t s) {
   if (a.n_rows <= 0 || a.F <= 0) return;
   SCL_REQUIRE(plan.group >= 1 && plan.group <= 32 && (plan.group & (plan.group - 1)) == 0, kErrInvalidArgument,
               "lane-group size must be a power of two in [1, 32]");
   SCL_REQUIRE(plan.kind == 0 || plan.kind == 2 || plan.kind == 3 || plan.kind == 4 || plan.kind == 5 ||
-                  plan.kind == 6 || plan.kind == 7 || (plan.kind == 1 && plan.vec > 1 && plan.group >= 4),
+                  plan.kind == 6 || plan.kind == 7 || plan.kind == 9 ||
+                  (plan.kind == 1 && plan.vec > 1 && plan.group >= 4),
               kErrInvalidArgument, "the pipelined SpMM needs 16-byte lane chunks and a lane group of at least 4");
   if (plan.vec > 1) {
     const int xs = (int)dtype_size(a.xtype), ys = (int)dtype_size(a.ytype);

@@ -140,6 +140,23 @@ class GpuGraph:
                     self._lib)
         return perm, rounds.value
 
+    def autotune(self, n_features: int, reps: int = 3, stream=None) -> dict:
+        """Pick the fastest bit-identical launch shape for this width and storage dtype."""
+        k, st, ms = ctypes.c_int(), ctypes.c_int(), ctypes.c_double()
+        check_error(self._lib.scl_gpu_graph_autotune(self._h, int(n_features), int(reps), ctypes.byref(k),
+                                                     ctypes.byref(st), ctypes.byref(ms), _stream_ptr(stream)),
+                    "autotune", self._lib)
+        return {"kind": k.value, "stage": st.value, "ms": ms.value}
+
+    def gather_floor(self, n_features: int, dtype=None, reps: int = 5, stream=None) -> float:
+        """Median ms of gathering one n_features-wide row per stored entry in
+        diffusion order (the memory-system floor of one SpMM step)."""
+        code = F32 if dtype is None else (dtype if isinstance(dtype, int) else dtype_code(dtype))
+        ms = ctypes.c_double()
+        check_error(self._lib.scl_gpu_graph_gather_floor(self._h, int(n_features), code, int(reps), ctypes.byref(ms),
+                                                         _stream_ptr(stream)), "gather_floor", self._lib)
+        return ms.value
+
     def export(self, master_dtype=np.float32):
         """(indptr int64, indices int32, values) as host NumPy arrays."""
         n, _, nnz = self.shape

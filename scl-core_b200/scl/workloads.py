@@ -1,11 +1,14 @@
 """Synthetic diffusion workloads on the device (benchmark and profiling cases).
 
     python -m scl.workloads spmm --cells 200000 --k 30 --features 64 --steps 3 [--storage bf16] [--no-reorder]
+    python -m scl.workloads backward --cells 200000 --k 30 --features 32 --steps 8 --every 4
 
 builds the seeded mixture graph on the current GPU (kNN with torch as an input
 generator, then this library's weights / symmetrisation / normalisation /
-reordering) and runs `steps` diffusion steps through scl_gpu_diffuse — the
-case the ncu captures under profiles/ were taken on.
+reordering) and runs `steps` diffusion steps through scl_gpu_diffuse (spmm),
+or a checkpointed forward plus the backward pass of L = sum((X_T - Y)^2)
+through scl_gpu_diffuse_checkpointed / scl_gpu_diffuse_backward (backward) —
+the cases the ncu captures under profiles/ were taken on.
 """
 from __future__ import annotations
 
@@ -43,7 +46,8 @@ def _main():
     import torch
 
     ap = argparse.ArgumentParser()
-    ap.add_argument("case", choices=["spmm"])
+    ap.add_argument("case", choices=["spmm", "backward"])
+    ap.add_argument("--every", type=int, default=4)
     ap.add_argument("--cells", type=int, default=200_000)
     ap.add_argument("--k", type=int, default=30)
     ap.add_argument("--features", type=int, default=64)
@@ -52,6 +56,18 @@ def _main():
     ap.add_argument("--no-reorder", action="store_true")
     ap.add_argument("--plan", default="", help="group,vec,kind,stage launch shape for diffuse (default: built-in)")
     a = ap.parse_args()
+    if a.case == "backward":
+        g, _, _, tm = build_graph(a.cells, a.k, reorder=False)
+        gen = torch.Generator(device="cuda").manual_seed(7)
+        X0 = torch.randn((a.cells, a.features), device="cuda", generator=gen)
+        Yt = torch.randn((a.cells, a.features), device="cuda", generator=gen)
+        XT, ck = g.diffuse_checkpointed(X0, a.steps, a.every)
+        dX, dW = g.diffuse_backward(X0, ck, 2.0 * (XT - Yt), a.steps, a.every)
+        torch.cuda.synchronize()
+        n, _, nnz = g.shape
+        print(f"cells={n} nnz={nnz} features={a.features} steps={a.steps} every={a.every} "
+              f"loss={float(((XT - Yt) ** 2).sum()):.6e} |dX|={float(dX.norm()):.6e} |dW|={float(dW.norm()):.6e}")
+        return
     g, _, _, tm = build_graph(a.cells, a.k, reorder=not a.no_reorder)
     if a.storage != "f32":
         g.set_storage(torch.bfloat16 if a.storage == "bf16" else torch.float16)

@@ -207,6 +207,16 @@ def test_skewed_and_empty_rows():
                 Y = torch.empty_like(Xd)
                 g.spmm(Xd, Y, group=32, vec=vec, kind=kind, stage=stage)
                 np.testing.assert_array_equal(bits(Y.cpu().numpy()), bits(ref1))
+        # 16-bit storage kernels (interleaved chains) on the same rows
+        g.set_storage(torch.bfloat16)
+        for F, group in ((64, 8), (128, 16)):
+            X0 = rng.standard_normal((n, F)).astype(np.float32)
+            Xd = torch.from_numpy(X0).cuda().to(torch.bfloat16)
+            ref1 = port.diffuse_lowp_chains(ip, ind, P, Xd.float().cpu().numpy(), 1, port.BF16, 32 // group, True)
+            for kind, stage in ((5, 4), (6, 4), (9, 0), (9, 1)):
+                Y = torch.empty((n, F), dtype=torch.float32, device="cuda")
+                g.spmm(Xd, Y, group=group, vec=8, kind=kind, stage=stage)
+                np.testing.assert_array_equal(bits(Y.cpu().numpy()), bits(ref1))
     finally:
         g.close()
 
@@ -413,12 +423,37 @@ def test_split_chain_shapes_are_exact(graph_3k, storage, F):
         chains = 32 // group
         ref1 = port.diffuse_lowp_chains(ip, ind, P, Xd.float().cpu().numpy(), 1, kind_code, chains, True)
         stages = (2, 4, 8) if group == 8 else (4, 8, 16)
-        for kind in (5, 6):
-            for stage in stages:
-                Y = torch.empty((n, F), dtype=torch.float32, device="cuda")
-                g.spmm(Xd, Y, group=group, vec=8, kind=kind, stage=stage)
-                np.testing.assert_array_equal(bits(Y.cpu().numpy()), bits(ref1))
+        shapes = [(k, st) for k in (5, 6) for st in stages] + [(9, 0), (9, 1)]
+        for kind, stage in shapes:
+            Y = torch.empty((n, F), dtype=torch.float32, device="cuda")
+            g.spmm(Xd, Y, group=group, vec=8, kind=kind, stage=stage)
+            np.testing.assert_array_equal(bits(Y.cpu().numpy()), bits(ref1))
         Yd = g.diffuse(Xd, 3, out_dtype=torch.float32).cpu().numpy()
         np.testing.assert_array_equal(bits(Yd), bits(port.diffuse_lowp_chains(ip, ind, P, X0, 3, kind_code, chains)))
+    finally:
+        g.close()
+
+
+@pytest.mark.parametrize("storage", ["f32", "bf16"])
+def test_autotune_keeps_the_bits(graph_3k, storage):
+    """The autotuner only picks among launch shapes of the default kernel's
+    family, so diffusion results are bit-identical before and after it."""
+    import torch
+
+    _, _, ip, ind, W = graph_3k
+    n = ip.size - 1
+    P = port.transition(ip, ind, W.astype(np.float32), False, True)
+    g = scl.gpu.GpuGraph.from_csr(ip, ind.astype(np.int32), P, (n, n))
+    try:
+        g.reorder(1)
+        if storage == "bf16":
+            g.set_storage(torch.bfloat16)
+        X0 = torch.from_numpy(np.random.default_rng(2).standard_normal((n, 64)).astype(np.float32)).cuda()
+        before = g.diffuse(X0, 4, out_dtype=torch.float32)
+        res = g.autotune(64, reps=2)
+        assert res["ms"] > 0 and res["kind"] in (4, 5, 6, 7, 9)
+        after = g.diffuse(X0, 4, out_dtype=torch.float32)
+        assert torch.equal(before, after)
+        assert g.gather_floor(64, reps=2) > 0
     finally:
         g.close()

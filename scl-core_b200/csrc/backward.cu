@@ -27,7 +27,10 @@
 //   k_adj_quarter  the same step for rows of 1, 2 or 4 blocks of eight 16-byte
 //               chunks: one load instruction gathers 4 entries (4 interleaved
 //               chains of G_s[i], summed pairwise at the row end), partial
-//               dots reduced within a quarter-warp (7 shuffles per 8 entries).
+//               dots reduced within a quarter-warp (7 shuffles per 8 entries);
+//               prefetch pipeline as in the forward row kernel. On a
+//               structurally symmetric graph the pass also recomputes one
+//               forward iterate of the previous segment (FUSE).
 // Checkpointing: the forward stores X_s for s = every, 2*every, ... < T (and,
 // with keep_last, the last segment's iterates); the backward recomputes every
 // other iterate of a segment from its checkpoint with the forward SpMM (the
@@ -110,7 +113,7 @@ template <class T, int VEC, int U>
 __global__ void __launch_bounds__(256)
 k_adj_step(const int64_t* __restrict__ tptr, const int32_t* __restrict__ tidx, const T* __restrict__ tval,
            const T* __restrict__ G1, const T* __restrict__ Xs, T* __restrict__ G0, T* __restrict__ gPt, int64_t n,
-           int64_t F) {
+           int64_t F, int gp_accum) {
   static_assert(32 % U == 0, "batch must divide 32");
   const int lane = threadIdx.x & 31;
   const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
@@ -170,7 +173,8 @@ k_adj_step(const int64_t* __restrict__ tptr, const int32_t* __restrict__ tidx, c
         }
         if (gPt != nullptr) {
           const T tot = transpose_reduce32<T>(p, lane);
-          if (lane < cnt) gPt[m] += tot;
+          // the first backward step overwrites (its first column block) instead of accumulating
+          if (lane < cnt) gPt[m] = ((gp_accum || c0 > 0) ? gPt[m] : T(0)) + tot;
         }
       }
       if (active) store_vec<T, VEC>(G0 + row * F + col, acc);
@@ -198,11 +202,17 @@ __device__ __forceinline__ void tr_round(T (&p)[8], int lq) {
   }
 }
 
-template <class T, int NCB, int U>
-__global__ void __launch_bounds__(256, (NCB == 1 && sizeof(T) == 4) ? 3 : 2)
+// FUSE (structurally symmetric graphs, whose P and P^T share indptr/indices):
+// the same pass also recomputes one forward iterate Xnew = P Xprev — a second
+// value stream pval (P in the same entry order) and a second gather stream,
+// 4 interleaved chains summed like G_s's — so a recompute step rides along
+// with a backward step instead of running as its own launch.
+template <class T, int NCB, int U, bool FUSE>
+__global__ void __launch_bounds__(256, (NCB == 1 && sizeof(T) == 4 && !FUSE) ? 3 : 2)
 k_adj_quarter(const int64_t* __restrict__ tptr, const int32_t* __restrict__ tidx, const T* __restrict__ tval,
               const T* __restrict__ G1, const T* __restrict__ Xs, T* __restrict__ G0, T* __restrict__ gPt,
-              int64_t n) {
+              int64_t n, const T* __restrict__ pval, const T* __restrict__ Xprev, T* __restrict__ Xnew,
+              int gp_accum) {
   constexpr int VEC = 16 / (int)sizeof(T);
   constexpr int CB = 8 * VEC;      // columns per block
   constexpr int F = NCB * CB;
@@ -210,25 +220,65 @@ k_adj_quarter(const int64_t* __restrict__ tptr, const int32_t* __restrict__ tidx
   static_assert(U == 4 || U == 8, "batch of 4 or 8 gathers per lane");
   const int lane = threadIdx.x & 31;
   const int q = lane >> 3, lq = lane & 7;
+  const int e_own = lq * 4 + q;    // chunk entry whose dot this lane finishes
   const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
-  for (int64_t row = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; row < n; row += nw) {
-    const int64_t start = tptr[row], end = tptr[row + 1];
-    T xi[NCB][VEC], acc[NCB][VEC];
+  int64_t row = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  if (row >= n) return;
+  // Prefetch pipeline (as in the forward row kernel): bounds two rows ahead,
+  // the next chunk's (index, value) pairs one chunk ahead, the next row's
+  // X_s chunk one row ahead, each chunk's accumulator values at its start.
+  int64_t s_cur = tptr[row], e_cur = tptr[row + 1];
+  int64_t s_nx = 0, e_nx = 0;
+  if (row + nw < n) {
+    s_nx = tptr[row + nw];
+    e_nx = tptr[row + nw + 1];
+  }
+  auto fetch = [&](int64_t pos, int64_t end, int32_t& j, T& v, T& v2) {
+    j = 0;
+    v = T(0);
+    v2 = T(0);
+    if (pos < end) {
+      j = __ldcs(tidx + pos);
+      v = __ldcs(tval + pos);
+      if constexpr (FUSE) v2 = __ldcs(pval + pos);
+    }
+  };
+  T xi[NCB][VEC], xn[NCB][VEC];
+#pragma unroll
+  for (int c = 0; c < NCB; ++c) {
+    load_vec<T, VEC>(Xs + row * F + c * CB + lq * VEC, xi[c]);
+#pragma unroll
+    for (int i = 0; i < VEC; ++i) xn[c][i] = T(0);
+    if (row + nw < n) load_vec<T, VEC>(Xs + (row + nw) * F + c * CB + lq * VEC, xn[c]);
+  }
+  int32_t j_c;
+  T v_c, w_c;
+  fetch(s_cur + lane, e_cur, j_c, v_c, w_c);
+  for (; row < n; row += nw) {
+    const int64_t nn = row + 2 * nw;
+    int64_t s_nn = 0, e_nn = 0;
+    if (nn < n) {
+      s_nn = tptr[nn];
+      e_nn = tptr[nn + 1];
+    }
+    T acc[NCB][VEC], accf[NCB][VEC];
 #pragma unroll
     for (int c = 0; c < NCB; ++c) {
-      load_vec<T, VEC>(Xs + row * F + c * CB + lq * VEC, xi[c]);
 #pragma unroll
-      for (int i = 0; i < VEC; ++i) acc[c][i] = T(0);
-    }
-    for (int64_t base = start; base < end; base += 32) {
-      const int64_t m = base + lane;
-      int32_t j_l = 0;
-      T v_l = T(0);
-      if (m < end) {
-        j_l = __ldcs(tidx + m);
-        v_l = __ldcs(tval + m);
+      for (int i = 0; i < VEC; ++i) {
+        acc[c][i] = T(0);
+        accf[c][i] = T(0);
       }
-      const int cnt = (int)((end - base) < 32 ? (end - base) : 32);
+    }
+    const int len = (int)(e_cur - s_cur);
+    for (int base = 0; base < len; base += 32) {
+      int32_t j_n;
+      T v_n, w_n;
+      if (base + 32 < len) fetch(s_cur + base + 32 + lane, e_cur, j_n, v_n, w_n);
+      else fetch(s_nx + lane, e_nx, j_n, v_n, w_n);
+      const int cnt = (len - base) < 32 ? (len - base) : 32;
+      T old = T(0);  // the first backward step overwrites the accumulator (no memset)
+      if (gPt != nullptr && gp_accum && e_own < cnt) old = gPt[s_cur + base + e_own];
       T p[8];
 #pragma unroll
       for (int u = 0; u < 8; ++u) p[u] = T(0);
@@ -238,21 +288,26 @@ k_adj_quarter(const int64_t* __restrict__ tptr, const int32_t* __restrict__ tidx
 #pragma unroll
           for (int c = 0; c < NCB; ++c) {
             T g[U][VEC];
+            T gx[FUSE ? U : 1][VEC];
 #pragma unroll
             for (int u = 0; u < U; ++u) {
               const int e = (b * U + u) * 4 + q;
-              const int32_t jj = __shfl_sync(0xffffffffu, j_l, e);
+              const int32_t jj = __shfl_sync(0xffffffffu, j_c, e);
               if (e < cnt) {
                 load_vec<T, VEC>(G1 + (int64_t)jj * F + c * CB + lq * VEC, g[u]);
+                if constexpr (FUSE) load_vec<T, VEC>(Xprev + (int64_t)jj * F + c * CB + lq * VEC, gx[u]);
               } else {
 #pragma unroll
-                for (int i = 0; i < VEC; ++i) g[u][i] = T(0);
+                for (int i = 0; i < VEC; ++i) {
+                  g[u][i] = T(0);
+                  if constexpr (FUSE) gx[u][i] = T(0);
+                }
               }
             }
 #pragma unroll
             for (int u = 0; u < U; ++u) {
               const int e = (b * U + u) * 4 + q;
-              const T vv = __shfl_sync(0xffffffffu, v_l, e);
+              const T vv = __shfl_sync(0xffffffffu, v_c, e);
               T d = p[b * U + u];
 #pragma unroll
               for (int i = 0; i < VEC; ++i) d = fma_t(g[u][i], xi[c][i], d);
@@ -260,6 +315,13 @@ k_adj_quarter(const int64_t* __restrict__ tptr, const int32_t* __restrict__ tidx
               if (e < cnt) {
 #pragma unroll
                 for (int i = 0; i < VEC; ++i) acc[c][i] = fma_t(vv, g[u][i], acc[c][i]);
+              }
+              if constexpr (FUSE) {
+                const T ww = __shfl_sync(0xffffffffu, w_c, e);
+                if (e < cnt) {
+#pragma unroll
+                  for (int i = 0; i < VEC; ++i) accf[c][i] = fma_t(ww, gx[u][i], accf[c][i]);
+                }
               }
             }
           }
@@ -269,10 +331,13 @@ k_adj_quarter(const int64_t* __restrict__ tptr, const int32_t* __restrict__ tidx
         tr_round<4>(p, lq);
         tr_round<2>(p, lq);
         tr_round<1>(p, lq);
-        const int e = lq * 4 + q;
-        if (e < cnt) gPt[base + e] += p[0];
+        if (e_own < cnt) gPt[s_cur + base + e_own] = old + p[0];
       }
+      j_c = j_n;
+      v_c = v_n;
+      w_c = w_n;
     }
+    if (len == 0) fetch(s_nx + lane, e_nx, j_c, v_c, w_c);  // nothing was prefetched for the next row
 #pragma unroll
     for (int c = 0; c < NCB; ++c) {
 #pragma unroll
@@ -281,7 +346,75 @@ k_adj_quarter(const int64_t* __restrict__ tptr, const int32_t* __restrict__ tidx
         acc[c][i] = acc[c][i] + __shfl_xor_sync(0xffffffffu, acc[c][i], 16);
       }
       if (q == 0) store_vec<T, VEC>(G0 + row * F + c * CB + lq * VEC, acc[c]);
+      if constexpr (FUSE) {
+#pragma unroll
+        for (int i = 0; i < VEC; ++i) {
+          accf[c][i] = accf[c][i] + __shfl_xor_sync(0xffffffffu, accf[c][i], 8);
+          accf[c][i] = accf[c][i] + __shfl_xor_sync(0xffffffffu, accf[c][i], 16);
+        }
+        if (q == 0) store_vec<T, VEC>(Xnew + row * F + c * CB + lq * VEC, accf[c]);
+      }
     }
+    // rotate: next row's X_s chunk is in xn; fetch the one after it
+#pragma unroll
+    for (int c = 0; c < NCB; ++c) {
+#pragma unroll
+      for (int i = 0; i < VEC; ++i) xi[c][i] = xn[c][i];
+      if (nn < n) load_vec<T, VEC>(Xs + nn * F + c * CB + lq * VEC, xn[c]);
+    }
+    s_cur = s_nx;
+    e_cur = e_nx;
+    s_nx = s_nn;
+    e_nx = e_nn;
+  }
+}
+
+// flag[0] = 1 when a and b (count entries) differ anywhere
+template <class I>
+__global__ void k_differ(const I* __restrict__ a, const I* __restrict__ b, int64_t count, int32_t* __restrict__ flag) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < count; i += (int64_t)gridDim.x * blockDim.x)
+    if (a[i] != b[i]) flag[0] = 1;
+}
+
+__global__ void k_invert_map(const int32_t* __restrict__ map, int64_t nnz, int32_t* __restrict__ inv) {
+  for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < nnz; q += (int64_t)gridDim.x * blockDim.x)
+    inv[map[q]] = (int32_t)q;
+}
+
+// Normalisation backward in one pass over P's rows (warp per row): gP of
+// entry p is read from the CSC-order accumulator through the inverse map, u_i
+// is reduced in FP64, then every entry's dW is written; v (symmetric mode) is
+// the CSC row dot computed beforehand.
+template <class T>
+__global__ void k_norm_bwd_gather(const int64_t* __restrict__ ptr, const int32_t* __restrict__ idx,
+                                  const T* __restrict__ P, const T* __restrict__ gPt, const int32_t* __restrict__ inv,
+                                  const double* __restrict__ deg, const double* __restrict__ v, int64_t n,
+                                  int symmetric, T* __restrict__ dW) {
+  const int64_t row = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (row >= n) return;
+  const int64_t s0 = ptr[row], s1 = ptr[row + 1];
+  double u = 0.0;
+  for (int64_t p = s0 + lane; p < s1; p += 32) u += (double)gPt[inv[p]] * (double)P[p];
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) u += __shfl_xor_sync(0xffffffffu, u, o);
+  const double di = deg[row];
+  const bool live = di > kMinProbB;
+  const double ai = live ? 1.0 / sqrt(di) : 0.0;
+  const double shift = live ? (symmetric ? (u + v[row]) / (2.0 * di) : u) : 0.0;
+  for (int64_t p = s0 + lane; p < s1; p += 32) {
+    double r = 0.0;
+    if (live) {
+      const double gp = (double)gPt[inv[p]];
+      if (symmetric) {
+        const double dj = deg[idx[p]];
+        const double aj = dj > kMinProbB ? 1.0 / sqrt(dj) : 0.0;
+        r = gp * ai * aj - shift;
+      } else {
+        r = (gp - shift) / di;
+      }
+    }
+    dW[p] = (T)r;
   }
 }
 
@@ -313,34 +446,8 @@ __global__ void k_row_dot(const int64_t* __restrict__ ptr, const T* __restrict__
   if (lane == 0) out[row] = s;
 }
 
-template <class T>
-__global__ void k_norm_bwd(const int64_t* __restrict__ ptr, const int32_t* __restrict__ idx,
-                           const T* __restrict__ gP, const double* __restrict__ deg, const double* __restrict__ u,
-                           const double* __restrict__ v, int64_t n, int symmetric, T* __restrict__ dW) {
-  const int64_t row = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
-  const int lane = threadIdx.x & 31;
-  if (row >= n) return;
-  const double di = deg[row];
-  const bool live = di > kMinProbB;
-  const double ai = live ? 1.0 / sqrt(di) : 0.0;
-  const double shift = live ? (symmetric ? (u[row] + v[row]) / (2.0 * di) : u[row]) : 0.0;
-  for (int64_t p = ptr[row] + lane, e = ptr[row + 1]; p < e; p += 32) {
-    double r = 0.0;
-    if (live) {
-      if (symmetric) {
-        const double dj = deg[idx[p]];
-        const double aj = dj > kMinProbB ? 1.0 / sqrt(dj) : 0.0;
-        r = (double)gP[p] * ai * aj - shift;
-      } else {
-        r = ((double)gP[p] - shift) / di;
-      }
-    }
-    dW[p] = (T)r;
-  }
-}
-
 template <class T, int VEC, int U>
-void launch_adj(const CsrView& t, const T* G1, const T* Xs, T* G0, T* gPt, int64_t F, cudaStream_t s) {
+void launch_adj(const CsrView& t, const T* G1, const T* Xs, T* G0, T* gPt, int gp_accum, int64_t F, cudaStream_t s) {
   auto kern = k_adj_step<T, VEC, U>;
   int dev = 0, per_sm = 0;
   SCL_CUDA(cudaGetDevice(&dev));
@@ -348,42 +455,58 @@ void launch_adj(const CsrView& t, const T* G1, const T* Xs, T* G0, T* gPt, int64
   const int64_t need = (t.n_rows * 32 + 255) / 256;
   const int64_t grid = std::max<int64_t>(1, std::min<int64_t>(need, (int64_t)std::max(per_sm, 1) * sm_count(dev)));
   kern<<<(unsigned)grid, 256, 0, s>>>(t.indptr, t.indices, static_cast<const T*>(t.values), G1, Xs, G0, gPt,
-                                      t.n_rows, F);
+                                      t.n_rows, F, gp_accum);
   SCL_CUDA(cudaGetLastError());
 }
 
-template <class T, int NCB, int U>
-void launch_adj_quarter(const CsrView& t, const T* G1, const T* Xs, T* G0, T* gPt, cudaStream_t s) {
-  auto kern = k_adj_quarter<T, NCB, U>;
+template <class T, int NCB, int U, bool FUSE = false>
+void launch_adj_quarter(const CsrView& t, const T* G1, const T* Xs, T* G0, T* gPt, int gp_accum, cudaStream_t s,
+                        const T* pval = nullptr, const T* Xprev = nullptr, T* Xnew = nullptr) {
+  auto kern = k_adj_quarter<T, NCB, U, FUSE>;
   int dev = 0, per_sm = 0;
   SCL_CUDA(cudaGetDevice(&dev));
   SCL_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, 256, 0));
   const int64_t need = (t.n_rows * 32 + 255) / 256;
   const int64_t grid = std::max<int64_t>(1, std::min<int64_t>(need, (int64_t)std::max(per_sm, 1) * sm_count(dev)));
   kern<<<(unsigned)grid, 256, 0, s>>>(t.indptr, t.indices, static_cast<const T*>(t.values), G1, Xs, G0, gPt,
-                                      t.n_rows);
+                                      t.n_rows, pval, Xprev, Xnew, gp_accum);
   SCL_CUDA(cudaGetLastError());
 }
 
+// Whether the fused step (backward + one forward recompute) covers this width.
 template <class T>
-void adj_step(const CsrView& t, const T* G1, const T* Xs, T* G0, T* gPt, int64_t F, cudaStream_t s) {
+bool adj_fusable(int64_t F, const void* a, const void* b, const void* c, const void* d, const void* e) {
+  constexpr int kV16 = 16 / (int)sizeof(T);
+  for (const void* p : {a, b, c, d, e})
+    if ((reinterpret_cast<uintptr_t>(p) & 15u) != 0) return false;
+  return F == 8 * kV16;
+}
+
+template <class T>
+void adj_step_fused(const CsrView& t, const T* pval, const T* G1, const T* Xs, T* G0, T* gPt, int gp_accum,
+                    const T* Xprev, T* Xnew, cudaStream_t s) {
+  launch_adj_quarter<T, 1, 4, true>(t, G1, Xs, G0, gPt, gp_accum, s, pval, Xprev, Xnew);
+}
+
+template <class T>
+void adj_step(const CsrView& t, const T* G1, const T* Xs, T* G0, T* gPt, int gp_accum, int64_t F, cudaStream_t s) {
   constexpr int kV16 = 16 / (int)sizeof(T);
   const auto al = [&](const void* p, int b) { return (reinterpret_cast<uintptr_t>(p) % (uintptr_t)b) == 0; };
   // quarter-warp kernel: rows of 1, 2 or 4 blocks of 8 sixteen-byte chunks
   if (al(G1, 16) && al(Xs, 16) && al(G0, 16)) {
-    if (F == 8 * kV16) return launch_adj_quarter<T, 1, 8>(t, G1, Xs, G0, gPt, s);
-    if (F == 16 * kV16) return launch_adj_quarter<T, 2, 4>(t, G1, Xs, G0, gPt, s);
-    if (F == 32 * kV16) return launch_adj_quarter<T, 4, 4>(t, G1, Xs, G0, gPt, s);
+    if (F == 8 * kV16) return launch_adj_quarter<T, 1, 4>(t, G1, Xs, G0, gPt, gp_accum, s);
+    if (F == 16 * kV16) return launch_adj_quarter<T, 2, 4>(t, G1, Xs, G0, gPt, gp_accum, s);
+    if (F == 32 * kV16) return launch_adj_quarter<T, 4, 4>(t, G1, Xs, G0, gPt, gp_accum, s);
   }
   // one 16-byte chunk per lane when the row fits one column block of the warp
   if (F % kV16 == 0 && F <= 32 * kV16 && F > 16 * kV16 && al(G1, 16) && al(Xs, 16) && al(G0, 16))
-    return launch_adj<T, kV16, 8>(t, G1, Xs, G0, gPt, F, s);
+    return launch_adj<T, kV16, 8>(t, G1, Xs, G0, gPt, gp_accum, F, s);
   if constexpr (kV16 / 2 > 1) {
     constexpr int kV8 = kV16 / 2;
     if (F % kV8 == 0 && F <= 32 * kV8 && F > 16 * kV8 && al(G1, 8) && al(Xs, 8) && al(G0, 8))
-      return launch_adj<T, kV8, 8>(t, G1, Xs, G0, gPt, F, s);
+      return launch_adj<T, kV8, 8>(t, G1, Xs, G0, gPt, gp_accum, F, s);
   }
-  return launch_adj<T, 1, 8>(t, G1, Xs, G0, gPt, F, s);
+  return launch_adj<T, 1, 8>(t, G1, Xs, G0, gPt, gp_accum, F, s);
 }
 
 }  // namespace
@@ -392,6 +515,32 @@ void adj_step(const CsrView& t, const T* G1, const T* Xs, T* G0, T* gPt, int64_t
 void build_adjoint(const DeviceCSR& g, Adjoint& a, cudaStream_t s) {
   transpose_map(g, a.t, a.tmap, s);
   a.values_ok = false;
+  a.tinv = DevBuf(std::max<int64_t>(g.nnz, 1) * 4, s);
+  if (g.nnz > 0) {
+    k_invert_map<<<std::min<unsigned>(nblk(g.nnz, 256), 148u * 16u), 256, 0, s>>>(a.tmap.as<int32_t>(), g.nnz,
+                                                                                   a.tinv.as<int32_t>());
+    SCL_CUDA(cudaGetLastError());
+  }
+  // a structurally symmetric P (the kNN union graphs) has P^T's structure:
+  // then one pass over it can serve P and P^T together (fused recompute)
+  a.sym_structure = false;
+  if (g.n_rows == g.n_cols) {
+    DevBuf flag(4, s);
+    SCL_CUDA(cudaMemsetAsync(flag.p, 0, 4, s));
+    const unsigned b1 = std::min<unsigned>(nblk(g.n_rows + 1, 256), 148u * 8u);
+    k_differ<int64_t><<<b1, 256, 0, s>>>(g.indptr.as<int64_t>(), a.t.indptr.as<int64_t>(), g.n_rows + 1,
+                                         flag.as<int32_t>());
+    if (g.nnz > 0) {
+      const unsigned b2 = std::min<unsigned>(nblk(g.nnz, 256), 148u * 8u);
+      k_differ<int32_t><<<b2, 256, 0, s>>>(g.indices.as<int32_t>(), a.t.indices.as<int32_t>(), g.nnz,
+                                           flag.as<int32_t>());
+    }
+    SCL_CUDA(cudaGetLastError());
+    int32_t h = 1;
+    SCL_CUDA(cudaMemcpyAsync(&h, flag.p, 4, cudaMemcpyDeviceToHost, s));
+    SCL_CUDA(cudaStreamSynchronize(s));
+    a.sym_structure = (h == 0);
+  }
 }
 
 void adjoint_values(const void* vals, DType t, Adjoint& a, cudaStream_t s) {
@@ -490,14 +639,16 @@ static void backward_typed(const CsrView& g, const Adjoint& adj, const T* X0, co
   const size_t blk = (size_t)n * (size_t)F * sizeof(T);
   const size_t elems = (size_t)n * (size_t)F;
   const CsrView tv = adj.t.view();
-  if (gPt) SCL_CUDA(cudaMemsetAsync(gPt, 0, std::max<int64_t>(g.nnz, 1) * sizeof(T), s));
   if (steps <= 0) {
+    if (gPt) SCL_CUDA(cudaMemsetAsync(gPt, 0, std::max<int64_t>(g.nnz, 1) * sizeof(T), s));
     SCL_CUDA(cudaMemcpyAsync(dX0, dY, blk, cudaMemcpyDeviceToDevice, s));
     return;
   }
+  int gp_accum = 0;  // the first backward step writes the accumulator
   const int64_t seg = std::min<int64_t>(every, steps);
-  // recomputed iterates of a segment (slot 0 of a segment aliases its checkpoint)
-  std::vector<DevBuf> xs(seg);
+  // recomputed iterates: two buffer sets, the segment being walked and the
+  // (earlier) segment being recomputed alongside it
+  std::vector<DevBuf> xs[2] = {std::vector<DevBuf>(seg), std::vector<DevBuf>(seg)};
   DevBuf Ga(blk, s), Gb(blk, s);
   const T* Gcur = dY;
   SpmmArgs a{};
@@ -509,28 +660,65 @@ static void backward_typed(const CsrView& g, const Adjoint& adj, const T* X0, co
   a.F = F;
   a.xtype = g.vtype;
   a.ytype = g.vtype;
-  const int64_t last_c = ((steps - 1) / every) * every;
-  for (int64_t c = last_c; c >= 0; c -= every) {
+  const bool fuse = adj.sym_structure && adj_fusable<T>(F, dY, X0, Ga.p, Gb.p, ckpt ? (const void*)ckpt : X0);
+  // kept iterates of segment c (checkpoint, X0 or keep_last slots); nullptr = to recompute
+  auto kept = [&](int64_t c) {
     const int64_t e = std::min<int64_t>(c + every, steps);
-    std::vector<const T*> X(e - c);
+    std::vector<const T*> X(e - c, nullptr);
     for (int64_t m = c; m < e; ++m) {
-      const int64_t slot = (m == 0) ? -1 : slot_of(m, steps, every, keep_last);
-      if (m == 0) X[0] = X0;
-      else if (slot >= 0) X[m - c] = ckpt + (size_t)slot * elems;
-      else X[m - c] = nullptr;
+      if (m == 0) {
+        X[0] = X0;
+      } else {
+        const int64_t slot = slot_of(m, steps, every, keep_last);
+        if (slot >= 0) X[m - c] = ckpt + (size_t)slot * elems;
+      }
     }
-    for (int64_t m = c + 1; m < e; ++m) {  // recompute what was not kept
-      if (X[m - c] != nullptr) continue;
-      if (!xs[m - c].p) xs[m - c] = DevBuf(blk, s);
-      a.X = X[m - c - 1];
-      a.Y = xs[m - c].p;
-      spmm(a, s);
-      X[m - c] = xs[m - c].as<T>();
-    }
+    return X;
+  };
+  auto recompute = [&](std::vector<const T*>& X, int64_t c, std::vector<DevBuf>& buf, int64_t m) {
+    if (!buf[m - c].p) buf[m - c] = DevBuf(blk, s);
+    a.X = X[m - c - 1];
+    a.Y = buf[m - c].p;
+    spmm(a, s);
+    X[m - c] = buf[m - c].as<T>();
+  };
+  const int64_t last_c = ((steps - 1) / every) * every;
+  std::vector<int64_t> segs;
+  for (int64_t c = last_c; c >= 0; c -= every) segs.push_back(c);
+  std::vector<const T*> X = kept(segs[0]);
+  for (int64_t m = segs[0] + 1; m < std::min<int64_t>(segs[0] + every, steps); ++m)
+    if (X[m - segs[0]] == nullptr) recompute(X, segs[0], xs[0], m);
+  for (size_t k = 0; k < segs.size(); ++k) {
+    const int64_t c = segs[k];
+    const int64_t e = std::min<int64_t>(c + every, steps);
+    const bool has_next = k + 1 < segs.size();
+    const int64_t cn = has_next ? segs[k + 1] : 0;
+    std::vector<const T*> Xn = has_next ? kept(cn) : std::vector<const T*>();
+    std::vector<DevBuf>& bn = xs[(k + 1) & 1];
+    int64_t mn = cn + 1;  // next iterate of segment cn to produce
+    auto advance = [&]() {
+      while (has_next && mn < c && Xn[mn - cn] != nullptr) ++mn;
+    };
+    advance();
     for (int64_t st = e - 1; st >= c; --st) {
       T* Gnext = (st == 0) ? dX0 : ((Gcur == Ga.as<T>()) ? Gb.as<T>() : Ga.as<T>());
-      adj_step<T>(tv, Gcur, X[st - c], Gnext, gPt, F, s);
+      if (fuse && has_next && mn < c) {
+        if (!bn[mn - cn].p) bn[mn - cn] = DevBuf(blk, s);
+        adj_step_fused<T>(tv, static_cast<const T*>(g.values), Gcur, X[st - c], Gnext, gPt, gp_accum,
+                          Xn[mn - cn - 1], bn[mn - cn].as<T>(), s);
+        Xn[mn - cn] = bn[mn - cn].as<T>();
+        ++mn;
+        advance();
+      } else {
+        adj_step<T>(tv, Gcur, X[st - c], Gnext, gPt, gp_accum, F, s);
+      }
+      gp_accum = 1;
       Gcur = Gnext;
+    }
+    if (has_next) {
+      for (int64_t m = cn + 1; m < c; ++m)
+        if (Xn[m - cn] == nullptr) recompute(Xn, cn, bn, m);
+      X = Xn;
     }
   }
 }
@@ -556,16 +744,13 @@ static void norm_bwd_typed(const CsrView& P, const Adjoint& adj, const T* gPt, c
                            T* dW, cudaStream_t s) {
   const int64_t n = P.n_rows, nnz = P.nnz;
   if (nnz == 0) return;
-  DevBuf gP(nnz * sizeof(T), s), u(std::max<int64_t>(n, 1) * 8, s), v(std::max<int64_t>(n, 1) * 8, s);
-  const unsigned b = std::min<unsigned>(nblk(nnz, 256), 148u * 16u);
-  k_scatter_entries<T><<<b, 256, 0, s>>>(gPt, adj.tmap.as<int32_t>(), nnz, gP.as<T>());
-  k_row_dot<T><<<nblk(n * 32, 256), 256, 0, s>>>(P.indptr, gP.as<T>(), static_cast<const T*>(P.values), n,
-                                                 u.as<double>());
-  if (symmetric)
+  DevBuf v(std::max<int64_t>(n, 1) * 8, s);
+  if (symmetric)  // v_i = sum over column i of P of gP * P: a row dot over the CSC view
     k_row_dot<T><<<nblk(n * 32, 256), 256, 0, s>>>(adj.t.indptr.as<int64_t>(), gPt, adj.t.values.as<T>(), n,
                                                    v.as<double>());
-  k_norm_bwd<T><<<nblk(n * 32, 256), 256, 0, s>>>(P.indptr, P.indices, gP.as<T>(), degrees, u.as<double>(),
-                                                  v.as<double>(), n, symmetric, dW);
+  k_norm_bwd_gather<T><<<nblk(n * 32, 256), 256, 0, s>>>(P.indptr, P.indices, static_cast<const T*>(P.values), gPt,
+                                                         adj.tinv.as<int32_t>(), degrees, v.as<double>(), n,
+                                                         symmetric, dW);
   SCL_CUDA(cudaGetLastError());
 }
 

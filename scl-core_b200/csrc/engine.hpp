@@ -230,7 +230,9 @@ void transpose_map(const DeviceCSR& g, DeviceCSR& gt, DevBuf& tmap, cudaStream_t
 struct Adjoint {
   DeviceCSR t;    // P^T: indptr int64[n+1], indices int32[nnz], values vtype[nnz]
   DevBuf tmap;    // int32[nnz]: entry q of P^T is entry tmap[q] of P
+  DevBuf tinv;    // int32[nnz]: entry p of P is entry tinv[p] of P^T
   bool values_ok = false;
+  bool sym_structure = false;  // P^T has P's indptr and indices (P's values need no remap)
 };
 void build_adjoint(const DeviceCSR& g, Adjoint& a, cudaStream_t s);
 void adjoint_values(const void* vals, DType t, Adjoint& a, cudaStream_t s);

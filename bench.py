@@ -423,6 +423,7 @@ def main():
                         "max_rel_err_vs_fp64": float(((Y32.double() - Y64).abs() / Y64.abs().clamp_min(1e-3)).max())}
         for name, tdt in (("bf16", torch.bfloat16), ("f16", torch.float16)):
             g.set_storage(tdt, stream=stream)
+            tuned_l = g.autotune(F, reps=3, stream=stream)  # fastest bit-identical shape for this storage
             Xl = X0.to(tdt)
             Yl = torch.empty((n, F), device=device, dtype=torch.float32)
 
@@ -439,6 +440,7 @@ def main():
                 X64s = g64.diffuse(X64s, 1)
                 step_err.append(float(torch.linalg.norm(Xs.double() - X64s) / torch.linalg.norm(X64s)))
             forms[name] = {"gbs": round(B16 * T / (tl * 1e-3) / 1e9, 2), "ms": round(tl, 4),
+                           "plan": {"kind": tuned_l["kind"], "stage": tuned_l["stage"]},
                            "speedup_vs_f32": round(t_ms / tl, 3), "rel_fro_err_vs_fp64": err,
                            "max_rel_err_vs_fp64": float(((Yl.double() - Y64).abs() / Y64.abs().clamp_min(1e-3)).max()),
                            "per_step_rel_fro_err": [round(e, 7) for e in step_err]}

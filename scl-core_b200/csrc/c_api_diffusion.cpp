@@ -1,6 +1,7 @@
 // Drop-in diffusion C ABI executed on the GPU.
 // Replaces scl/binding/c_api/diffusion.cpp:36-116 and 318-341 (argument
 // checks, defaults and messages kept) with uploads + CUDA kernels.
+#include <functional>
 #include <cstring>
 #include <vector>
 
@@ -42,7 +43,11 @@ thread_local Stats t_stats;
 
 // Host -> device copy of the handle (indptr int64, indices int32, values Real).
 // Rows whose storage is adjacent are copied as one run.
-std::shared_ptr<sclabi::DeviceMirror> upload(const scl_sparse_matrix& m, cudaStream_t s, double& h2d) {
+// `after_copies` (optional) runs once the host->device copies are issued on
+// s, before the validation that waits for them, so the caller can start work
+// on other streams right behind the copies.
+std::shared_ptr<sclabi::DeviceMirror> upload(const scl_sparse_matrix& m, cudaStream_t s, double& h2d,
+                                             const std::function<void()>& after_copies = {}) {
   auto mir = std::make_shared<sclabi::DeviceMirror>();
   mir->device = current_device();
   DeviceCSR& g = mir->g;
@@ -82,6 +87,7 @@ std::shared_ptr<sclabi::DeviceMirror> upload(const scl_sparse_matrix& m, cudaStr
     h2d += (double)run * (sizeof(Real) + sizeof(Index));
     i = j;
   }
+  if (after_copies) after_copies();
   if (idx_tmp.p) convert_indices(idx_tmp.p, sclabi::kIndexDType, g.indices.as<int32_t>(), nnz, s);
   DevStatus st(s);
   validate_csr(g, st.ptr(), s);
@@ -89,9 +95,13 @@ std::shared_ptr<sclabi::DeviceMirror> upload(const scl_sparse_matrix& m, cudaStr
   return mir;
 }
 
-std::shared_ptr<sclabi::DeviceMirror> device_graph(scl_sparse_matrix& m, cudaStream_t s, double& h2d) {
-  if (m.mirror && m.mirror->device == current_device()) return m.mirror;
-  return upload(m, s, h2d);
+std::shared_ptr<sclabi::DeviceMirror> device_graph(scl_sparse_matrix& m, cudaStream_t s, double& h2d,
+                                                   const std::function<void()>& after_copies = {}) {
+  if (m.mirror && m.mirror->device == current_device()) {
+    if (after_copies) after_copies();
+    return m.mirror;
+  }
+  return upload(m, s, h2d, after_copies);
 }
 
 struct EventTimer {
@@ -124,12 +134,36 @@ void diffuse_host_block(scl_sparse_matrix& m, Real* X, Index n_nodes, Index n_fe
               "Diffusion: column indices would address rows beyond n_nodes");
   const int dev = current_device();
   cudaStream_t s = library_stream(dev);
+  cudaStream_t cs = library_copy_stream(dev);
   Stats st;
-  auto mir = device_graph(m, s, st.h2d);
+  // The graph is uploaded on the main stream; the dense block follows on the
+  // copy stream as soon as the graph's copies are issued, so its transfer
+  // overlaps the graph's validation and the locality reordering built on the
+  // main stream; the diffusion waits for both.
   const int64_t total = (int64_t)n_nodes * n_features;
-  DevBuf Xd(total * sizeof(Real), s);
-  SCL_CUDA(cudaMemcpyAsync(Xd.p, X, total * sizeof(Real), cudaMemcpyHostToDevice, s));
-  st.h2d += (double)total * sizeof(Real);
+  DevBuf Xd(total * sizeof(Real), cs);
+  // on every exit (errors included) the copy stream is drained before the
+  // caller's X can be released, and the events are destroyed
+  struct CopyGuard {
+    cudaStream_t s;
+    cudaEvent_t e[2] = {nullptr, nullptr};
+    ~CopyGuard() {
+      cudaStreamSynchronize(s);
+      for (cudaEvent_t x : e)
+        if (x) cudaEventDestroy(x);
+    }
+  } guard{cs};
+  SCL_CUDA(cudaEventCreateWithFlags(&guard.e[0], cudaEventDisableTiming));
+  SCL_CUDA(cudaEventCreateWithFlags(&guard.e[1], cudaEventDisableTiming));
+  cudaEvent_t graph_copied = guard.e[0], x_ready = guard.e[1];
+  auto issue_x = [&]() {  // behind the graph's copies, ahead of its validation
+    SCL_CUDA(cudaEventRecord(graph_copied, s));
+    SCL_CUDA(cudaStreamWaitEvent(cs, graph_copied, 0));
+    SCL_CUDA(cudaMemcpyAsync(Xd.p, X, total * sizeof(Real), cudaMemcpyHostToDevice, cs));
+    st.h2d += (double)total * sizeof(Real);
+    SCL_CUDA(cudaEventRecord(x_ready, cs));
+  };
+  auto mir = device_graph(m, s, st.h2d, issue_x);
   EventTimer tm(s);
   tm.start();
   if (want_reorder(mir->g, n_features, n_steps, sizeof(Real))) {
@@ -138,8 +172,10 @@ void diffuse_host_block(scl_sparse_matrix& m, Real* X, Index n_nodes, Index n_fe
       build_reorder(mir->g.view(), *mir->reo, s);
     }
     if (!mir->reo->values_ok) reorder_values(mir->g.values.p, mir->g.vtype, *mir->reo, s);
+    SCL_CUDA(cudaStreamWaitEvent(s, x_ready, 0));
     diffuse_reordered(*mir->reo, Xd.p, sclabi::kRealDType, Xd.p, sclabi::kRealDType, n_features, n_steps, s);
   } else {
+    SCL_CUDA(cudaStreamWaitEvent(s, x_ready, 0));
     diffuse(mir->g.view(), Xd.p, sclabi::kRealDType, Xd.p, sclabi::kRealDType, sclabi::kRealDType, n_features,
             n_steps, s);
   }
@@ -147,6 +183,7 @@ void diffuse_host_block(scl_sparse_matrix& m, Real* X, Index n_nodes, Index n_fe
   SCL_CUDA(cudaMemcpyAsync(X, Xd.p, total * sizeof(Real), cudaMemcpyDeviceToHost, s));
   st.d2h += (double)total * sizeof(Real);
   SCL_CUDA(cudaStreamSynchronize(s));
+  SCL_CUDA(cudaStreamSynchronize(cs));  // Xd is returned to the pool on the copy stream
   st.device_ms = tm.ms();
   t_stats = st;
 }

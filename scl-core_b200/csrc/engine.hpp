@@ -60,6 +60,7 @@ bool is_float_dtype(DType t);
 // ---------------------------------------------------------------------------
 int current_device();                 // throws kErrFeatureUnavailable without a GPU
 cudaStream_t library_stream(int dev);  // non-blocking stream owned by the engine
+cudaStream_t library_copy_stream(int dev);  // second engine stream, for copies overlapped with work
 void* dev_alloc(size_t bytes, cudaStream_t s);
 void dev_free(void* p, cudaStream_t s);
 int sm_count(int dev);

@@ -95,7 +95,7 @@ SCL_EXPORT scl_error_t scl_gpu_diffuse_noalloc(const int64_t* indptr, const int3
   SCL_API_CHECK_NULL(Y, "Matrix Y is null");
   SCL_API_CHECK(n_rows > 0 && n_features > 0 && n_steps >= 0, SCL_ERROR_INVALID_ARGUMENT,
                 "Dimensions must be positive");
-  SCL_API_CHECK(n_rows * n_features <= kNoAllocMaxElems, SCL_ERROR_INVALID_ARGUMENT,
+  SCL_API_CHECK(n_features <= kNoAllocMaxElems / n_rows, SCL_ERROR_INVALID_ARGUMENT,
                 "n_rows * n_features exceeds the 8,388,608-element scratch array of the no-allocation entry point");
   SCL_API_CHECK(X != Y, SCL_ERROR_INVALID_ARGUMENT, "X and Y must be different buffers");
   SCL_API_TRY

@@ -38,6 +38,7 @@ namespace {
 struct DeviceState {
   bool init = false;
   cudaStream_t stream = nullptr;
+  cudaStream_t copy_stream = nullptr;  // host<->device copies overlapped with work on `stream`
   cudaMemPool_t pool = nullptr;
   int sms = 0;
 };
@@ -53,6 +54,7 @@ DeviceState& state(int dev) {
     SCL_CUDA(cudaGetDevice(&prev));
     SCL_CUDA(cudaSetDevice(dev));
     SCL_CUDA(cudaStreamCreateWithFlags(&st.stream, cudaStreamNonBlocking));
+    SCL_CUDA(cudaStreamCreateWithFlags(&st.copy_stream, cudaStreamNonBlocking));
     cudaMemPoolProps props = {};
     props.allocType = cudaMemAllocationTypePinned;
     props.handleTypes = cudaMemHandleTypeNone;
@@ -84,6 +86,7 @@ int current_device() {
 }
 
 cudaStream_t library_stream(int dev) { return state(dev).stream; }
+cudaStream_t library_copy_stream(int dev) { return state(dev).copy_stream; }
 
 int sm_count(int dev) { return state(dev).sms; }
 

@@ -89,6 +89,7 @@ struct BatchParams {
   const float* values;      // [nnz_total]
   const int64_t* tile_row;  // [2 n_tiles + 2]: first rows at [t], end rows at [n_tiles + 1 + t]
   const int32_t* tile_graph;     // [n_tiles]
+  const int32_t* row_order;      // [n_total]: a tile's rows by decreasing length (positions = the tile's rows)
   const uint32_t* graph_tiles;   // [n_graphs] tiles per graph
   unsigned* done;                // [n_graphs] finished tiles per graph (cumulative over steps)
   unsigned* claim;               // [1] next work item
@@ -105,7 +106,7 @@ struct BatchParams {
 // G lanes per row (rows per warp = 32 / G), VEC floats per lane per pass, U
 // gathers in flight per lane.
 template <int G, int VEC, int U>
-__global__ void __launch_bounds__(kBatchThreads)
+__global__ void __launch_bounds__(kBatchThreads, 3)
 k_batch_diffuse(BatchParams p) {
   __shared__ long long s_item;
   __shared__ int s_go;
@@ -158,8 +159,25 @@ k_batch_diffuse(BatchParams p) {
     float* __restrict__ dst = ((p.steps - 1 - s) & 1) ? p.scratch : p.Y;
     const bool coherent = s > 0;
     const int64_t r0 = p.tile_row[t], r1 = p.tile_row[p.n_tiles + 1 + t];
-    for (int64_t row = r0 + slot; row < r1; row += kSlots) {
-      const int64_t start = p.indptr[row], end = p.indptr[row + 1];
+    // The groups of a warp take consecutive rows of the tile's length order,
+    // so rows processed side by side have about the same length. The next
+    // row's id and bounds, and each row's next chunk of (index, value) pairs,
+    // are fetched one step ahead.
+    int64_t idx = r0 + slot;
+    int64_t row = 0, start = 0, end = 0;
+    if (idx < r1) {
+      row = p.row_order[idx];
+      start = p.indptr[row];
+      end = p.indptr[row + 1];
+    }
+    while (idx < r1) {
+      const int64_t nidx = idx + kSlots;
+      int64_t nrow = 0, nstart = 0, nend = 0;
+      if (nidx < r1) {
+        nrow = p.row_order[nidx];
+        nstart = p.indptr[nrow];
+        nend = p.indptr[nrow + 1];
+      }
       for (int64_t c0 = 0; c0 < F; c0 += CPP) {
         const int64_t col = c0 + (int64_t)lg * VEC;
         const bool active = col < F;
@@ -169,17 +187,29 @@ k_batch_diffuse(BatchParams p) {
         const float* __restrict__ Xc = src + (active ? col : 0);
         // chunks of CH entries: lane lg of the group holds entries lg + G*k
         // (k < K), broadcast by shuffles; U gathers in flight per batch
+        int32_t jl[K];
+        float vl[K];
+#pragma unroll
+        for (int k = 0; k < K; ++k) {
+          const int64_t m = start + lg + (int64_t)G * k;
+          jl[k] = 0;
+          vl[k] = 0.0f;
+          if (m < end) {
+            jl[k] = __ldg(p.indices + m);
+            vl[k] = __ldg(p.values + m);
+          }
+        }
         for (int64_t base = start; base < end; base += CH) {
-          int32_t jl[K];
-          float vl[K];
+          int32_t jn[K];
+          float vn[K];
 #pragma unroll
           for (int k = 0; k < K; ++k) {
-            const int64_t m = base + lg + (int64_t)G * k;
-            jl[k] = 0;
-            vl[k] = 0.0f;
+            const int64_t m = base + CH + lg + (int64_t)G * k;
+            jn[k] = 0;
+            vn[k] = 0.0f;
             if (m < end) {
-              jl[k] = __ldg(p.indices + m);
-              vl[k] = __ldg(p.values + m);
+              jn[k] = __ldg(p.indices + m);
+              vn[k] = __ldg(p.values + m);
             }
           }
           const int cnt = (int)((end - base) < CH ? (end - base) : CH);
@@ -203,9 +233,18 @@ k_batch_diffuse(BatchParams p) {
               }
             }
           }
+#pragma unroll
+          for (int k = 0; k < K; ++k) {
+            jl[k] = jn[k];
+            vl[k] = vn[k];
+          }
         }
         if (active) store_y<VEC>(dst + row * F + col, acc);
       }
+      idx = nidx;
+      row = nrow;
+      start = nstart;
+      end = nend;
     }
     __syncthreads();
     if (threadIdx.x == 0) {
@@ -347,6 +386,17 @@ void BatchSolver::build_tiles(int64_t tile_nnz, cudaStream_t s) {
     }
   }
   n_tiles_ = (int64_t)trow.size();
+  // each tile's rows by decreasing length (stable), for balanced lane groups
+  std::vector<int32_t> rord(n_total_);
+  std::iota(rord.begin(), rord.end(), 0);
+  for (size_t t = 0; t < trow.size(); ++t) {
+    std::stable_sort(rord.begin() + trow[t], rord.begin() + tend[t], [&](int32_t a, int32_t b) {
+      return (h_indptr_[a + 1] - h_indptr_[a]) > (h_indptr_[b + 1] - h_indptr_[b]);
+    });
+  }
+  row_order_ = DevBuf(std::max<int64_t>(n_total_, 1) * 4, s);
+  if (n_total_ > 0)
+    SCL_CUDA(cudaMemcpyAsync(row_order_.p, rord.data(), n_total_ * 4, cudaMemcpyHostToDevice, s));
   // tile_row layout for the kernel: [t] = first row, [t+1] = end row is only
   // valid when tiles are contiguous in row space, which schedule order breaks;
   // store (first, end) interleaved as two arrays instead
@@ -401,6 +451,7 @@ void* BatchSolver::params_for(const float* X0, float* Y, void* storage) const {
   p->values = values_.as<float>();
   p->tile_row = tiles_.as<int64_t>();
   p->tile_graph = tile_graph_.as<int32_t>();
+  p->row_order = row_order_.as<int32_t>();
   p->graph_tiles = graph_tiles_.as<uint32_t>();
   p->done = counters_.as<unsigned>();
   p->claim = counters_.as<unsigned>() + n_graphs_;

@@ -315,7 +315,7 @@ class BatchSolver {
   int unroll_ = 8, grid_ = 1, group_ = 1, vec_ = 1, blocks_per_sm_ = 0, stall_graph_ = -1;
   double tuned_ms_ = 0.0;
   std::vector<int64_t> row_off_, nnz_off_, h_indptr_;
-  DevBuf indptr_, indices_, values_, tiles_, tile_graph_, graph_tiles_, counters_, status_, scratch_;
+  DevBuf indptr_, indices_, values_, tiles_, tile_graph_, graph_tiles_, counters_, status_, scratch_, row_order_;
   cudaGraph_t graph_ = nullptr;
   cudaGraphExec_t exec_ = nullptr;
   cudaGraphNode_t knode_ = nullptr;

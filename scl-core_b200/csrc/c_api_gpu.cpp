@@ -280,7 +280,7 @@ SCL_EXPORT scl_error_t scl_gpu_graph_set_plan(scl_gpu_graph_t graph, int64_t n_f
                     (kind == 3 && group == 32 && (stage == 16 || stage == 32) && bytes >= 4) ||
                     ((kind == 4 || kind == 7) && group == 32 && (stage == 8 || stage == 16 || stage == 32) &&
                      n_features == 32 * vec && (bytes == 4 || bytes == 8 || bytes == 16)) ||
-                    (kind == 9 && dtype_size(graph->store_type) == 2 && bytes == 16 &&
+                    ((kind == 9 || kind == 10) && dtype_size(graph->store_type) == 2 && bytes == 16 &&
                      n_features == (int64_t)group * vec && (group == 8 || group == 16) &&
                      (stage == 0 || stage == 1)) ||
                     ((kind == 5 || kind == 6) && dtype_size(graph->store_type) == 2 && bytes == 16 &&

@@ -20,6 +20,7 @@
 #include <cuda_fp16.h>
 
 #include <cstdio>
+#include <type_traits>
 
 #include "chunk_cursor.cuh"
 #include "engine.hpp"
@@ -1065,6 +1066,196 @@ k_spmm_split_pipe(const int64_t* __restrict__ indptr, const int32_t* __restrict_
   cp_async_wait_group<0>();
 }
 
+// ---- lean pipelined split-chain kernel (16-bit storage) -----------------------------
+// k_spmm_split_pipe with the per-entry overhead cut: full chunks of 32
+// entries (the common case) issue their copies and consume their slots with
+// no per-entry predicate, every copy targets a constant offset from one
+// shared-memory base address, and MODE selects the product form: 0 =
+// fma.rn.f32.{bf16,f16} per element; 1 (bf16 only) = each 32-bit word's two
+// bf16 values unpacked by a shift and a mask into an f32 pair and both
+// accumulators advanced by one fma.rn.f32x2 (two independent IEEE fmas, so
+// the bits equal mode 0's). Same chains and bits as k_spmm_split.
+__device__ __forceinline__ void fma2_bf16_word(unsigned long long& acc2, unsigned long long v2, unsigned w) {
+  unsigned long long x2;
+  asm("{\n\t.reg .b32 lo, hi;\n\tshl.b32 lo, %1, 16;\n\tand.b32 hi, %1, 0xffff0000;\n\tmov.b64 %0, {lo, hi};\n\t}"
+      : "=l"(x2)
+      : "r"(w));
+  asm("fma.rn.f32x2 %0, %1, %2, %0;" : "+l"(acc2) : "l"(v2), "l"(x2));
+}
+
+template <bool FULL, int MODE, int U, int Q, class XT>
+__device__ __forceinline__ void lean_consume(const uint4* __restrict__ sb, const unsigned short (&vq)[U], int q,
+                                             int cnt, float (&acc)[8], unsigned long long (&acc2)[4]) {
+#pragma unroll
+  for (int u = 0; u < U; ++u) {
+    const int e = u * Q + q;
+    const unsigned short vv = vq[u];
+    if (FULL || e < cnt) {
+      const uint4 raw = sb[u * 32];
+      if constexpr (MODE == 1) {
+        const float vf = __uint_as_float((unsigned)vv << 16);
+        unsigned long long v2;
+        asm("mov.b64 %0, {%1, %1};" : "=l"(v2) : "f"(vf));
+        fma2_bf16_word(acc2[0], v2, raw.x);
+        fma2_bf16_word(acc2[1], v2, raw.y);
+        fma2_bf16_word(acc2[2], v2, raw.z);
+        fma2_bf16_word(acc2[3], v2, raw.w);
+      } else {
+        const unsigned short* ex = reinterpret_cast<const unsigned short*>(&raw);
+#pragma unroll
+        for (int i = 0; i < 8; ++i) acc[i] = fma_mixed<XT>(vv, ex[i], acc[i]);
+      }
+    }
+  }
+}
+
+// For 256-byte rows (16 entries per lane per chunk) the chunk's (index, value)
+// pairs are staged in shared memory quarter-major (entry e at position
+// (e % Q) * U + e / Q), so a lane reads the U indices or values of its own
+// entries with a few vector loads instead of U shuffles; for 128-byte rows the
+// shuffles were measured faster and are kept.
+template <class VT, class XT, class YT, int ROWB, int MODE>
+__global__ void __launch_bounds__(32 * split_pipe_warps<ROWB>())
+k_spmm_split_lean(const int64_t* __restrict__ indptr, const int32_t* __restrict__ indices,
+                  const VT* __restrict__ values, const XT* __restrict__ X, YT* __restrict__ Y,
+                  const int32_t* __restrict__ row_map, int64_t n_rows) {
+  static_assert(sizeof(XT) == 2 && sizeof(VT) == 2, "the split-chain kernel is for 16-bit storage");
+  constexpr int L = ROWB / 16;
+  constexpr int Q = 32 / L;
+  constexpr int U = 32 / Q;
+  constexpr int VEC = 8;
+  constexpr int WARPS = split_pipe_warps<ROWB>();
+  constexpr int NT = 32 * WARPS;
+  constexpr unsigned SLOT = 32 * 16;  // bytes between a lane's consecutive slots
+  extern __shared__ uint4 smem_lean[];
+  __shared__ __align__(16) int32_t s_j[WARPS][2][32];
+  __shared__ __align__(16) unsigned short s_v[WARPS][2][32];
+  const int lane = threadIdx.x & 31;
+  const int w = threadIdx.x >> 5;
+  const int q = lane / L;
+  const int lq = lane & (L - 1);
+  const int tpos = (lane % Q) * U + lane / Q;  // where this lane's pair goes in the staging
+  const uint4* __restrict__ my = smem_lean + (size_t)w * 2 * U * 32 + lane;
+  const unsigned sbase = (unsigned)__cvta_generic_to_shared(my);
+  const char* __restrict__ Xb = reinterpret_cast<const char*>(X) + lq * 16;
+  const unsigned short* __restrict__ vbits = reinterpret_cast<const unsigned short*>(values);
+  const int64_t nw = ((int64_t)gridDim.x * NT) >> 5;
+  const int64_t row0 = ((int64_t)blockIdx.x * NT + threadIdx.x) >> 5;
+  if (row0 >= n_rows) return;
+  ChunkCursor cur;
+  cur.init(indptr, row0, n_rows, nw);
+  Chunk C = cur.next(indptr);
+  int32_t jC = 0;
+  unsigned short vC = 0;
+  if (C.valid && lane < C.cnt) {
+    jC = __ldcs(indices + C.pos + lane);
+    vC = __ldcs(vbits + C.pos + lane);
+  }
+  Chunk B;
+  unsigned short vB = 0;  // B's values, one per lane (shuffle path)
+  int st = 0;
+  float acc[VEC];
+  unsigned long long acc2[4];
+#pragma unroll
+  for (int i = 0; i < VEC; ++i) acc[i] = 0.0f;
+#pragma unroll
+  for (int i = 0; i < 4; ++i) acc2[i] = 0ull;
+  while (B.valid || C.valid) {
+    Chunk D = cur.next(indptr);
+    int32_t jD = 0;
+    unsigned short vD = 0;
+    if (D.valid && lane < D.cnt) {
+      jD = __ldcs(indices + D.pos + lane);
+      vD = __ldcs(vbits + D.pos + lane);
+    }
+    constexpr bool STG = (ROWB == 256);
+    if constexpr (STG) {  // stage C's pairs (its stage was last read two iterations ago)
+      __syncwarp();
+      s_j[w][st][tpos] = jC;
+      s_v[w][st][tpos] = vC;
+      __syncwarp();
+    }
+    if (C.valid) {
+      int32_t jq[U];
+      if constexpr (STG) {
+#pragma unroll
+        for (int k = 0; k < U; k += 4) {
+          const int4 j4 = *reinterpret_cast<const int4*>(&s_j[w][st][q * U + k]);
+          jq[k] = j4.x; jq[k + 1] = j4.y; jq[k + 2] = j4.z; jq[k + 3] = j4.w;
+        }
+      } else {
+#pragma unroll
+        for (int u = 0; u < U; ++u) jq[u] = __shfl_sync(0xffffffffu, jC, u * Q + q);
+      }
+      const unsigned sst = sbase + (unsigned)st * (U * SLOT);
+      if (C.cnt == 32) {
+#pragma unroll
+        for (int u = 0; u < U; ++u)
+          asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(sst + u * SLOT),
+                       "l"(Xb + (size_t)(uint32_t)jq[u] * (size_t)ROWB) : "memory");
+      } else {
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+          if (u * Q + q < C.cnt)
+            asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(sst + u * SLOT),
+                         "l"(Xb + (size_t)(uint32_t)jq[u] * (size_t)ROWB) : "memory");
+        }
+      }
+    }
+    cp_async_commit_group();
+    if (B.valid) {
+      cp_async_wait_group<1>();
+      if (B.first) {
+#pragma unroll
+        for (int i = 0; i < VEC; ++i) acc[i] = 0.0f;
+#pragma unroll
+        for (int i = 0; i < 4; ++i) acc2[i] = 0ull;
+      }
+      unsigned short vq[U];
+      if constexpr (STG) {
+#pragma unroll
+        for (int k = 0; k < U; k += 8) {
+          const uint4 v8 = *reinterpret_cast<const uint4*>(&s_v[w][st ^ 1][q * U + k]);
+          const unsigned short* pv = reinterpret_cast<const unsigned short*>(&v8);
+#pragma unroll
+          for (int i = 0; i < 8; ++i) vq[k + i] = pv[i];
+        }
+      } else {
+#pragma unroll
+        for (int u = 0; u < U; ++u) vq[u] = (unsigned short)__shfl_sync(0xffffffffu, (unsigned)vB, u * Q + q);
+      }
+      const uint4* __restrict__ sb = my + (st ^ 1) * U * 32;
+      if (B.cnt == 32) lean_consume<true, MODE, U, Q, XT>(sb, vq, q, 32, acc, acc2);
+      else lean_consume<false, MODE, U, Q, XT>(sb, vq, q, B.cnt, acc, acc2);
+      if (B.last) {
+        if constexpr (MODE == 1) {
+#pragma unroll
+          for (int i = 0; i < 4; ++i) {
+            acc[2 * i] = __uint_as_float((unsigned)(acc2[i] & 0xffffffffull));
+            acc[2 * i + 1] = __uint_as_float((unsigned)(acc2[i] >> 32));
+          }
+        }
+#pragma unroll
+        for (int o = L; o < 32; o <<= 1) {
+#pragma unroll
+          for (int i = 0; i < VEC; ++i) acc[i] = acc[i] + __shfl_xor_sync(0xffffffffu, acc[i], o);
+        }
+        if (q == 0) {
+          const int64_t orow = row_map ? (int64_t)row_map[B.row] : B.row;
+          VecStore<YT, VEC>::store(Y + orow * (ROWB / 2) + lq * VEC, acc);
+        }
+      }
+    }
+    B = C;
+    vB = vC;
+    C = D;
+    jC = jD;
+    vC = vD;
+    st ^= 1;
+  }
+  cp_async_wait_group<0>();
+}
+
 // Persistent grid size: resident blocks per SM (from the occupancy
 // calculator) times the SM count, capped by the blocks the rows need.
 template <class K>
@@ -1262,6 +1453,46 @@ void launch_split_pipe(const SpmmArgs& a, int mixed, cudaStream_t s) {
   throw Error(kErrInvalidArgument, "the pipelined split-chain SpMM needs 128- or 256-byte rows");
 }
 
+// kind 10: lean pipelined split-chain kernel; stage = MODE (0 mixed fma, 1 bf16 f32x2 fma)
+template <class VT, class XT, class YT, int ROWB, int MODE>
+void launch_split_lean_r(const SpmmArgs& a, cudaStream_t s) {
+  auto kern = k_spmm_split_lean<VT, XT, YT, ROWB, MODE>;
+  constexpr int smem = split_pipe_smem<ROWB>();
+  constexpr int nt = 32 * split_pipe_warps<ROWB>();
+  SCL_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+  SCL_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                (int)cudaSharedmemCarveoutMaxShared));
+  int dev = 0, per_sm = 0;
+  SCL_CUDA(cudaGetDevice(&dev));
+  SCL_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, nt, smem));
+  const int64_t need = (a.n_rows * 32 + nt - 1) / nt;
+  const int64_t grid = std::max<int64_t>(1, std::min<int64_t>(need, (int64_t)std::max(per_sm, 1) * sm_count(dev)));
+  kern<<<(unsigned)grid, nt, smem, s>>>(a.indptr, a.indices, static_cast<const VT*>(a.values),
+                                        static_cast<const XT*>(a.X), static_cast<YT*>(a.Y), a.row_map, a.n_rows);
+  SCL_CUDA(cudaGetLastError());
+}
+
+template <class VT, class XT, class YT>
+void launch_split_lean(const SpmmArgs& a, int mode, cudaStream_t s) {
+  const int64_t rowb = a.F * (int64_t)sizeof(XT);
+  constexpr bool kBf16 = std::is_same<XT, __nv_bfloat16>::value && std::is_same<VT, __nv_bfloat16>::value;
+  SCL_REQUIRE(mode == 0 || (mode == 1 && kBf16), kErrInvalidArgument,
+              "lean split-chain SpMM: stage 1 (packed f32x2 fma) needs bf16 storage");
+  if (rowb == 128) {
+    if constexpr (kBf16) {
+      if (mode == 1) return launch_split_lean_r<VT, XT, YT, 128, 1>(a, s);
+    }
+    return launch_split_lean_r<VT, XT, YT, 128, 0>(a, s);
+  }
+  if (rowb == 256) {
+    if constexpr (kBf16) {
+      if (mode == 1) return launch_split_lean_r<VT, XT, YT, 256, 1>(a, s);
+    }
+    return launch_split_lean_r<VT, XT, YT, 256, 0>(a, s);
+  }
+  throw Error(kErrInvalidArgument, "the lean split-chain SpMM needs 128- or 256-byte rows");
+}
+
 // kinds 5/6: split-chain kernel for 16-bit storage (6 = mixed-precision fma);
 // stage = gathers per lane per batch (U * chains must divide 32)
 template <class VT, class XT, class YT, int ROWB, int U, bool MIXED>
@@ -1334,6 +1565,14 @@ void launch_typed(const SpmmArgs& a, const SpmmPlan& plan, cudaStream_t s) {
                 "the flat-stream SpMM covers a row with one chunk per lane of a warp");
     return launch_flow<VT, XT, YT, AT>(a, plan.stage, s);
   }
+  if (plan.kind == 10) {
+    SCL_REQUIRE(plan.vec == kVec && (int64_t)plan.group * kVec == a.F && (plan.stage == 0 || plan.stage == 1),
+                kErrInvalidArgument, "the lean split-chain SpMM covers a row with one 16-byte chunk per lane");
+    if constexpr (sizeof(XT) == 2 && sizeof(VT) == 2 && sizeof(AT) == 4) {
+      return launch_split_lean<VT, XT, YT>(a, plan.stage, s);
+    }
+    throw Error(kErrInvalidArgument, "the lean split-chain SpMM is for bf16 or f16 storage");
+  }
   if (plan.kind == 9) {
     SCL_REQUIRE(plan.vec == kVec && (int64_t)plan.group * kVec == a.F && (plan.stage == 0 || plan.stage == 1),
                 kErrInvalidArgument, "the pipelined split-chain SpMM covers a row with one 16-byte chunk per lane");
@@ -1393,12 +1632,12 @@ SpmmPlan default_spmm_plan(int64_t F, DType xtype, const void* X, const void* Y,
       (reinterpret_cast<uintptr_t>(Y) % (uintptr_t)(8 * ys)) == 0) {
     // 16-bit storage: one 16-byte chunk per lane, 4 (128-byte rows) or 2
     // (256-byte rows) entries per load instruction, mixed-precision fma
-    // (measured at 500k cells: 128-byte rows fastest with 2 gathers per lane
-    // per batch; 256-byte rows with the cp.async pipeline)
+    // (measured at 500k cells: the lean cp.async pipeline with mixed-precision
+    // fma is fastest for both 128- and 256-byte rows)
     p.group = (int)(rb / 16);
     p.vec = 8;
-    p.kind = (rb == 128) ? 6 : 9;
-    p.stage = (rb == 128) ? 2 : 1;
+    p.kind = 10;
+    p.stage = 0;
     return p;
   }
   if (rb == 128 || rb == 256 || rb == 512) {
@@ -1441,7 +1680,7 @@ std::vector<SpmmPlan> candidate_plans(int64_t F, DType xtype, const void* X, con
     p.stage = stage;
     c.push_back(p);
   };
-  if (d.kind == 5 || d.kind == 6 || d.kind == 9) {
+  if (d.kind == 5 || d.kind == 6 || d.kind == 9 || d.kind == 10) {
     // interleaved-chain family (16-bit storage): same bits for every member
     const int rb = (int)(F * (int64_t)dtype_size(xtype));
     const int group = rb / 16;
@@ -1451,6 +1690,8 @@ std::vector<SpmmPlan> candidate_plans(int64_t F, DType xtype, const void* X, con
       add(group, 8, 5, st);
     }
     add(group, 8, 9, 1);
+    add(group, 8, 10, 0);
+    if (xtype == kBF16) add(group, 8, 10, 1);
   } else if (d.kind == 4) {
     // sequential-chain family, fixed row pitch
     for (int st : {8, 16, 32}) add(32, d.vec, 4, st);
@@ -1464,7 +1705,7 @@ void spmm_with_plan(const SpmmArgs& a, const SpmmPlan& plan, cudaStream_t s) {
   SCL_REQUIRE(plan.group >= 1 && plan.group <= 32 && (plan.group & (plan.group - 1)) == 0, kErrInvalidArgument,
               "lane-group size must be a power of two in [1, 32]");
   SCL_REQUIRE(plan.kind == 0 || plan.kind == 2 || plan.kind == 3 || plan.kind == 4 || plan.kind == 5 ||
-                  plan.kind == 6 || plan.kind == 7 || plan.kind == 9 ||
+                  plan.kind == 6 || plan.kind == 7 || plan.kind == 9 || plan.kind == 10 ||
                   (plan.kind == 1 && plan.vec > 1 && plan.group >= 4),
               kErrInvalidArgument, "the pipelined SpMM needs 16-byte lane chunks and a lane group of at least 4");
   if (plan.vec > 1) {

@@ -213,7 +213,7 @@ def test_skewed_and_empty_rows():
             X0 = rng.standard_normal((n, F)).astype(np.float32)
             Xd = torch.from_numpy(X0).cuda().to(torch.bfloat16)
             ref1 = port.diffuse_lowp_chains(ip, ind, P, Xd.float().cpu().numpy(), 1, port.BF16, 32 // group, True)
-            for kind, stage in ((5, 4), (6, 4), (9, 0), (9, 1)):
+            for kind, stage in ((5, 4), (6, 4), (9, 0), (9, 1), (10, 0), (10, 1)):
                 Y = torch.empty((n, F), dtype=torch.float32, device="cuda")
                 g.spmm(Xd, Y, group=group, vec=8, kind=kind, stage=stage)
                 np.testing.assert_array_equal(bits(Y.cpu().numpy()), bits(ref1))
@@ -423,7 +423,9 @@ def test_split_chain_shapes_are_exact(graph_3k, storage, F):
         chains = 32 // group
         ref1 = port.diffuse_lowp_chains(ip, ind, P, Xd.float().cpu().numpy(), 1, kind_code, chains, True)
         stages = (2, 4, 8) if group == 8 else (4, 8, 16)
-        shapes = [(k, st) for k in (5, 6) for st in stages] + [(9, 0), (9, 1)]
+        shapes = [(k, st) for k in (5, 6) for st in stages] + [(9, 0), (9, 1), (10, 0)]
+        if storage == "bf16":
+            shapes.append((10, 1))  # packed f32x2 fma
         for kind, stage in shapes:
             Y = torch.empty((n, F), dtype=torch.float32, device="cuda")
             g.spmm(Xd, Y, group=group, vec=8, kind=kind, stage=stage)
@@ -451,7 +453,7 @@ def test_autotune_keeps_the_bits(graph_3k, storage):
         X0 = torch.from_numpy(np.random.default_rng(2).standard_normal((n, 64)).astype(np.float32)).cuda()
         before = g.diffuse(X0, 4, out_dtype=torch.float32)
         res = g.autotune(64, reps=2)
-        assert res["ms"] > 0 and res["kind"] in (4, 5, 6, 7, 9)
+        assert res["ms"] > 0 and res["kind"] in (4, 5, 6, 7, 9, 10)
         after = g.diffuse(X0, 4, out_dtype=torch.float32)
         assert torch.equal(before, after)
         assert g.gather_floor(64, reps=2) > 0

@@ -62,13 +62,48 @@ class ClockSampler:
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
 
-    def __init__(self, gpu_index: int):
+    def __init__(self, gpu_index: int, uuid: str = None):
         self.gpu = gpu_index
+        self.uuid = uuid
         self.samples = []
+        self.source = None
         self._stop = threading.Event()
         self._t = None
 
+    def _nvml_handle(self):
+        import pynvml
+
+        pynvml.nvmlInit()
+        if self.uuid:
+            try:
+                return pynvml, pynvml.nvmlDeviceGetHandleByUUID(self.uuid)
+            except Exception:
+                pass
+        return pynvml, pynvml.nvmlDeviceGetHandleByIndex(self.gpu)
+
+    def _run_nvml(self, nv, h):
+        """Read-only NVML queries every 10 ms (the same fields nvidia-smi prints)."""
+        bits = [nv.nvmlClocksEventReasonHwSlowdown, nv.nvmlClocksEventReasonHwThermalSlowdown,
+                nv.nvmlClocksEventReasonSwThermalSlowdown, nv.nvmlClocksEventReasonSwPowerCap]
+        mx = nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM)
+        while not self._stop.is_set():
+            try:
+                sm = nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM)
+                r = nv.nvmlDeviceGetCurrentClocksEventReasons(h)
+                pw = nv.nvmlDeviceGetPowerUsage(h) / 1000.0
+                self.samples.append([str(self.gpu), str(sm), str(mx), f"{pw:.1f}", hex(r)]
+                                    + ["Active" if r & b else "Not Active" for b in bits])
+            except Exception:
+                pass
+            self._stop.wait(0.01)
+
     def _run(self):
+        try:
+            nv, h = self._nvml_handle()
+            self.source = "nvml 10 ms"
+            return self._run_nvml(nv, h)
+        except Exception:
+            self.source = "nvidia-smi 200 ms"
         while not self._stop.is_set():
             try:
                 out = subprocess.run(["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}",
@@ -97,7 +132,14 @@ class ClockSampler:
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
         reasons = sorted({names[i] for s in self.samples for i in range(4) if s[5 + i].strip() == "Active"})
         return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
-                "reasons": reasons, "samples": len(self.samples)}
+                "reasons": reasons, "samples": len(self.samples), "source": self.source}
+
+
+def gpu_uuid(torch, device):
+    try:
+        return "GPU-" + str(torch.cuda.get_device_properties(device).uuid)
+    except Exception:
+        return None
 
 
 # ---- inputs ------------------------------------------------------------------------
@@ -393,7 +435,7 @@ def main():
     if dist is not None:
         dist.barrier()
     torch.cuda.synchronize()
-    with ClockSampler(local) as clk:
+    with ClockSampler(local, gpu_uuid(torch, device)) as clk:
         times = timed_calls(torch, run_f32, args.steps, warmup, flush, stream)
     torch.cuda.synchronize()
     t_ms = float(np.mean(times))

@@ -126,11 +126,14 @@ SCL_EXPORT scl_error_t scl_gpu_graph_reorder_info(scl_gpu_graph_t graph, int32_t
  * rows with kind 4's lane layout (stage = gathers per batch 8/16/32; batches
  * stay full across row ends); 9 = kind 5/6's layout and chains with the
  * gathers copied by cp.async into shared memory, two chunks of 32 entries in
- * flight per warp (stage 0 = plain fma, 1 = mixed-precision fma). group <= 0
- * picks the default shape. X and Y must be in
- * the storage dtype (Y may also be F32). Every shape of kinds 0-4 and 7
- * computes the same bits (the sequential fma chain); kinds 5, 6 and 9 compute
- * the same bits as each other (the interleaved chains). */
+ * flight per warp (stage 0 = plain fma, 1 = mixed-precision fma); 10 = kind
+ * 9's layout and chains with predicate-free full chunks (the default for
+ * 16-bit storage; stage 0 = mixed-precision fma, 1 = bf16 only, each word's
+ * two elements advanced by one packed f32x2 fma). group <= 0 picks the
+ * default shape. X and Y must be in the storage dtype (Y may also be F32).
+ * Every shape of kinds 0-4 and 7 computes the same bits (the sequential fma
+ * chain); kinds 5, 6, 9 and 10 compute the same bits as each other (the
+ * interleaved chains). */
 SCL_EXPORT scl_error_t scl_gpu_spmm(scl_gpu_graph_t graph, const void* X, void* Y, scl_dtype_t y_dtype,
                                     int64_t n_features, int group, int vec, int kind, int stage, void* stream);
 

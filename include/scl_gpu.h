@@ -96,6 +96,18 @@ SCL_EXPORT scl_error_t scl_gpu_graph_set_plan(scl_gpu_graph_t graph, int64_t n_f
  * structure when one is set), at full occupancy and with the L2 flushed before
  * each repetition. It is the memory-system floor of one SpMM step on this
  * graph (row pitch 128, 256 or 512 bytes). Synchronises `stream`. */
+/* Status of the bulk-copy SpMM (plan kind 11; no counterpart in scl-core):
+ * every wait of that kernel on its copies is bounded (2 s); a wait that gives
+ * up records SCL_ERROR_CONVERGENCE and the global warp index, and the warp
+ * leaves its rows unwritten. Synchronises `stream`, stores the code (0 = none)
+ * and the warp (NULL allowed), and clears the word. */
+SCL_EXPORT scl_error_t scl_gpu_spmm_status(int32_t* code, int32_t* warp, void* stream);
+
+/* Test hook for that bounded wait: global warp `warp` of later kind-11
+ * launches expects 16 bytes more than its first chunk copies, so that wait
+ * runs out; -1 turns the hook off. Synchronises `stream`. */
+SCL_EXPORT scl_error_t scl_gpu_spmm_inject_stall(int64_t warp, void* stream);
+
 SCL_EXPORT scl_error_t scl_gpu_graph_gather_floor(scl_gpu_graph_t graph, int64_t n_features, scl_dtype_t dtype,
                                                   int reps, double* ms, void* stream);
 
@@ -129,9 +141,14 @@ SCL_EXPORT scl_error_t scl_gpu_graph_reorder_info(scl_gpu_graph_t graph, int32_t
  * flight per warp (stage 0 = plain fma, 1 = mixed-precision fma); 10 = kind
  * 9's layout and chains with predicate-free full chunks (the default for
  * 16-bit storage; stage 0 = mixed-precision fma, 1 = bf16 only, each word's
- * two elements advanced by one packed f32x2 fma). group <= 0 picks the
+ * two elements advanced by one packed f32x2 fma); 11 = FP32/FP64, warp per
+ * row with kind 4's lane layout, the gathered X rows copied whole by the
+ * bulk-copy engine (cp.async.bulk, one row per lane of a 32-entry chunk) into
+ * a per-warp shared-memory ring of `stage` chunks (2, 3, 4 or 6; 128/256/512-
+ * byte rows, FP64 256/512), waits bounded and reported through
+ * scl_gpu_spmm_status. group <= 0 picks the
  * default shape. X and Y must be in the storage dtype (Y may also be F32).
- * Every shape of kinds 0-4 and 7 computes the same bits (the sequential fma
+ * Every shape of kinds 0-4, 7 and 11 computes the same bits (the sequential fma
  * chain); kinds 5, 6, 9 and 10 compute the same bits as each other (the
  * interleaved chains). */
 SCL_EXPORT scl_error_t scl_gpu_spmm(scl_gpu_graph_t graph, const void* X, void* Y, scl_dtype_t y_dtype,

@@ -394,28 +394,46 @@ __global__ void k_norm_bwd_gather(const int64_t* __restrict__ ptr, const int32_t
   const int lane = threadIdx.x & 31;
   if (row >= n) return;
   const int64_t s0 = ptr[row], s1 = ptr[row + 1];
+  // The first KEEP entries per lane (rows up to 32*KEEP entries, the common
+  // case) are gathered once, all in flight together, and kept in registers
+  // for the second pass; longer rows gather the rest twice. Each lane still
+  // sums its entries in increasing position order.
+  constexpr int KEEP = 4;
+  double gk[KEEP];
   double u = 0.0;
-  for (int64_t p = s0 + lane; p < s1; p += 32) u += (double)gPt[inv[p]] * (double)P[p];
+#pragma unroll
+  for (int k = 0; k < KEEP; ++k) {
+    const int64_t p = s0 + lane + 32 * k;
+    gk[k] = 0.0;
+    if (p < s1) gk[k] = (double)gPt[inv[p]];
+  }
+#pragma unroll
+  for (int k = 0; k < KEEP; ++k) {
+    const int64_t p = s0 + lane + 32 * k;
+    if (p < s1) u += gk[k] * (double)P[p];
+  }
+  for (int64_t p = s0 + lane + 32 * KEEP; p < s1; p += 32) u += (double)gPt[inv[p]] * (double)P[p];
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) u += __shfl_xor_sync(0xffffffffu, u, o);
   const double di = deg[row];
   const bool live = di > kMinProbB;
   const double ai = live ? 1.0 / sqrt(di) : 0.0;
   const double shift = live ? (symmetric ? (u + v[row]) / (2.0 * di) : u) : 0.0;
-  for (int64_t p = s0 + lane; p < s1; p += 32) {
-    double r = 0.0;
-    if (live) {
-      const double gp = (double)gPt[inv[p]];
-      if (symmetric) {
-        const double dj = deg[idx[p]];
-        const double aj = dj > kMinProbB ? 1.0 / sqrt(dj) : 0.0;
-        r = gp * ai * aj - shift;
-      } else {
-        r = (gp - shift) / di;
-      }
+  auto grad = [&](int64_t p, double gp) -> double {
+    if (!live) return 0.0;
+    if (symmetric) {
+      const double dj = deg[idx[p]];
+      const double aj = dj > kMinProbB ? 1.0 / sqrt(dj) : 0.0;
+      return gp * ai * aj - shift;
     }
-    dW[p] = (T)r;
+    return (gp - shift) / di;
+  };
+#pragma unroll
+  for (int k = 0; k < KEEP; ++k) {
+    const int64_t p = s0 + lane + 32 * k;
+    if (p < s1) dW[p] = (T)grad(p, gk[k]);
   }
+  for (int64_t p = s0 + lane + 32 * KEEP; p < s1; p += 32) dW[p] = (T)grad(p, (double)gPt[inv[p]]);
 }
 
 template <class T>

@@ -280,6 +280,12 @@ SCL_EXPORT scl_error_t scl_gpu_graph_set_plan(scl_gpu_graph_t graph, int64_t n_f
                     (kind == 3 && group == 32 && (stage == 16 || stage == 32) && bytes >= 4) ||
                     ((kind == 4 || kind == 7) && group == 32 && (stage == 8 || stage == 16 || stage == 32) &&
                      n_features == 32 * vec && (bytes == 4 || bytes == 8 || bytes == 16)) ||
+                    (kind == 12 && (group == 8 || group == 16 || group == 32) && bytes == 16 &&
+                     n_features == (int64_t)group * vec && dtype_size(graph->store_type) >= 4 &&
+                     (stage == 4 || stage == 8 || stage == 16)) ||
+                    (kind == 11 && group == 32 && n_features == 32 * vec && dtype_size(graph->store_type) >= 4 &&
+                     (bytes == 4 || bytes == 8 || bytes == 16) && bytes >= (int)dtype_size(graph->store_type) &&
+                     (stage == 2 || stage == 3 || stage == 4 || stage == 6)) ||
                     ((kind == 9 || kind == 10) && dtype_size(graph->store_type) == 2 && bytes == 16 &&
                      n_features == (int64_t)group * vec && (group == 8 || group == 16) &&
                      (stage == 0 || stage == 1)) ||
@@ -552,6 +558,21 @@ SCL_EXPORT scl_error_t scl_gpu_batch_status(scl_gpu_batch_t batch, int* code, in
   const int32_t c = batch->solver.status(as_stream(stream), &it);
   if (code) *code = c;
   if (item) *item = it;
+  SCL_API_RETURN_OK;
+  SCL_API_CATCH
+}
+
+SCL_EXPORT scl_error_t scl_gpu_spmm_status(int32_t* code, int32_t* warp, void* stream) {
+  SCL_API_CHECK(code != nullptr, SCL_ERROR_NULL_POINTER, "code must not be NULL");
+  SCL_API_TRY
+  *code = spmm_bulk_status(as_stream(stream), warp);
+  SCL_API_RETURN_OK;
+  SCL_API_CATCH
+}
+
+SCL_EXPORT scl_error_t scl_gpu_spmm_inject_stall(int64_t warp, void* stream) {
+  SCL_API_TRY
+  spmm_bulk_inject_stall(warp, as_stream(stream));
   SCL_API_RETURN_OK;
   SCL_API_CATCH
 }

@@ -168,6 +168,15 @@ std::vector<SpmmPlan> candidate_plans(int64_t F, DType xtype, const void* X, con
 // nonzeros in stored order (FP32 accumulation, FP64 when values/X are f64).
 void spmm(const SpmmArgs& a, cudaStream_t s);
 void spmm_with_plan(const SpmmArgs& a, const SpmmPlan& plan, cudaStream_t s);
+// Plan kind 11: row gathers by bulk copies into a per-warp shared-memory ring
+// of `ns` stages (2, 3, 4 or 6); FP32/FP64 rows of 128/256/512 bytes (FP64:
+// 256/512), same bits as kinds 0-4. Its bounded waits report through
+// spmm_bulk_status (error code, 0 if none; the warp that gave up), which
+// synchronises `s` and clears the word.
+bool spmm_bulk_fits(int64_t F, DType t, const void* X, const void* Y);
+void spmm_bulk(const SpmmArgs& a, int ns, cudaStream_t s);
+int32_t spmm_bulk_status(cudaStream_t s, int32_t* warp);
+void spmm_bulk_inject_stall(int64_t warp, cudaStream_t s);
 
 // Y = P^steps X0. Intermediate iterates are stored as `mtype` (which must equal
 // the graph's value dtype) in pool buffers; the last step writes Y in `ytype`.

@@ -679,6 +679,173 @@ k_spmm_row(const int64_t* __restrict__ indptr, const int32_t* __restrict__ indic
   }
 }
 
+// ---- multi-row kernel with 16-byte lanes (FP32/FP64, 128/256-byte rows) ------------
+// A gathered row is covered by L = ROWB/16 lanes with one 16-byte chunk each,
+// so one load instruction of the warp fetches R = 32/L rows: the warp advances
+// R consecutive output rows together, lane group q (lanes q*L .. q*L+L-1)
+// owning row q of the group and lane lq of it the VEC columns
+// [lq*VEC, (lq+1)*VEC). Each lane runs its columns' sequential fma chains over
+// its row's entries in stored order (the same bits as k_spmm_row). Per chunk
+// of 32 entries a row's (index, value) pairs are staged in shared memory and
+// read back 4 at a time; the group's rows run in lockstep to the longest one,
+// shorter rows predicated off, and batches where every row of the group still
+// has U entries issue their U gathers without predicates. The next chunk's
+// pairs (or the next group's first) are in flight while a chunk is consumed,
+// and row bounds are fetched a group ahead, as in k_spmm_row.
+template <class T, int ROWB, int U, int MINB>
+__global__ void __launch_bounds__(kSpmmThreads, MINB)
+k_spmm_rows16(const int64_t* __restrict__ indptr, const int32_t* __restrict__ indices, const T* __restrict__ values,
+              const T* __restrict__ X, T* __restrict__ Y, const int32_t* __restrict__ row_map, int64_t n_rows) {
+  constexpr int L = ROWB / 16;
+  constexpr int R = 32 / L;
+  constexpr int VEC = 16 / (int)sizeof(T);
+  constexpr int WARPS = kSpmmThreads / 32;
+  static_assert(L == 8 || L == 16 || L == 32, "row pitch must be 128, 256 or 512 bytes");
+  static_assert(U == 4 || U == 8 || U == 16, "batch must be 4, 8 or 16");
+  __shared__ __align__(16) int32_t s_j[WARPS][2][32 * R];
+  __shared__ __align__(16) T s_v[WARPS][2][32 * R];
+  const int lane = threadIdx.x & 31;
+  const int w = threadIdx.x >> 5;
+  const int q = lane / L;
+  const int lq = lane % L;
+  const int64_t n_grp = (n_rows + R - 1) / R;
+  const int64_t nw = ((int64_t)gridDim.x * kSpmmThreads) >> 5;
+  int64_t grp = ((int64_t)blockIdx.x * kSpmmThreads + threadIdx.x) >> 5;
+  if (grp >= n_grp) return;
+  const char* __restrict__ Xl = reinterpret_cast<const char*>(X) + lq * 16;
+  auto gather = [&](int32_t j) -> uint4 {
+    return __ldg(reinterpret_cast<const uint4*>(Xl + (size_t)(uint32_t)j * ROWB));
+  };
+  auto bounds = [&](int64_t g, int64_t& b0, int64_t& b1) {
+    const int64_t r = g * R + q;
+    b0 = b1 = 0;
+    if (g < n_grp && r < n_rows) {
+      b0 = indptr[r];
+      b1 = indptr[r + 1];
+    }
+  };
+  // pairs [b0 + base, b0 + base + 32) of a row, R per lane of its group
+  auto fetch = [&](int64_t b0, int64_t b1, int base, int32_t (&j)[R], T (&v)[R]) {
+#pragma unroll
+    for (int k = 0; k < R; ++k) {
+      const int64_t p = b0 + base + lq + L * k;
+      j[k] = 0;
+      v[k] = T(0);
+      if (p < b1) {
+        j[k] = __ldcs(indices + p);
+        v[k] = __ldcs(values + p);
+      }
+    }
+  };
+  auto publish = [&](int b, const int32_t (&j)[R], const T (&v)[R]) {
+#pragma unroll
+    for (int k = 0; k < R; ++k) {
+      s_j[w][b][q * 32 + lq + L * k] = j[k];
+      s_v[w][b][q * 32 + lq + L * k] = v[k];
+    }
+  };
+  int64_t s_cur, e_cur, s_nx, e_nx;
+  bounds(grp, s_cur, e_cur);
+  bounds(grp + nw, s_nx, e_nx);
+  int buf = 0;
+  {
+    int32_t j[R];
+    T v[R];
+    fetch(s_cur, e_cur, 0, j, v);
+    publish(0, j, v);
+    __syncwarp();
+  }
+  for (; grp < n_grp; grp += nw) {
+    int64_t s_nn, e_nn;
+    bounds(grp + 2 * nw, s_nn, e_nn);
+    const int len = (int)(e_cur - s_cur);
+    int maxlen = len, minlen = len;
+#pragma unroll
+    for (int o = L; o < 32; o <<= 1) {
+      maxlen = max(maxlen, __shfl_xor_sync(0xffffffffu, maxlen, o));
+      minlen = min(minlen, __shfl_xor_sync(0xffffffffu, minlen, o));
+    }
+    T acc[VEC];
+#pragma unroll
+    for (int i = 0; i < VEC; ++i) acc[i] = T(0);
+    for (int base = 0; base < maxlen; base += 32) {
+      int32_t jn[R];
+      T vn[R];
+      if (base + 32 < maxlen) fetch(s_cur, e_cur, base + 32, jn, vn);
+      else fetch(s_nx, e_nx, 0, jn, vn);
+      const int cnt = len - base;  // this lane's row: entries left (may be <= 0)
+      const int cmax = min(maxlen - base, 32);
+      const int cmin = min(minlen - base, 32);
+      const int32_t* __restrict__ jb = &s_j[w][buf][q * 32];
+      const T* __restrict__ vb = &s_v[w][buf][q * 32];
+#pragma unroll 1
+      for (int t = 0; t < cmax; t += U) {
+        uint4 xr[U];
+        const bool full = (t + U <= cmin);
+#pragma unroll
+        for (int u = 0; u < U; u += 4) {
+          const int4 j4 = *reinterpret_cast<const int4*>(jb + t + u);
+          if (full) {
+            xr[u] = gather(j4.x);
+            xr[u + 1] = gather(j4.y);
+            xr[u + 2] = gather(j4.z);
+            xr[u + 3] = gather(j4.w);
+          } else {
+            if (t + u < cnt) xr[u] = gather(j4.x);
+            if (t + u + 1 < cnt) xr[u + 1] = gather(j4.y);
+            if (t + u + 2 < cnt) xr[u + 2] = gather(j4.z);
+            if (t + u + 3 < cnt) xr[u + 3] = gather(j4.w);
+          }
+        }
+#pragma unroll
+        for (int u = 0; u < U; u += 4) {
+          T vq[4];
+          if constexpr (sizeof(T) == 4) {
+            const float4 v4 = *reinterpret_cast<const float4*>(vb + t + u);
+            vq[0] = v4.x; vq[1] = v4.y; vq[2] = v4.z; vq[3] = v4.w;
+          } else {
+            const double2 va = *reinterpret_cast<const double2*>(vb + t + u);
+            const double2 vc = *reinterpret_cast<const double2*>(vb + t + u + 2);
+            vq[0] = va.x; vq[1] = va.y; vq[2] = vc.x; vq[3] = vc.y;
+          }
+#pragma unroll
+          for (int r = 0; r < 4; ++r) {
+            if (full || t + u + r < cnt) {
+              const T* ex = reinterpret_cast<const T*>(&xr[u + r]);
+#pragma unroll
+              for (int i = 0; i < VEC; ++i) acc[i] = fma_acc(vq[r], ex[i], acc[i]);
+            }
+          }
+        }
+      }
+      // the other buffer was last read one chunk ago, before the last __syncwarp
+      publish(buf ^ 1, jn, vn);
+      __syncwarp();
+      buf ^= 1;
+    }
+    if (maxlen == 0) {  // empty rows only: nothing was prefetched, stage the next group's first chunk
+      int32_t j[R];
+      T v[R];
+      fetch(s_nx, e_nx, 0, j, v);
+      publish(buf, j, v);
+      __syncwarp();
+    }
+    const int64_t r = grp * R + q;
+    if (r < n_rows) {
+      const int64_t orow = row_map ? (int64_t)row_map[r] : r;
+      uint4 o;
+      T* op = reinterpret_cast<T*>(&o);
+#pragma unroll
+      for (int i = 0; i < VEC; ++i) op[i] = acc[i];
+      *reinterpret_cast<uint4*>(reinterpret_cast<char*>(Y) + orow * ROWB + lq * 16) = o;
+    }
+    s_cur = s_nx;
+    e_cur = e_nx;
+    s_nx = s_nn;
+    e_nx = e_nn;
+  }
+}
+
 // ---- flat-stream kernel: a warp walks the entries of a block of rows ---------------
 // A task is R consecutive rows; their entries [indptr[r0], indptr[r0+R]) are
 // one contiguous stream that the warp consumes in batches of U gathers, with
@@ -1389,6 +1556,37 @@ void launch_row(const SpmmArgs& a, int U, cudaStream_t s) {
   throw Error(kErrInvalidArgument, "the fixed-pitch SpMM needs 128-, 256- or 512-byte rows");
 }
 
+// kind 12: multi-row kernel with 16-byte lanes; stage = gathers per batch (4/8/16)
+template <class T, int ROWB, int U, int MINB>
+void launch_rows16_u(const SpmmArgs& a, cudaStream_t s) {
+  constexpr int R = 32 / (ROWB / 16);
+  auto kern = k_spmm_rows16<T, ROWB, U, MINB>;
+  const int64_t groups = (a.n_rows + R - 1) / R;
+  const dim3 grid(persistent_blocks(kern, 0, groups, 32));
+  kern<<<grid, kSpmmThreads, 0, s>>>(a.indptr, a.indices, static_cast<const T*>(a.values),
+                                     static_cast<const T*>(a.X), static_cast<T*>(a.Y), a.row_map, a.n_rows);
+  SCL_CUDA(cudaGetLastError());
+}
+
+template <class T, int ROWB>
+void launch_rows16_rb(const SpmmArgs& a, int U, cudaStream_t s) {
+  if (U == 4) return launch_rows16_u<T, ROWB, 4, 4>(a, s);
+  if (U == 8) return launch_rows16_u<T, ROWB, 8, 3>(a, s);
+  if (U == 16) return launch_rows16_u<T, ROWB, 16, 2>(a, s);
+  throw Error(kErrInvalidArgument, "multi-row SpMM batch must be 4, 8 or 16");
+}
+
+template <class T>
+void launch_rows16(const SpmmArgs& a, int U, cudaStream_t s) {
+  const int64_t rowb = a.F * (int64_t)sizeof(T);
+  SCL_REQUIRE(reinterpret_cast<uintptr_t>(a.X) % 16 == 0 && reinterpret_cast<uintptr_t>(a.Y) % 16 == 0,
+              kErrInvalidArgument, "the multi-row SpMM needs 16-byte aligned X and Y");
+  if (rowb == 128) return launch_rows16_rb<T, 128>(a, U, s);
+  if (rowb == 256) return launch_rows16_rb<T, 256>(a, U, s);
+  if (rowb == 512) return launch_rows16_rb<T, 512>(a, U, s);
+  throw Error(kErrInvalidArgument, "the multi-row SpMM needs 128-, 256- or 512-byte rows");
+}
+
 // kind 7: flat-stream kernel over tasks of 16 consecutive rows; stage = gathers per batch
 template <class VT, class XT, class YT, class AT, int ROWB, int U>
 void launch_flow_u(const SpmmArgs& a, cudaStream_t s) {
@@ -1565,6 +1763,16 @@ void launch_typed(const SpmmArgs& a, const SpmmPlan& plan, cudaStream_t s) {
                 "the flat-stream SpMM covers a row with one chunk per lane of a warp");
     return launch_flow<VT, XT, YT, AT>(a, plan.stage, s);
   }
+  if (plan.kind == 12) {
+    SCL_REQUIRE((int64_t)plan.group * plan.vec == a.F && plan.vec * (int)sizeof(XT) == 16 &&
+                    (plan.group == 8 || plan.group == 16 || plan.group == 32),
+                kErrInvalidArgument, "the multi-row SpMM covers a row with 16-byte chunks, 8/16/32 lanes per row");
+    if constexpr (std::is_same<VT, XT>::value && std::is_same<XT, YT>::value && std::is_same<YT, AT>::value &&
+                  sizeof(AT) >= 4) {
+      return launch_rows16<AT>(a, plan.stage, s);
+    }
+    throw Error(kErrInvalidArgument, "the multi-row SpMM is for FP32 or FP64 values, X and Y of one dtype");
+  }
   if (plan.kind == 10) {
     SCL_REQUIRE(plan.vec == kVec && (int64_t)plan.group * kVec == a.F && (plan.stage == 0 || plan.stage == 1),
                 kErrInvalidArgument, "the lean split-chain SpMM covers a row with one 16-byte chunk per lane");
@@ -1696,6 +1904,12 @@ std::vector<SpmmPlan> candidate_plans(int64_t F, DType xtype, const void* X, con
     // sequential-chain family, fixed row pitch
     for (int st : {8, 16, 32}) add(32, d.vec, 4, st);
     for (int st : {8, 16}) add(32, d.vec, 7, st);
+    if (spmm_bulk_fits(F, xtype, X, Y) && xtype == ytype)
+      for (int st : {2, 3}) add(32, d.vec, 11, st);
+    const int rb = (int)(F * (int64_t)dtype_size(xtype));
+    if (xtype == ytype && (rb == 128 || rb == 256) && (reinterpret_cast<uintptr_t>(X) & 15u) == 0 &&
+        (reinterpret_cast<uintptr_t>(Y) & 15u) == 0)
+      for (int st : {4, 8, 16}) add(rb / 16, 16 / (int)dtype_size(xtype), 12, st);
   }
   return c;
 }
@@ -1705,9 +1919,14 @@ void spmm_with_plan(const SpmmArgs& a, const SpmmPlan& plan, cudaStream_t s) {
   SCL_REQUIRE(plan.group >= 1 && plan.group <= 32 && (plan.group & (plan.group - 1)) == 0, kErrInvalidArgument,
               "lane-group size must be a power of two in [1, 32]");
   SCL_REQUIRE(plan.kind == 0 || plan.kind == 2 || plan.kind == 3 || plan.kind == 4 || plan.kind == 5 ||
-                  plan.kind == 6 || plan.kind == 7 || plan.kind == 9 || plan.kind == 10 ||
+                  plan.kind == 6 || plan.kind == 7 || plan.kind == 9 || plan.kind == 10 || plan.kind == 11 ||
+                  plan.kind == 12 ||
                   (plan.kind == 1 && plan.vec > 1 && plan.group >= 4),
               kErrInvalidArgument, "the pipelined SpMM needs 16-byte lane chunks and a lane group of at least 4");
+  if (plan.kind == 11) {
+    SCL_REQUIRE(plan.group == 32 && (int64_t)plan.vec * 32 == a.F, kErrInvalidArgument, "the bulk-copy SpMM covers a row with one chunk per lane of a warp");
+    return spmm_bulk(a, plan.stage, s);
+  }
   if (plan.vec > 1) {
     const int xs = (int)dtype_size(a.xtype), ys = (int)dtype_size(a.ytype);
     const int xb = plan.vec * xs, yb = plan.vec * ys;

@@ -148,6 +148,21 @@ class GpuGraph:
                     "autotune", self._lib)
         return {"kind": k.value, "stage": st.value, "ms": ms.value}
 
+    def spmm_status(self, stream=None):
+        """(code, warp) of the bulk-copy SpMM's bounded waits in this graph's
+        library since the last call (0 = none); synchronises and clears."""
+        code, warp = ctypes.c_int(0), ctypes.c_int(0)
+        check_error(self._lib.scl_gpu_spmm_status(ctypes.byref(code), ctypes.byref(warp), _stream_ptr(stream)),
+                    "spmm_status", self._lib)
+        return code.value, warp.value
+
+    def inject_spmm_stall(self, warp: int, stream=None) -> "GpuGraph":
+        """Test hook: global warp `warp` of later bulk-copy SpMM launches
+        expects more bytes than it copies, so its first wait runs out (-1 = off)."""
+        check_error(self._lib.scl_gpu_spmm_inject_stall(int(warp), _stream_ptr(stream)), "spmm_inject_stall",
+                    self._lib)
+        return self
+
     def gather_floor(self, n_features: int, dtype=None, reps: int = 5, stream=None) -> float:
         """Median ms of gathering one n_features-wide row per stored entry in
         diffusion order (the memory-system floor of one SpMM step)."""

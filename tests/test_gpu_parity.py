@@ -203,9 +203,13 @@ def test_skewed_and_empty_rows():
             X0 = rng.standard_normal((n, F)).astype(np.float32)
             ref1 = port.spmm(ip, ind, P, X0)
             Xd = torch.from_numpy(X0).cuda()
-            for kind, stage in ((4, 8), (4, 32), (7, 8), (7, 16), (7, 32)):
+            for kind, stage in ((4, 8), (4, 32), (7, 8), (7, 16), (7, 32), (11, 2), (11, 3), (11, 6)):
                 Y = torch.empty_like(Xd)
                 g.spmm(Xd, Y, group=32, vec=vec, kind=kind, stage=stage)
+                np.testing.assert_array_equal(bits(Y.cpu().numpy()), bits(ref1))
+            for stage in (4, 8, 16):  # multi-row kernel: F/4 lanes per row, 32/(F/4) rows per warp
+                Y = torch.empty_like(Xd)
+                g.spmm(Xd, Y, group=F // 4, vec=4, kind=12, stage=stage)
                 np.testing.assert_array_equal(bits(Y.cpu().numpy()), bits(ref1))
         # 16-bit storage kernels (interleaved chains) on the same rows
         g.set_storage(torch.bfloat16)
@@ -312,11 +316,14 @@ def test_every_launch_shape_is_exact(graph_3k, group):
     Xd = torch.from_numpy(X0).cuda()
     ref1 = port.spmm(ip, ind, P, X0)
     shapes = [(1, 0, 8), (4, 0, 8)] + ([(4, 1, s) for s in (4, 8, 16)] if group >= 4 else [])
+    if group == 16:
+        shapes += [(4, 12, 4), (4, 12, 8), (4, 12, 16)]  # two rows per warp, 16-byte lanes
     if group == 32:
         shapes.append((2, 0, 8))  # whole warp per row, 8-byte lane chunks
         shapes += [(2, 2, 8), (2, 2, 16), (2, 3, 16), (2, 3, 32), (1, 3, 16)]  # row-block streams
         shapes += [(2, 4, 8), (2, 4, 16), (2, 4, 32)]  # fixed-pitch warp-per-row
         shapes += [(2, 7, 8), (2, 7, 16), (2, 7, 32)]  # flat entry stream over row blocks
+        shapes += [(2, 11, 2), (2, 11, 3), (2, 11, 4), (2, 11, 6)]  # bulk-copy gathers into a ring
     for vec, kind, stage in shapes:
         Y = torch.empty_like(Xd)
         g.spmm(Xd, Y, group=group, vec=vec, kind=kind, stage=stage)
@@ -453,7 +460,7 @@ def test_autotune_keeps_the_bits(graph_3k, storage):
         X0 = torch.from_numpy(np.random.default_rng(2).standard_normal((n, 64)).astype(np.float32)).cuda()
         before = g.diffuse(X0, 4, out_dtype=torch.float32)
         res = g.autotune(64, reps=2)
-        assert res["ms"] > 0 and res["kind"] in (4, 5, 6, 7, 9, 10)
+        assert res["ms"] > 0 and res["kind"] in (4, 5, 6, 7, 9, 10, 11, 12)
         after = g.diffuse(X0, 4, out_dtype=torch.float32)
         assert torch.equal(before, after)
         assert g.gather_floor(64, reps=2) > 0

@@ -267,6 +267,69 @@ def bench_backward(torch, scl, device, stream, reps, warmup, flush):
             "fwd_bwd_over_fwd": round(t_fb / t_f, 3)}
 
 
+def bench_impute(torch, scl, device, reps, warmup, with_reference=True):
+    """MAGIC imputation through the drop-in C ABI (scl_impute_magic, host
+    buffers in and out, pinned): 100,000 cells, Gaussian kNN affinity (k=15,
+    (W+W^T)/2, not normalised: MAGIC normalises its rows itself), a sparse
+    expression matrix of 100,000 x 1,000 at 5 % density (seeded, values in
+    [0, 1)), t = 3. The same call on scl-core's own CPU implementation
+    (oracle/_ref, all host threads) is timed once beside it and its output
+    compared with the GPU's bit for bit."""
+    import ctypes
+
+    import scipy.sparse as sp
+
+    n, k, G, t = 100_000, 15, 1000, 3
+    pts = scl.synthetic.mixture(n, seed=11)
+    ki, kd = scl.synthetic.knn_device(pts, k, device=device, block=8192)
+    g = scl.gpu.GpuGraph.from_knn(ki, kd)
+    ip, ind, W = g.export()
+    g.close()
+    del ki, kd, pts
+    Xs = sp.random(n, G, density=0.05, random_state=12, format="csr", dtype=np.float32)
+    Xs.sort_indices()
+    pin = lambda a: torch.from_numpy(np.ascontiguousarray(a)).pin_memory().numpy()
+    x_arr = (pin(Xs.indptr.astype(np.int32)), pin(Xs.indices.astype(np.int32)), pin(Xs.data))
+    t_arr = (pin(ip.astype(np.int32)), pin(ind.astype(np.int32)), pin(W.astype(np.float32)))
+    M = scl.CsrMatrix.wrap(*x_arr, (n, G))
+    A = scl.CsrMatrix.wrap(*t_arr, (n, n))
+    out = torch.empty((n, G), dtype=torch.float32).pin_memory().numpy()
+    lib = M.lib
+    P = out.ctypes.data_as(ctypes.POINTER(lib.real_type))
+    ts = []
+    for it in range(warmup + reps):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        rc = lib.scl_impute_magic(M.handle, A.handle, n, G, t, P)
+        dt = time.perf_counter() - t0
+        if rc != 0:
+            raise RuntimeError(f"scl_impute_magic failed: {rc}")
+        if it >= warmup:
+            ts.append(dt)
+    st = scl.diffusion.last_stats(lib)
+    res = {"workload": "MAGIC imputation, 100k cells, kNN affinity k=15, 1,000 genes at 5% density, t=3, "
+                       "host buffers through scl_impute_magic",
+           "cells": n, "genes": G, "expr_nnz": int(Xs.nnz), "graph_nnz": int(ind.size), "t": t,
+           "e2e_ms": round(1e3 * float(np.median(ts)), 3), "device_ms": round(float(st["device_ms"]), 3),
+           "h2d_bytes": int(st["h2d_bytes"]), "d2h_bytes": int(st["d2h_bytes"])}
+    if with_reference:
+        try:
+            from oracle import ref
+
+            R = ref.RefLib("f32_i32")
+            t0 = time.perf_counter()
+            want = R.impute("magic", (Xs.indptr, Xs.indices, Xs.data), (n, G), True, (ip, ind, W), n, G, t)
+            rdt = time.perf_counter() - t0
+            res.update({"reference_cpu_ms": round(1e3 * rdt, 1), "reference_cores": os.cpu_count(),
+                        "reference_lib": R.path.name, "e2e_speedup_vs_reference": round(rdt / float(np.median(ts)), 2),
+                        "bit_identical_to_reference": bool(np.array_equal(want.view(np.uint32),
+                                                                          out.view(np.uint32)))})
+        except Exception as e:  # informational; never fail the run on it
+            res["reference_cpu_ms"] = f"unavailable: {e}"
+    del M, A
+    return res
+
+
 def bench_batched(torch, scl, device, stream, reps, warmup, rank=0, world=1, dist=None):
     """Batched form: 64 graphs, cell counts log-uniform in [2,000, 100,000]
     (seed 0), each its own 10-component mixture, k=15, row-normalised FP32,
@@ -342,6 +405,7 @@ def main():
     ap.add_argument("--no-forms", action="store_true", help="skip the BF16/FP16 forms")
     ap.add_argument("--no-backward", action="store_true", help="skip the forward+backward configuration")
     ap.add_argument("--no-batched", action="store_true", help="skip the batched configuration")
+    ap.add_argument("--no-impute", action="store_true", help="skip the MAGIC imputation configuration")
     args = ap.parse_args()
     warmup = max(3, args.warmup)
 
@@ -498,6 +562,10 @@ def main():
     if not args.no_batched:
         batched = bench_batched(torch, scl, device, stream, args.steps, warmup, rank, world, dist)
 
+    impute = None
+    if rank == 0 and not args.no_impute:
+        impute = bench_impute(torch, scl, device, min(args.steps, 3), 1, with_reference=not args.no_cpu_baseline)
+
     # ---- end to end through the drop-in C ABI with pinned host buffers --------------------
     e2e = None
     if not args.no_e2e:
@@ -568,6 +636,7 @@ def main():
             "fwd_bwd_ms": fwd_bwd["fwd_bwd_ms"] if fwd_bwd else None,
             "fwd_bwd": fwd_bwd,
             "batched": batched,
+            "impute": impute,
             "graph_build_ms": round(build_ms, 3),
             "reorder_ms": round(reorder_ms, 3),
             "reorder_cc_rounds": cc_rounds,

@@ -206,3 +206,57 @@ def adjoint(indptr, indices, W, X0, Y, steps, symmetric=False):
     loss = lib().oracle_adjoint_f64(n, _ptr(indptr), _ptr(indices), _ptr(W), int(symmetric), _ptr(X0), _ptr(Y),
                                     F, steps, _ptr(dX0), _ptr(dW))
     return loss, dX0, dW
+
+
+# ---- imputation (scl/kernel/impute.hpp:599-735) -------------------------------
+def densify(indptr, indices, values, csr, n_cells, n_genes):
+    """The dense block imputation starts from (impute.hpp:608-640, 680-697):
+    zero, then every stored (cell, gene) with cell < n_cells and gene < n_genes
+    in stored order, so a later duplicate overwrites an earlier one. A CSR
+    matrix is cells x genes, a CSC one genes-major."""
+    indptr = np.asarray(indptr, np.int64)
+    ind = np.asarray(indices, np.int64)
+    vals = np.asarray(values)
+    n_prim = min(indptr.size - 1, n_cells if csr else n_genes)
+    end = int(indptr[n_prim])
+    prim = np.repeat(np.arange(n_prim, dtype=np.int64), np.diff(indptr[: n_prim + 1]))
+    sec, v = ind[:end], vals[:end]
+    c, g = (prim, sec) if csr else (sec, prim)
+    ok = (c >= 0) & (c < n_cells) & (g >= 0) & (g < n_genes)
+    pos, v = c[ok] * n_genes + g[ok], v[ok]
+    out = np.zeros(n_cells * n_genes, vals.dtype)
+    if pos.size:
+        _, first_rev = np.unique(pos[::-1], return_index=True)  # last occurrence of each position
+        keep = pos.size - 1 - first_rev
+        out[pos[keep]] = v[keep]
+    return out.reshape(n_cells, n_genes)
+
+
+def impute_diffusion(x_csr, x_is_csr, t_csr, n_cells, n_genes, steps):
+    """impute.hpp:599-661: densify, then `steps` SpMMs over the transition's
+    rows (each output element the sequential fma chain)."""
+    X = densify(*x_csr, x_is_csr, n_cells, n_genes)
+    for _ in range(steps):
+        X = spmm(t_csr[0], t_csr[1], np.asarray(t_csr[2], X.dtype), X)
+    return X
+
+
+def impute_magic(x_csr, x_is_csr, t_csr, n_cells, n_genes, steps):
+    """impute.hpp:668-735: only a CSR matrix seeds the block; affinity rows are
+    summed sequentially in the value precision, weighted a * (1 / sum), and a
+    row whose sum is below 1e-12 keeps its previous values."""
+    dt = np.asarray(t_csr[2]).dtype
+    X = densify(*x_csr, True, n_cells, n_genes) if x_is_csr else np.zeros((n_cells, n_genes), dt)
+    ip = np.asarray(t_csr[0], np.int64)
+    a = np.ascontiguousarray(t_csr[2], dt)
+    sums = row_sums(ip, a)
+    copy = sums < dt.type(1e-12)
+    with np.errstate(divide="ignore", invalid="ignore"):
+        inv = (dt.type(1) / sums).astype(dt)
+        w = (a * np.repeat(inv, np.diff(ip))).astype(dt)
+    w[np.repeat(copy, np.diff(ip))] = 0
+    for _ in range(steps):
+        Y = spmm(ip, t_csr[1], w, X)
+        Y[copy] = X[copy]
+        X = Y
+    return X

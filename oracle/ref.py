@@ -1,7 +1,7 @@
 """ORACLE — test infrastructure only.
 
 ctypes front-end of scl-core's OWN diffusion implementation, compiled from the
-reference sources (scl/binding/c_api/{diffusion,core/core,core/sparse,algebra}.cpp)
+reference sources (scl/binding/c_api/{diffusion,core/core,core/sparse,algebra,impute}.cpp)
 into ``oracle/_ref/libscl_ref_<real>_<index>_<isa>.so`` by ``oracle/Makefile``.
 It is driven exactly the way the reference's Python wrapper drives it
 (python/scl/core/sparse.py:420-459): zero-copy ``scl_sparse_wrap`` of
@@ -74,11 +74,14 @@ class RefLib:
         L.scl_diffusion_diffuse_vector.argtypes = [P, P, ctypes.c_size_t, I]
         L.scl_diffusion_magic_impute.argtypes = [P, P, I, I, I]
         L.scl_algebra_spmm.argtypes = [P, P, I, P, self.c_real, self.c_real]
+        L.scl_impute_diffusion.argtypes = [P, P, I, I, I, P]
+        L.scl_impute_magic.argtypes = [P, P, I, I, I, P]
         L.scl_get_last_error.restype = ctypes.c_char_p
         for fn in ("scl_sparse_wrap", "scl_sparse_create_with_strategy", "scl_sparse_destroy",
                    "scl_sparse_transpose", "scl_sparse_export", "scl_sparse_nnz", "scl_sparse_is_contiguous",
                    "scl_diffusion_compute_transition_matrix", "scl_diffusion_diffuse_matrix",
-                   "scl_diffusion_diffuse_vector", "scl_diffusion_magic_impute", "scl_algebra_spmm"):
+                   "scl_diffusion_diffuse_vector", "scl_diffusion_magic_impute", "scl_algebra_spmm",
+                   "scl_impute_diffusion", "scl_impute_magic"):
             getattr(L, fn).restype = ctypes.c_int32
         self.L = L
 
@@ -166,6 +169,20 @@ class RefLib:
             return Y
         finally:
             self.destroy(h)
+
+    def impute(self, kind, x_csr, x_shape, x_is_csr, t_csr, n_cells, n_genes, steps):
+        """scl_impute_diffusion (kind 'diffusion') or scl_impute_magic on
+        wrapped copies: x_csr / t_csr are (indptr, indices, data) triples."""
+        hx, kx = self.wrap(*x_csr, x_shape, is_csr=x_is_csr)
+        ht, kt = self.wrap(*t_csr, (n_cells, n_cells))
+        out = np.zeros((n_cells, n_genes), self.real_dtype)
+        fn = self.L.scl_impute_diffusion if kind == "diffusion" else self.L.scl_impute_magic
+        try:
+            self._check(fn(hx, ht, n_cells, n_genes, steps, out.ctypes.data))
+            return out
+        finally:
+            self.destroy(ht)
+            self.destroy(hx)
 
     def create_transition_error(self, indptr, indices, data, n, strategy=3):
         """(code, message) of compute_transition_matrix on a block-allocated copy."""

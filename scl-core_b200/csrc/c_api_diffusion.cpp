@@ -7,6 +7,7 @@
 
 #include "abi.hpp"
 #include "scl_diffusion.h"
+#include "scl_impute.h"
 
 using sclabi::Index;
 using sclabi::Real;
@@ -188,6 +189,44 @@ void diffuse_host_block(scl_sparse_matrix& m, Real* X, Index n_nodes, Index n_fe
   t_stats = st;
 }
 
+// Imputation (scl/binding/c_api/impute.cpp:93-157): the sparse expression
+// matrix becomes a dense n_cells x n_genes block on the device, which is
+// diffused over the cells graph and copied back into X_imputed.
+void impute_host(scl_sparse_matrix& X, scl_sparse_matrix& T, Index n_cells, Index n_genes, Index n_steps,
+                 Real* X_imputed, bool magic) {
+  SCL_REQUIRE(X.valid, SCL_ERROR_INVALID_ARGUMENT, "Expression matrix is not valid");
+  SCL_REQUIRE(T.valid, SCL_ERROR_INVALID_ARGUMENT, "Transition matrix is not valid");
+  SCL_REQUIRE(T.primary_dim() == n_cells, SCL_ERROR_DIMENSION_MISMATCH,
+              "Imputation: n_cells must equal the transition matrix's primary dimension");
+  SCL_REQUIRE(T.secondary_dim() <= n_cells, SCL_ERROR_DIMENSION_MISMATCH,
+              "Imputation: column indices would address cells beyond n_cells");
+  SCL_REQUIRE(X.primary_dim() >= (X.is_csr ? n_cells : n_genes), SCL_ERROR_DIMENSION_MISMATCH,
+              "Imputation: the expression matrix has fewer cells (CSR rows) or genes (CSC columns) than requested");
+  const int dev = current_device();
+  cudaStream_t s = library_stream(dev);
+  Stats st;
+  const bool seed = !magic || X.is_csr;  // MAGIC starts from zero for a CSC matrix, as the reference
+  std::shared_ptr<sclabi::DeviceMirror> xm;
+  if (seed) xm = device_graph(X, s, st.h2d);
+  auto tm = device_graph(T, s, st.h2d);
+  const int64_t total = (int64_t)n_cells * n_genes;
+  DevBuf D(std::max<int64_t>(total, 1) * sizeof(Real), s);
+  EventTimer tmr(s);
+  tmr.start();
+  if (seed) densify_expression(xm->g.view(), X.is_csr, n_cells, n_genes, D.p, s);
+  else SCL_CUDA(cudaMemsetAsync(D.p, 0, total * sizeof(Real), s));
+  if (magic)
+    magic_diffuse(tm->g.view(), D.p, n_genes, n_steps, s);
+  else
+    diffuse(tm->g.view(), D.p, sclabi::kRealDType, D.p, sclabi::kRealDType, sclabi::kRealDType, n_genes, n_steps, s);
+  tmr.stop();
+  SCL_CUDA(cudaMemcpyAsync(X_imputed, D.p, total * sizeof(Real), cudaMemcpyDeviceToHost, s));
+  st.d2h += (double)total * sizeof(Real);
+  SCL_CUDA(cudaStreamSynchronize(s));
+  st.device_ms = tmr.ms();
+  t_stats = st;
+}
+
 }  // namespace
 
 extern "C" {
@@ -366,6 +405,39 @@ SCL_EXPORT scl_error_t scl_diffusion_gpu_last_stats(double* device_ms, double* h
   if (h2d_bytes) *h2d_bytes = t_stats.h2d;
   if (d2h_bytes) *d2h_bytes = t_stats.d2h;
   SCL_API_RETURN_OK;
+}
+
+SCL_EXPORT scl_error_t scl_impute_diffusion(scl_sparse_t matrix, scl_sparse_t transition_matrix, scl_index_t n_cells,
+                                            scl_index_t n_genes, scl_index_t n_steps, scl_real_t* X_imputed) {
+  SCL_API_CHECK_NULL(matrix, "Matrix is null");
+  SCL_API_CHECK_NULL(transition_matrix, "Transition matrix is null");
+  SCL_API_CHECK_NULL(X_imputed, "Output imputed matrix is null");
+  SCL_API_CHECK(n_cells > 0 && n_genes > 0 && n_steps > 0, SCL_ERROR_INVALID_ARGUMENT, "Dimensions must be positive");
+  SCL_API_TRY
+  impute_host(*matrix, *transition_matrix, n_cells, n_genes, n_steps, X_imputed, false);
+  SCL_API_RETURN_OK;
+  SCL_API_CATCH
+}
+
+SCL_EXPORT scl_error_t scl_impute_magic(scl_sparse_t matrix, scl_sparse_t affinity_matrix, scl_index_t n_cells,
+                                        scl_index_t n_genes, scl_index_t t, scl_real_t* X_imputed) {
+  SCL_API_CHECK_NULL(matrix, "Matrix is null");
+  SCL_API_CHECK_NULL(affinity_matrix, "Affinity matrix is null");
+  SCL_API_CHECK_NULL(X_imputed, "Output imputed matrix is null");
+  SCL_API_CHECK(n_cells > 0 && n_genes > 0 && t > 0, SCL_ERROR_INVALID_ARGUMENT, "Dimensions must be positive");
+  SCL_API_TRY
+  impute_host(*matrix, *affinity_matrix, n_cells, n_genes, t, X_imputed, true);
+  SCL_API_RETURN_OK;
+  SCL_API_CATCH
+}
+
+SCL_EXPORT scl_error_t scl_impute_knn(scl_sparse_t, const scl_index_t*, const scl_real_t*, scl_index_t, scl_index_t,
+                                      scl_index_t, scl_real_t*, scl_real_t, scl_real_t) {
+  SCL_NOT_IMPLEMENTED("scl_impute_knn");
+}
+SCL_EXPORT scl_error_t scl_impute_knn_weighted(scl_sparse_t, const scl_index_t*, const scl_real_t*, scl_index_t,
+                                               scl_index_t, scl_index_t, scl_real_t*, scl_real_t, scl_real_t) {
+  SCL_NOT_IMPLEMENTED("scl_impute_knn_weighted");
 }
 
 }  // extern "C"

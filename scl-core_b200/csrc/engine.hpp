@@ -268,6 +268,12 @@ void normalize_backward(const CsrView& P, const Adjoint& adj, const void* gPt, c
 // that visits the same column sequence (probe.cu).
 double gather_floor_ms(const int32_t* idx, int64_t M, int64_t n_rows, int64_t row_bytes, int reps, cudaStream_t s);
 
+// Imputation (impute.cu): the dense cells x genes block of a sparse expression
+// matrix (csr: primary = cells, else primary = genes), and MAGIC's t steps
+// X <- W X with W the row-normalised affinity (rows with sum < 1e-12 copy X).
+void densify_expression(const CsrView& m, bool csr, int64_t n_cells, int64_t n_genes, void* dense, cudaStream_t s);
+void magic_diffuse(const CsrView& aff, void* X, int64_t F, int64_t steps, cudaStream_t s);
+
 // dL/dP in CSR order from its CSC-order accumulator.
 void scatter_adjoint_entries(const Adjoint& adj, const void* gPt, DType t, void* gP, cudaStream_t s);
 

@@ -1,0 +1,157 @@
+// Diffusion and MAGIC imputation on the device (scl/kernel/impute.hpp:599-735).
+//
+// Both start from a dense cells x genes block built from a sparse expression
+// matrix and then run t SpMM steps over the cells graph; the steps are this
+// library's SpMM kernels (each output element the sequential fma chain over its
+// row's entries, as scl-core's axpy_simd forms it with MulAdd). MAGIC first
+// normalises the affinity rows the way impute.hpp:700-735 does: a sequential
+// row sum in the storage precision, w = a * (1 / sum) per entry, and rows whose
+// sum is below 1e-12 copy their input row instead of averaging.
+#include <algorithm>
+
+#include "engine.hpp"
+
+namespace sclgpu {
+namespace {
+
+// Zero-initialised X_imputed, then every stored (cell, gene) with cell <
+// n_cells and gene < n_genes written in stored order; a later duplicate of the
+// same position overwrites an earlier one (impute.hpp:608-640, 680-697). A warp
+// walks one primary row (a cell for CSR, a gene for CSC) in chunks of 32; in a
+// chunk only the last lane holding a position writes it, and chunks are
+// ordered by __syncwarp.
+template <class T>
+__global__ void k_densify(const int64_t* __restrict__ ptr, const int32_t* __restrict__ idx, const T* __restrict__ val,
+                          int64_t n_primary, int64_t n_cells, int64_t n_genes, int csr, T* __restrict__ dense) {
+  const int lane = threadIdx.x & 31;
+  const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
+  for (int64_t p = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; p < n_primary; p += nw) {
+    const int64_t s0 = ptr[p], s1 = ptr[p + 1];
+    for (int64_t base = s0; base < s1; base += 32) {
+      const int64_t k = base + lane;
+      int32_t sec = -1;
+      T v = T(0);
+      if (k < s1) {
+        sec = idx[k];
+        v = val[k];
+      }
+      const bool ok = sec >= 0 && (csr ? (int64_t)sec < n_genes : (int64_t)sec < n_cells);
+      const unsigned grp = __match_any_sync(0xffffffffu, ok ? sec : -2 - lane);
+      if (ok && lane == 31 - __clz(grp)) {
+        const int64_t c = csr ? p : (int64_t)sec;
+        const int64_t g = csr ? (int64_t)sec : p;
+        dense[c * n_genes + g] = v;
+      }
+      __syncwarp();
+    }
+  }
+}
+
+// One thread per affinity row: sum its values in stored order (storage
+// precision), then w = a * (1 / sum) for every entry; rows with sum < eps are
+// marked to copy their input row and listed in copy_rows.
+template <class T>
+__global__ void k_magic_weights(const int64_t* __restrict__ ptr, const T* __restrict__ val, int64_t n, T eps,
+                                T* __restrict__ w, int32_t* __restrict__ copy_rows, unsigned long long* n_copy) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t s0 = ptr[i], s1 = ptr[i + 1];
+    T sum = T(0);
+    for (int64_t k = s0; k < s1; ++k) sum += val[k];
+    if (sum < eps) {
+      copy_rows[atomicAdd(n_copy, 1ull)] = (int32_t)i;
+      for (int64_t k = s0; k < s1; ++k) w[k] = T(0);
+    } else {
+      const T inv = T(1) / sum;
+      for (int64_t k = s0; k < s1; ++k) w[k] = val[k] * inv;
+    }
+  }
+}
+
+template <class T>
+__global__ void k_copy_rows(const int32_t* __restrict__ rows, int64_t n_copy, const T* __restrict__ in,
+                            T* __restrict__ out, int64_t F) {
+  const int64_t total = n_copy * F;
+  for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < total; e += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t r = rows[e / F];
+    out[r * F + e % F] = in[r * F + e % F];
+  }
+}
+
+unsigned grid_for(int64_t threads) {
+  int dev = 0;
+  SCL_CUDA(cudaGetDevice(&dev));
+  const int64_t want = (threads + 255) / 256;
+  return (unsigned)std::max<int64_t>(1, std::min<int64_t>(want, (int64_t)sm_count(dev) * 16));
+}
+
+}  // namespace
+
+void densify_expression(const CsrView& m, bool csr, int64_t n_cells, int64_t n_genes, void* dense, cudaStream_t s) {
+  SCL_REQUIRE(m.vtype == kF32 || m.vtype == kF64, kErrTypeMismatch, "expression values must be f32 or f64");
+  const size_t esz = dtype_size(m.vtype);
+  SCL_CUDA(cudaMemsetAsync(dense, 0, (size_t)n_cells * (size_t)n_genes * esz, s));
+  const int64_t n_primary = std::min<int64_t>(m.n_rows, csr ? n_cells : n_genes);
+  if (n_primary <= 0 || m.nnz == 0) return;
+  const unsigned grid = grid_for(n_primary * 32);
+  if (m.vtype == kF32)
+    k_densify<float><<<grid, 256, 0, s>>>(m.indptr, m.indices, static_cast<const float*>(m.values), n_primary,
+                                          n_cells, n_genes, csr ? 1 : 0, static_cast<float*>(dense));
+  else
+    k_densify<double><<<grid, 256, 0, s>>>(m.indptr, m.indices, static_cast<const double*>(m.values), n_primary,
+                                           n_cells, n_genes, csr ? 1 : 0, static_cast<double*>(dense));
+  SCL_CUDA(cudaGetLastError());
+}
+
+void magic_diffuse(const CsrView& aff, void* X, int64_t F, int64_t steps, cudaStream_t s) {
+  SCL_REQUIRE(aff.vtype == kF32 || aff.vtype == kF64, kErrTypeMismatch, "affinity values must be f32 or f64");
+  SCL_REQUIRE(aff.n_cols <= aff.n_rows, kErrDimensionMismatch, "affinity columns must address rows of X");
+  const int64_t n = aff.n_rows;
+  if (steps <= 0 || n == 0 || F == 0) return;
+  const size_t esz = dtype_size(aff.vtype);
+  DevBuf w(std::max<int64_t>(aff.nnz, 1) * esz, s);
+  DevBuf rows(std::max<int64_t>(n, 1) * sizeof(int32_t), s);
+  DevBuf cnt(sizeof(unsigned long long), s);
+  SCL_CUDA(cudaMemsetAsync(cnt.p, 0, sizeof(unsigned long long), s));
+  const unsigned g = grid_for(n);
+  if (aff.vtype == kF32)
+    k_magic_weights<float><<<g, 256, 0, s>>>(aff.indptr, static_cast<const float*>(aff.values), n, 1e-12f,
+                                             w.as<float>(), rows.as<int32_t>(), cnt.as<unsigned long long>());
+  else
+    k_magic_weights<double><<<g, 256, 0, s>>>(aff.indptr, static_cast<const double*>(aff.values), n, 1e-12,
+                                              w.as<double>(), rows.as<int32_t>(), cnt.as<unsigned long long>());
+  SCL_CUDA(cudaGetLastError());
+  unsigned long long n_copy = 0;
+  SCL_CUDA(cudaMemcpyAsync(&n_copy, cnt.p, sizeof(n_copy), cudaMemcpyDeviceToHost, s));
+  SCL_CUDA(cudaStreamSynchronize(s));
+  DevBuf tmp(std::max<int64_t>(n * F, 1) * esz, s);
+  SpmmArgs a{};
+  a.indptr = aff.indptr;
+  a.indices = aff.indices;
+  a.values = w.p;
+  a.vtype = aff.vtype;
+  a.n_rows = n;
+  a.F = F;
+  a.xtype = aff.vtype;
+  a.ytype = aff.vtype;
+  void* in = X;
+  void* out = tmp.p;
+  for (int64_t st = 0; st < steps; ++st) {
+    a.X = in;
+    a.Y = out;
+    spmm(a, s);
+    if (n_copy > 0) {
+      const unsigned gc = grid_for((int64_t)n_copy * F);
+      if (aff.vtype == kF32)
+        k_copy_rows<float><<<gc, 256, 0, s>>>(rows.as<int32_t>(), (int64_t)n_copy, static_cast<const float*>(in),
+                                              static_cast<float*>(out), F);
+      else
+        k_copy_rows<double><<<gc, 256, 0, s>>>(rows.as<int32_t>(), (int64_t)n_copy, static_cast<const double*>(in),
+                                               static_cast<double*>(out), F);
+      SCL_CUDA(cudaGetLastError());
+    }
+    std::swap(in, out);
+  }
+  if (in != X) SCL_CUDA(cudaMemcpyAsync(X, in, (size_t)n * (size_t)F * esz, cudaMemcpyDeviceToDevice, s));
+}
+
+}  // namespace sclgpu

@@ -406,6 +406,7 @@ def main():
     ap.add_argument("--no-backward", action="store_true", help="skip the forward+backward configuration")
     ap.add_argument("--no-batched", action="store_true", help="skip the batched configuration")
     ap.add_argument("--no-impute", action="store_true", help="skip the MAGIC imputation configuration")
+    ap.add_argument("--no-walks", action="store_true", help="skip the personalized PageRank configuration")
     args = ap.parse_args()
     warmup = max(3, args.warmup)
 
@@ -568,6 +569,7 @@ def main():
 
     # ---- end to end through the drop-in C ABI with pinned host buffers --------------------
     e2e = None
+    walks = None
     if not args.no_e2e:
         Xh = torch.empty((n, F), dtype=torch.float32).pin_memory()
         iph = torch.from_numpy(ip.astype(np.int32)).pin_memory()
@@ -596,6 +598,34 @@ def main():
                "ms_per_step": round(1e3 * e_s, 3), "api": "scl_diffusion_diffuse_matrix (libscl_f32_i32.so)",
                "bit_exact_vs_device_path": bool(np.array_equal(Xn.view(np.uint32),
                                                                Y.cpu().numpy().view(np.uint32)))}
+        # personalized PageRank on the same graph and host handle (scl_diffusion_personalized_pagerank,
+        # alpha 0.85, tol 1e-6 on the L1 change, at most 100 steps), beside scl-core's own build
+        if rank == 0 and not args.no_walks:
+            walks = {"workload": "personalized PageRank, 500k cells k=30 row-normalised graph, seed 0, "
+                                 "alpha 0.85, tol 1e-6, max 100 steps, host buffers"}
+            pt = []
+            for it in range(warmup + args.steps):
+                t0 = time.perf_counter()
+                pr = scl.diffusion.personalized_pagerank(m, 0)
+                if it >= warmup:
+                    pt.append(time.perf_counter() - t0)
+            st = scl.diffusion.last_stats(m.lib)
+            walks.update({"e2e_ms": round(1e3 * float(np.median(pt)), 3), "device_ms": round(st["device_ms"], 3),
+                          "h2d_bytes": int(st["h2d_bytes"]), "d2h_bytes": int(st["d2h_bytes"])})
+            if not args.no_cpu_baseline:
+                try:
+                    from oracle import ref
+
+                    R = ref.RefLib("f32_i32")
+                    t0 = time.perf_counter()
+                    want = R.walk("ppr", ip, ind, Pm, n, seed=0, alpha=0.85, max_iter=100, tol=1e-6)
+                    rdt = time.perf_counter() - t0
+                    walks.update({"reference_cpu_ms": round(1e3 * rdt, 1), "reference_cores": os.cpu_count(),
+                                  "e2e_speedup_vs_reference": round(rdt / float(np.median(pt)), 2),
+                                  "max_rel_diff_vs_reference": float(np.max(np.abs(pr - want) /
+                                                                            np.maximum(np.abs(want), 1e-30)))})
+                except Exception as e:  # informational; never fail the run on it
+                    walks["reference_cpu_ms"] = f"unavailable: {e}"
         del m
 
     # ---- CPU baseline (rank 0, N=1) ------------------------------------------------------------
@@ -637,6 +667,7 @@ def main():
             "fwd_bwd": fwd_bwd,
             "batched": batched,
             "impute": impute,
+            "walks": walks,
             "graph_build_ms": round(build_ms, 3),
             "reorder_ms": round(reorder_ms, 3),
             "reorder_cc_rounds": cc_rounds,

@@ -46,8 +46,24 @@ SCL_EXPORT scl_error_t scl_diffusion_diffuse_matrix(scl_sparse_t transition, scl
 SCL_EXPORT scl_error_t scl_diffusion_magic_impute(scl_sparse_t transition, scl_real_t* X, scl_index_t n_nodes,
                                                   scl_index_t n_features, scl_index_t t);
 
-/* The remaining scl-core diffusion entry points (diffusion.h:38-96,108-119) are
- * exported for link compatibility and return SCL_ERROR_NOT_IMPLEMENTED. */
+/* Vector walks (diffusion.h:58-96, 119; diffusion.cpp:179-248, 285-312,
+ * 375-399): scl_diffusion_random_walk_with_restart,
+ * scl_diffusion_personalized_pagerank, scl_diffusion_heat_kernel_signature and
+ * scl_diffusion_lazy_random_walk keep the reference's arguments, defaults
+ * (alpha 0 -> 0.85, tol 0 -> 1e-6, max_iter 0 -> 100, HKS steps 0 -> 10,
+ * laziness 0 -> 0.5), checks and the restart walk's buffer swap (after an
+ * unconverged last step the caller's array holds the previous iterate, as in
+ * the reference). Each step is one kernel: (P x)_i as the sequential fma chain,
+ * then y = fma(c_x, x, c_p (P x)) (lazy, HKS) or y = fma(alpha, (P x),
+ * (1 - alpha) r) (restart); the restart walk's L1 change is summed in FP64.
+ * scl-core's own SpMV rounding depends on its compiler's contraction, so these
+ * agree with it to a few ulps rather than bit for bit. The walk's size is the
+ * handle's primary dimension; n_nodes must be at least that
+ * (SCL_ERROR_DIMENSION_MISMATCH otherwise).
+ *
+ * DPT, diffusion map embedding and diffusion distance (diffusion.h:38-55,
+ * 79-84, 108-113) are exported for link compatibility and return
+ * SCL_ERROR_NOT_IMPLEMENTED. */
 SCL_EXPORT scl_error_t scl_diffusion_compute_dpt(scl_sparse_t transition, scl_index_t root_cell,
                                                  scl_real_t* pseudotime, scl_size_t n_nodes, scl_index_t max_iter,
                                                  scl_real_t tol);

@@ -493,3 +493,103 @@ double oracle_adjoint_f64(int64_t n, const int64_t* indptr, const int64_t* indic
   free(u); free(v); free(gP); free(G); free(Gn); free(Xs); free(P); free(d);
   return loss;
 }
+
+/* ===================================================================== */
+/* Vector walks — diffusion.hpp:833-900 (random walk with restart),       */
+/* 961-1007 (heat-kernel signature), 1157-1194 (lazy random walk), on    */
+/* spmv_parallel (169-221). Each (P x)_i is the sequential fma chain over */
+/* the row's entries; the step's combination is rounded as               */
+/*   lazy / heat kernel: y = fma(c_x, x, c_p * (P x))                     */
+/*   restart:            y = fma(alpha, (P x), (1 - alpha) * r)           */
+/* The restart walk's convergence sum is sum |y - x| (differences in the */
+/* value type, summed in double in row order) and stops when it is below */
+/* tol; buffers swap after every step that has not converged, so the    */
+/* caller's array ends with the last iterate written into it.           */
+/* ===================================================================== */
+void oracle_walk_linear_f32(int64_t n, const int64_t* indptr, const int64_t* indices, const float* values, float* x,
+                            int64_t steps, float cx, float cp) {
+  float* y = (float*)malloc(sizeof(float) * (size_t)(n > 0 ? n : 1));
+  for (int64_t st = 0; st < steps; ++st) {
+    for (int64_t i = 0; i < n; ++i) {
+      float s = 0.0f;
+      for (int64_t p = indptr[i]; p < indptr[i + 1]; ++p) s = fmaf(values[p], x[indices[p]], s);
+      y[i] = fmaf(cx, x[i], cp * s);
+    }
+    memcpy(x, y, sizeof(float) * (size_t)n);
+  }
+  free(y);
+}
+
+void oracle_walk_linear_f64(int64_t n, const int64_t* indptr, const int64_t* indices, const double* values, double* x,
+                            int64_t steps, double cx, double cp) {
+  double* y = (double*)malloc(sizeof(double) * (size_t)(n > 0 ? n : 1));
+  for (int64_t st = 0; st < steps; ++st) {
+    for (int64_t i = 0; i < n; ++i) {
+      double s = 0.0;
+      for (int64_t p = indptr[i]; p < indptr[i + 1]; ++p) s = fma(values[p], x[indices[p]], s);
+      y[i] = fma(cx, x[i], cp * s);
+    }
+    memcpy(x, y, sizeof(double) * (size_t)n);
+  }
+  free(y);
+}
+
+int64_t oracle_walk_restart_f32(int64_t n, const int64_t* indptr, const int64_t* indices, const float* values,
+                                const float* r, float* scores, float alpha, int64_t max_iter, float tol) {
+  float* tmp = (float*)malloc(sizeof(float) * (size_t)(n > 0 ? n : 1));
+  float* cur = scores;
+  float* nxt = tmp;
+  const float beta = 1.0f - alpha;
+  int64_t it = 0;
+  for (; it < max_iter; ++it) {
+    double l1 = 0.0;
+    for (int64_t i = 0; i < n; ++i) {
+      float s = 0.0f;
+      for (int64_t p = indptr[i]; p < indptr[i + 1]; ++p) s = fmaf(values[p], cur[indices[p]], s);
+      const float y = fmaf(alpha, s, beta * r[i]);
+      const float d = y - cur[i];
+      l1 += (double)(d >= 0.0f ? d : -d);
+      nxt[i] = y;
+    }
+    if (l1 < (double)tol) {
+      memcpy(cur, nxt, sizeof(float) * (size_t)n);
+      ++it;
+      break;
+    }
+    float* t = cur;
+    cur = nxt;
+    nxt = t;
+  }
+  free(tmp);
+  return it;
+}
+
+int64_t oracle_walk_restart_f64(int64_t n, const int64_t* indptr, const int64_t* indices, const double* values,
+                                const double* r, double* scores, double alpha, int64_t max_iter, double tol) {
+  double* tmp = (double*)malloc(sizeof(double) * (size_t)(n > 0 ? n : 1));
+  double* cur = scores;
+  double* nxt = tmp;
+  const double beta = 1.0 - alpha;
+  int64_t it = 0;
+  for (; it < max_iter; ++it) {
+    double l1 = 0.0;
+    for (int64_t i = 0; i < n; ++i) {
+      double s = 0.0;
+      for (int64_t p = indptr[i]; p < indptr[i + 1]; ++p) s = fma(values[p], cur[indices[p]], s);
+      const double y = fma(alpha, s, beta * r[i]);
+      const double d = y - cur[i];
+      l1 += (d >= 0.0 ? d : -d);
+      nxt[i] = y;
+    }
+    if (l1 < tol) {
+      memcpy(cur, nxt, sizeof(double) * (size_t)n);
+      ++it;
+      break;
+    }
+    double* t = cur;
+    cur = nxt;
+    nxt = t;
+  }
+  free(tmp);
+  return it;
+}

@@ -14,6 +14,8 @@
  *   - Gaussian kNN affinity + (W+W^T)/2 union (no single reference function:
  *       scl/kernel/kernel.hpp:403-453 local_bandwidth, scl/kernel/impute.hpp:156-159
  *       distance_to_weight, scl/kernel/neighbors.hpp:319-478 kNN list format)
+ *   - vector walks: lazy random walk, heat-kernel signature, random walk with
+ *       restart (scl/kernel/diffusion.hpp:833-900, 961-1007, 1157-1194)
  *   - BF16/FP16 storage variants and the FP64 adjoint (new in this project).
  *
  * Arithmetic contract: every multiply-add that the reference performs through
@@ -108,6 +110,16 @@ int64_t oracle_symmetrize_f32(int64_t n, int64_t k, const int64_t* knn_idx, cons
 double oracle_adjoint_f64(int64_t n, const int64_t* indptr, const int64_t* indices,
                           const double* W, int symmetric, const double* X0, const double* Y,
                           int64_t F, int64_t steps, double* dX0, double* dW);
+
+/* ---- vector walks (diffusion.hpp:833-900, 961-1007, 1157-1194) ------ */
+void oracle_walk_linear_f32(int64_t n, const int64_t* indptr, const int64_t* indices, const float* values, float* x,
+                            int64_t steps, float cx, float cp);
+void oracle_walk_linear_f64(int64_t n, const int64_t* indptr, const int64_t* indices, const double* values, double* x,
+                            int64_t steps, double cx, double cp);
+int64_t oracle_walk_restart_f32(int64_t n, const int64_t* indptr, const int64_t* indices, const float* values,
+                                const float* r, float* scores, float alpha, int64_t max_iter, float tol);
+int64_t oracle_walk_restart_f64(int64_t n, const int64_t* indptr, const int64_t* indices, const double* values,
+                                const double* r, double* scores, double alpha, int64_t max_iter, double tol);
 
 #ifdef __cplusplus
 }

@@ -42,6 +42,10 @@ _SIGS = {
     "oracle_symmetrize_f64": ([_i64, _i64, _p, _p, _p, _p, _p], _i64),
     "oracle_symmetrize_f32": ([_i64, _i64, _p, _p, _p, _p, _p], _i64),
     "oracle_adjoint_f64": ([_i64, _p, _p, _p, _int, _p, _p, _i64, _i64, _p, _p], ctypes.c_double),
+    "oracle_walk_linear_f32": ([_i64, _p, _p, _p, _p, _i64, ctypes.c_float, ctypes.c_float], None),
+    "oracle_walk_linear_f64": ([_i64, _p, _p, _p, _p, _i64, ctypes.c_double, ctypes.c_double], None),
+    "oracle_walk_restart_f32": ([_i64, _p, _p, _p, _p, _p, ctypes.c_float, _i64, ctypes.c_float], _i64),
+    "oracle_walk_restart_f64": ([_i64, _p, _p, _p, _p, _p, ctypes.c_double, _i64, ctypes.c_double], _i64),
 }
 
 
@@ -260,3 +264,45 @@ def impute_magic(x_csr, x_is_csr, t_csr, n_cells, n_genes, steps):
         Y[copy] = X[copy]
         X = Y
     return X
+
+
+# ---- vector walks (scl/kernel/diffusion.hpp:833-900, 961-1007, 1157-1194) -----
+def walk_linear(indptr, indices, values, x, steps, c_x, c_p):
+    """x <- fma(c_x, x, c_p * (P x)), `steps` times (lazy random walk and the
+    heat-kernel signature); dtype follows x."""
+    indptr, indices = _csr(indptr, indices)
+    n = indptr.size - 1
+    x = np.array(x, copy=True)
+    v = np.ascontiguousarray(values, x.dtype)
+    fn = lib().oracle_walk_linear_f32 if x.dtype == np.float32 else lib().oracle_walk_linear_f64
+    fn(n, _ptr(indptr), _ptr(indices), _ptr(v), _ptr(x), int(steps), float(c_x), float(c_p))
+    return x
+
+
+def restart_vector(seeds, n, dtype):
+    """diffusion.hpp:852-870: 1 on every in-range seed, divided by the number
+    of in-range seeds (repeats counted); None when there is none."""
+    r = np.zeros(n, dtype)
+    count = 0
+    for s in seeds:
+        if 0 <= int(s) < n:
+            r[int(s)] = 1
+            count += 1
+    if count == 0:
+        return None
+    return (r * (dtype(1) / dtype(count))).astype(dtype)
+
+
+def walk_restart(indptr, indices, values, seeds, n, alpha, max_iter, tol, dtype=np.float32):
+    """Random walk with restart as scl-core runs it (scores start as the
+    restart vector; buffers swap after each unconverged step). Returns
+    (scores, steps taken)."""
+    indptr, indices = _csr(indptr, indices)
+    r = restart_vector(seeds, n, dtype)
+    if r is None:
+        return np.zeros(n, dtype), 0
+    scores = r.copy()
+    v = np.ascontiguousarray(values, dtype)
+    fn = lib().oracle_walk_restart_f32 if dtype == np.float32 else lib().oracle_walk_restart_f64
+    it = fn(n, _ptr(indptr), _ptr(indices), _ptr(v), _ptr(r), _ptr(scores), float(alpha), int(max_iter), float(tol))
+    return scores, int(it)

@@ -75,13 +75,20 @@ class RefLib:
         L.scl_diffusion_magic_impute.argtypes = [P, P, I, I, I]
         L.scl_algebra_spmm.argtypes = [P, P, I, P, self.c_real, self.c_real]
         L.scl_impute_diffusion.argtypes = [P, P, I, I, I, P]
+        R_ = self.c_real
+        L.scl_diffusion_random_walk_with_restart.argtypes = [P, P, ctypes.c_size_t, P, ctypes.c_size_t, R_, I, R_]
+        L.scl_diffusion_personalized_pagerank.argtypes = [P, I, P, ctypes.c_size_t, R_, I, R_]
+        L.scl_diffusion_lazy_random_walk.argtypes = [P, P, ctypes.c_size_t, I, R_]
+        L.scl_diffusion_heat_kernel_signature.argtypes = [P, P, ctypes.c_size_t, R_, I]
         L.scl_impute_magic.argtypes = [P, P, I, I, I, P]
         L.scl_get_last_error.restype = ctypes.c_char_p
         for fn in ("scl_sparse_wrap", "scl_sparse_create_with_strategy", "scl_sparse_destroy",
                    "scl_sparse_transpose", "scl_sparse_export", "scl_sparse_nnz", "scl_sparse_is_contiguous",
                    "scl_diffusion_compute_transition_matrix", "scl_diffusion_diffuse_matrix",
                    "scl_diffusion_diffuse_vector", "scl_diffusion_magic_impute", "scl_algebra_spmm",
-                   "scl_impute_diffusion", "scl_impute_magic"):
+                   "scl_impute_diffusion", "scl_impute_magic", "scl_diffusion_random_walk_with_restart",
+                   "scl_diffusion_personalized_pagerank", "scl_diffusion_lazy_random_walk",
+                   "scl_diffusion_heat_kernel_signature"):
             getattr(L, fn).restype = ctypes.c_int32
         self.L = L
 
@@ -183,6 +190,35 @@ class RefLib:
         finally:
             self.destroy(ht)
             self.destroy(hx)
+
+    def walk(self, kind, indptr, indices, data, n, out_len=None, **kw):
+        """The vector walks on a wrapped n x n handle: kind 'rwr' (seeds, alpha,
+        max_iter, tol), 'ppr' (seed, alpha, max_iter, tol), 'lazy' (x, steps,
+        laziness) or 'hks' (t, steps). Returns the output vector."""
+        h, keep = self.wrap(indptr, indices, data, (n, n))
+        m = n if out_len is None else out_len
+        try:
+            if kind == "lazy":
+                out = np.array(kw["x"], dtype=self.real_dtype, copy=True)
+                self._check(self.L.scl_diffusion_lazy_random_walk(h, out.ctypes.data, out.size, kw["steps"],
+                                                                  kw.get("laziness", 0.5)))
+                return out
+            out = np.full(m, -7.0, self.real_dtype)
+            if kind == "hks":
+                self._check(self.L.scl_diffusion_heat_kernel_signature(h, out.ctypes.data, m, kw.get("t", 1.0),
+                                                                       kw.get("steps", 10)))
+            elif kind == "ppr":
+                self._check(self.L.scl_diffusion_personalized_pagerank(h, kw["seed"], out.ctypes.data, m,
+                                                                       kw.get("alpha", 0.85), kw.get("max_iter", 100),
+                                                                       kw.get("tol", 1e-6)))
+            else:
+                seeds = np.ascontiguousarray(kw["seeds"], self.index_dtype)
+                self._check(self.L.scl_diffusion_random_walk_with_restart(
+                    h, seeds.ctypes.data, seeds.size, out.ctypes.data, m, kw.get("alpha", 0.85),
+                    kw.get("max_iter", 100), kw.get("tol", 1e-6)))
+            return out
+        finally:
+            self.destroy(h)
 
     def create_transition_error(self, indptr, indices, data, n, strategy=3):
         """(code, message) of compute_transition_matrix on a block-allocated copy."""

@@ -227,6 +227,94 @@ void impute_host(scl_sparse_matrix& X, scl_sparse_matrix& T, Index n_cells, Inde
   t_stats = st;
 }
 
+// Vector walks (diffusion.cpp:179-248, 285-312, 375-399): the handle's
+// primary dimension n is the walk's size; the caller's vector must hold at
+// least n entries (only those are read and written).
+struct WalkSetup {
+  int dev;
+  cudaStream_t s;
+  std::shared_ptr<sclabi::DeviceMirror> mir;
+  Index n;
+};
+
+WalkSetup walk_setup(scl_sparse_matrix& m, size_t n_nodes, const char* too_small, Stats& st) {
+  SCL_REQUIRE(m.valid, SCL_ERROR_INVALID_ARGUMENT, "Transition matrix is not valid");
+  const Index n = m.primary_dim();
+  SCL_REQUIRE(n_nodes >= (size_t)n, SCL_ERROR_DIMENSION_MISMATCH, too_small);
+  SCL_REQUIRE(m.secondary_dim() <= n, SCL_ERROR_DIMENSION_MISMATCH,
+              "Walk: column indices would address entries beyond the vector");
+  WalkSetup w;
+  w.dev = current_device();
+  w.s = library_stream(w.dev);
+  w.mir = device_graph(m, w.s, st.h2d);
+  w.n = n;
+  return w;
+}
+
+// x <- c_x x + c_p P x, `steps` times, on the first n entries of x.
+void walk_linear_host(scl_sparse_matrix& m, Real* x, size_t n_nodes, Index steps, Real c_x, Real c_p,
+                      const char* too_small) {
+  Stats st;
+  WalkSetup w = walk_setup(m, n_nodes, too_small, st);
+  if (w.n == 0 || steps <= 0) return;
+  DevBuf xd(w.n * sizeof(Real), w.s);
+  SCL_CUDA(cudaMemcpyAsync(xd.p, x, w.n * sizeof(Real), cudaMemcpyHostToDevice, w.s));
+  st.h2d += (double)w.n * sizeof(Real);
+  EventTimer tm(w.s);
+  tm.start();
+  walk_linear(w.mir->g.view(), xd.p, steps, (double)c_x, (double)c_p, w.s);
+  tm.stop();
+  SCL_CUDA(cudaMemcpyAsync(x, xd.p, w.n * sizeof(Real), cudaMemcpyDeviceToHost, w.s));
+  st.d2h += (double)w.n * sizeof(Real);
+  SCL_CUDA(cudaStreamSynchronize(w.s));
+  st.device_ms = tm.ms();
+  t_stats = st;
+}
+
+// random_walk_with_restart (diffusion.hpp:833-895): restart = 1 / (number of
+// in-range seeds, repeats counted) on every in-range seed; no in-range seed
+// gives zero scores.
+void walk_restart_host(scl_sparse_matrix& m, const Index* seeds, size_t n_seeds, Real* scores, size_t n_nodes,
+                       Real alpha, Index max_iter, Real tol) {
+  Stats st;
+  WalkSetup w = walk_setup(m, n_nodes, "RWR: output buffer too small", st);
+  if (w.n == 0) return;
+  std::vector<Real> r((size_t)w.n, Real(0));
+  size_t count = 0;
+  for (size_t i = 0; i < n_seeds; ++i) {
+    const Index idx = seeds[i];
+    if (idx >= 0 && idx < w.n) {
+      r[(size_t)idx] = Real(1);
+      ++count;
+    }
+  }
+  if (count == 0) {
+    std::memset(scores, 0, (size_t)w.n * sizeof(Real));
+    return;
+  }
+  const Real inv = Real(1) / static_cast<Real>(count);
+  for (Real& v : r) v *= inv;
+  DevBuf rd(w.n * sizeof(Real), w.s), sd(w.n * sizeof(Real), w.s);
+  SCL_CUDA(cudaMemcpyAsync(rd.p, r.data(), w.n * sizeof(Real), cudaMemcpyHostToDevice, w.s));
+  SCL_CUDA(cudaMemcpyAsync(sd.p, rd.p, w.n * sizeof(Real), cudaMemcpyDeviceToDevice, w.s));
+  st.h2d += (double)w.n * sizeof(Real);
+  EventTimer tm(w.s);
+  tm.start();
+  walk_restart(w.mir->g.view(), rd.p, sd.p, (double)alpha, max_iter, (double)tol, w.s);
+  tm.stop();
+  SCL_CUDA(cudaMemcpyAsync(scores, sd.p, w.n * sizeof(Real), cudaMemcpyDeviceToHost, w.s));
+  st.d2h += (double)w.n * sizeof(Real);
+  SCL_CUDA(cudaStreamSynchronize(w.s));
+  st.device_ms = tm.ms();
+  t_stats = st;
+}
+
+constexpr Real kDefaultAlpha = Real(0.85);  // diffusion.cpp:20-27
+constexpr Real kDefaultTol = Real(1e-6);
+constexpr Index kDefaultMaxIter = 100;
+constexpr Index kDefaultStepsHks = 10;
+constexpr Real kDefaultLaziness = Real(0.5);
+
 }  // namespace
 
 extern "C" {
@@ -344,27 +432,69 @@ SCL_EXPORT scl_error_t scl_diffusion_compute_dpt_multi_root(scl_sparse_t, const 
                                                             scl_size_t, scl_index_t) {
   SCL_NOT_IMPLEMENTED("scl_diffusion_compute_dpt_multi_root");
 }
-SCL_EXPORT scl_error_t scl_diffusion_random_walk_with_restart(scl_sparse_t, const scl_index_t*, scl_size_t, scl_real_t*,
-                                                              scl_size_t, scl_real_t, scl_index_t, scl_real_t) {
-  SCL_NOT_IMPLEMENTED("scl_diffusion_random_walk_with_restart");
+SCL_EXPORT scl_error_t scl_diffusion_random_walk_with_restart(scl_sparse_t transition, const scl_index_t* seed_nodes,
+                                                              scl_size_t n_seeds, scl_real_t* scores,
+                                                              scl_size_t n_nodes, scl_real_t alpha,
+                                                              scl_index_t max_iter, scl_real_t tol) {
+  SCL_API_CHECK_NULL(transition, "Transition matrix is null");
+  SCL_API_CHECK_NULL(seed_nodes, "Seed nodes array is null");
+  SCL_API_CHECK_NULL(scores, "Output scores array is null");
+  SCL_API_CHECK(n_seeds > 0 && n_nodes > 0, SCL_ERROR_INVALID_ARGUMENT, "Dimensions must be positive");
+  SCL_API_CHECK(alpha >= 0 && alpha <= 1, SCL_ERROR_INVALID_ARGUMENT, "Alpha must be in [0, 1]");
+  SCL_API_TRY
+  walk_restart_host(*transition, seed_nodes, n_seeds, scores, n_nodes, alpha == Real(0) ? kDefaultAlpha : alpha,
+                    max_iter == 0 ? kDefaultMaxIter : max_iter, tol == Real(0) ? kDefaultTol : tol);
+  SCL_API_RETURN_OK;
+  SCL_API_CATCH
 }
-SCL_EXPORT scl_error_t scl_diffusion_personalized_pagerank(scl_sparse_t, scl_index_t, scl_real_t*, scl_size_t,
-                                                           scl_real_t, scl_index_t, scl_real_t) {
-  SCL_NOT_IMPLEMENTED("scl_diffusion_personalized_pagerank");
+SCL_EXPORT scl_error_t scl_diffusion_personalized_pagerank(scl_sparse_t transition, scl_index_t seed_node,
+                                                           scl_real_t* scores, scl_size_t n_nodes, scl_real_t alpha,
+                                                           scl_index_t max_iter, scl_real_t tol) {
+  SCL_API_CHECK_NULL(transition, "Transition matrix is null");
+  SCL_API_CHECK_NULL(scores, "Output scores array is null");
+  SCL_API_CHECK(n_nodes > 0, SCL_ERROR_INVALID_ARGUMENT, "Number of nodes must be positive");
+  SCL_API_CHECK(alpha >= 0 && alpha <= 1, SCL_ERROR_INVALID_ARGUMENT, "Alpha must be in [0, 1]");
+  SCL_API_TRY
+  const Index seed = seed_node;
+  walk_restart_host(*transition, &seed, 1, scores, n_nodes, alpha == Real(0) ? kDefaultAlpha : alpha,
+                    max_iter == 0 ? kDefaultMaxIter : max_iter, tol == Real(0) ? kDefaultTol : tol);
+  SCL_API_RETURN_OK;
+  SCL_API_CATCH
 }
 SCL_EXPORT scl_error_t scl_diffusion_diffusion_map_embedding(scl_sparse_t, scl_real_t*, scl_index_t, scl_index_t,
                                                              scl_index_t) {
   SCL_NOT_IMPLEMENTED("scl_diffusion_diffusion_map_embedding");
 }
-SCL_EXPORT scl_error_t scl_diffusion_heat_kernel_signature(scl_sparse_t, scl_real_t*, scl_size_t, scl_real_t,
-                                                           scl_index_t) {
-  SCL_NOT_IMPLEMENTED("scl_diffusion_heat_kernel_signature");
+SCL_EXPORT scl_error_t scl_diffusion_heat_kernel_signature(scl_sparse_t transition, scl_real_t* signature,
+                                                           scl_size_t n_nodes, scl_real_t t, scl_index_t n_steps) {
+  SCL_API_CHECK_NULL(transition, "Transition matrix is null");
+  SCL_API_CHECK_NULL(signature, "Output signature array is null");
+  SCL_API_CHECK(n_nodes > 0, SCL_ERROR_INVALID_ARGUMENT, "Number of nodes must be positive");
+  SCL_API_CHECK(t > 0, SCL_ERROR_INVALID_ARGUMENT, "Time parameter t must be positive");
+  SCL_API_TRY
+  const Index steps = (n_steps == 0) ? kDefaultStepsHks : n_steps;
+  const Index n = transition->primary_dim();
+  SCL_REQUIRE(n_nodes >= (size_t)n, SCL_ERROR_DIMENSION_MISMATCH, "HKS: output buffer too small");
+  for (Index i = 0; i < n; ++i) signature[i] = Real(1);  // diffusion.hpp:975 (identity diagonal)
+  const Real dt = t / static_cast<Real>(steps);
+  walk_linear_host(*transition, signature, n_nodes, steps, Real(1) - dt, dt, "HKS: output buffer too small");
+  SCL_API_RETURN_OK;
+  SCL_API_CATCH
 }
 SCL_EXPORT scl_error_t scl_diffusion_diffusion_distance(scl_sparse_t, scl_real_t*, scl_size_t, scl_index_t) {
   SCL_NOT_IMPLEMENTED("scl_diffusion_diffusion_distance");
 }
-SCL_EXPORT scl_error_t scl_diffusion_lazy_random_walk(scl_sparse_t, scl_real_t*, scl_size_t, scl_index_t, scl_real_t) {
-  SCL_NOT_IMPLEMENTED("scl_diffusion_lazy_random_walk");
+SCL_EXPORT scl_error_t scl_diffusion_lazy_random_walk(scl_sparse_t transition, scl_real_t* x, scl_size_t n_nodes,
+                                                      scl_index_t n_steps, scl_real_t laziness) {
+  SCL_API_CHECK_NULL(transition, "Transition matrix is null");
+  SCL_API_CHECK_NULL(x, "Vector x is null");
+  SCL_API_CHECK(n_nodes > 0 && n_steps > 0, SCL_ERROR_INVALID_ARGUMENT, "Dimensions must be positive");
+  SCL_API_CHECK(laziness >= 0 && laziness <= 1, SCL_ERROR_INVALID_ARGUMENT, "Laziness must be in [0, 1]");
+  SCL_API_TRY
+  const Real lazy = (laziness == Real(0)) ? kDefaultLaziness : laziness;
+  walk_linear_host(*transition, x, n_nodes, n_steps, lazy, Real(1) - lazy, "LazyRW: vector size mismatch");
+  SCL_API_RETURN_OK;
+  SCL_API_CATCH
 }
 
 SCL_EXPORT scl_error_t scl_diffusion_gpu_set_degree_mode(int mode) {

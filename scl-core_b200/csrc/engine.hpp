@@ -274,6 +274,14 @@ double gather_floor_ms(const int32_t* idx, int64_t M, int64_t n_rows, int64_t ro
 void densify_expression(const CsrView& m, bool csr, int64_t n_cells, int64_t n_genes, void* dense, cudaStream_t s);
 void magic_diffuse(const CsrView& aff, void* X, int64_t F, int64_t steps, cudaStream_t s);
 
+// Vector walks (walks.cu). walk_linear: x <- c_x x + c_p P x, `steps` times
+// (lazy random walk, heat-kernel signature). walk_restart: the restart walk
+// y = alpha P x + (1 - alpha) r until the L1 change is below tol or max_iter
+// steps, scores holding r on entry; returns the steps taken.
+void walk_linear(const CsrView& P, void* x, int64_t steps, double c_x, double c_p, cudaStream_t s);
+int64_t walk_restart(const CsrView& P, const void* r, void* scores, double alpha, int64_t max_iter, double tol,
+                     cudaStream_t s);
+
 // dL/dP in CSR order from its CSC-order accumulator.
 void scatter_adjoint_entries(const Adjoint& adj, const void* gPt, DType t, void* gP, cudaStream_t s);
 

@@ -52,6 +52,49 @@ def magic_impute(mat: CsrMatrix, X: np.ndarray, t: int = 0) -> np.ndarray:
     return X
 
 
+def random_walk_with_restart(mat: CsrMatrix, seeds, n_nodes: int = None, alpha: float = 0.85, max_iter: int = 100,
+                             tol: float = 1e-6) -> np.ndarray:
+    """Scores of the walk that restarts on `seeds` (scl_diffusion_random_walk_with_restart)."""
+    lib = mat.lib
+    n = mat.shape[0] if n_nodes is None else int(n_nodes)
+    seeds = np.ascontiguousarray(seeds, dtype=mat.index_dtype)
+    out = np.zeros(n, dtype=mat.real_dtype)
+    check_error(lib.scl_diffusion_random_walk_with_restart(
+        mat.handle, seeds.ctypes.data_as(ctypes.POINTER(lib.index_type)), seeds.size,
+        out.ctypes.data_as(ctypes.POINTER(lib.real_type)), n, alpha, int(max_iter), tol),
+        "random_walk_with_restart", lib)
+    return out
+
+
+def personalized_pagerank(mat: CsrMatrix, seed: int, n_nodes: int = None, alpha: float = 0.85, max_iter: int = 100,
+                          tol: float = 1e-6) -> np.ndarray:
+    lib = mat.lib
+    n = mat.shape[0] if n_nodes is None else int(n_nodes)
+    out = np.zeros(n, dtype=mat.real_dtype)
+    check_error(lib.scl_diffusion_personalized_pagerank(mat.handle, int(seed),
+                                                        out.ctypes.data_as(ctypes.POINTER(lib.real_type)), n, alpha,
+                                                        int(max_iter), tol), "personalized_pagerank", lib)
+    return out
+
+
+def heat_kernel_signature(mat: CsrMatrix, n_nodes: int = None, t: float = 1.0, n_steps: int = 10) -> np.ndarray:
+    lib = mat.lib
+    n = mat.shape[0] if n_nodes is None else int(n_nodes)
+    out = np.zeros(n, dtype=mat.real_dtype)
+    check_error(lib.scl_diffusion_heat_kernel_signature(mat.handle, out.ctypes.data_as(ctypes.POINTER(lib.real_type)),
+                                                        n, t, int(n_steps)), "heat_kernel_signature", lib)
+    return out
+
+
+def lazy_random_walk(mat: CsrMatrix, x: np.ndarray, n_steps: int, laziness: float = 0.5) -> np.ndarray:
+    """x <- laziness x + (1 - laziness) P x, n_steps times, in place; returns x."""
+    x = _as_real(mat, x)
+    P = ctypes.POINTER(mat.lib.real_type)
+    check_error(mat.lib.scl_diffusion_lazy_random_walk(mat.handle, x.ctypes.data_as(P), x.shape[0], int(n_steps),
+                                                       laziness), "lazy_random_walk", mat.lib)
+    return x
+
+
 def set_degree_mode(mat_or_lib, mode: int) -> None:
     """0 = FP64 degrees (default), 1 = value-type degrees as scl-core computes them."""
     lib = getattr(mat_or_lib, "lib", mat_or_lib)

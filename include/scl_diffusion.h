@@ -61,9 +61,17 @@ SCL_EXPORT scl_error_t scl_diffusion_magic_impute(scl_sparse_t transition, scl_r
  * handle's primary dimension; n_nodes must be at least that
  * (SCL_ERROR_DIMENSION_MISMATCH otherwise).
  *
- * DPT, diffusion map embedding and diffusion distance (diffusion.h:38-55,
- * 79-84, 108-113) are exported for link compatibility and return
- * SCL_ERROR_NOT_IMPLEMENTED. */
+ * Diffusion pseudotime (diffusion.h:38-55; diffusion.cpp:122-172;
+ * diffusion.hpp:670-831): scl_diffusion_compute_dpt walks from one root
+ * (max_iter 0 -> 100, tol 0 -> 1e-6; a root outside the graph is
+ * SCL_ERROR_INVALID_ARGUMENT), accumulating hitting times and visit
+ * probabilities until the largest unvisited probability is below tol, then
+ * scales the visited rows' (> 0.5) mean hitting times to [0, 1] (others 1);
+ * scl_diffusion_compute_dpt_multi_root averages that over the in-range roots
+ * (none: all ones), each walked with the default tolerance.
+ *
+ * Diffusion map embedding and diffusion distance (diffusion.h:79-84, 108-113)
+ * are exported for link compatibility and return SCL_ERROR_NOT_IMPLEMENTED. */
 SCL_EXPORT scl_error_t scl_diffusion_compute_dpt(scl_sparse_t transition, scl_index_t root_cell,
                                                  scl_real_t* pseudotime, scl_size_t n_nodes, scl_index_t max_iter,
                                                  scl_real_t tol);

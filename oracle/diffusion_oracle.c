@@ -593,3 +593,62 @@ int64_t oracle_walk_restart_f64(int64_t n, const int64_t* indptr, const int64_t*
   free(tmp);
   return it;
 }
+
+/* ===================================================================== */
+/* Diffusion pseudotime — diffusion.hpp:670-772 (one root). p starts as   */
+/* the root's indicator; each step p_new = P p (sequential fma chains),  */
+/* then rows with visited < 0.99 and p_new > 1e-15 add                    */
+/* new = p_new * (1 - visited) to visited (capped at 1) and              */
+/* fma(step, new, hitting) to the hitting time; stop when the largest    */
+/* 1 - visited is below tol. Visited rows (> 0.5) get hitting / visited  */
+/* scaled by 1 / (largest such value), the others 1.                     */
+/* ===================================================================== */
+#define ORACLE_DPT_BODY(T, FMA)                                                                       \
+  T* p = (T*)calloc((size_t)(n > 0 ? n : 1), sizeof(T));                                              \
+  T* q = (T*)calloc((size_t)(n > 0 ? n : 1), sizeof(T));                                              \
+  T* hit = (T*)calloc((size_t)(n > 0 ? n : 1), sizeof(T));                                            \
+  T* vis = (T*)calloc((size_t)(n > 0 ? n : 1), sizeof(T));                                            \
+  p[root] = (T)1;                                                                                     \
+  vis[root] = (T)1;                                                                                   \
+  for (int64_t it = 1; it <= max_iter; ++it) {                                                        \
+    T mu = (T)0;                                                                                      \
+    for (int64_t i = 0; i < n; ++i) {                                                                 \
+      T s = (T)0;                                                                                     \
+      for (int64_t k = indptr[i]; k < indptr[i + 1]; ++k) s = FMA(values[k], p[indices[k]], s);       \
+      q[i] = s;                                                                                       \
+      if (vis[i] < (T)0.99 && s > (T)1e-15) {                                                         \
+        const T np = s * ((T)1 - vis[i]);                                                             \
+        hit[i] = FMA((T)it, np, hit[i]);                                                              \
+        T v = vis[i] + np;                                                                            \
+        vis[i] = v < (T)1 ? v : (T)1;                                                                 \
+      }                                                                                               \
+      const T u = (T)1 - vis[i];                                                                      \
+      mu = u > mu ? u : mu;                                                                           \
+    }                                                                                                 \
+    if (mu < tol) break;                                                                              \
+    T* t = p;                                                                                         \
+    p = q;                                                                                            \
+    q = t;                                                                                            \
+  }                                                                                                   \
+  T mt = (T)0;                                                                                        \
+  for (int64_t i = 0; i < n; ++i)                                                                     \
+    if (vis[i] > (T)0.5) {                                                                            \
+      hit[i] = hit[i] / vis[i];                                                                       \
+      mt = hit[i] > mt ? hit[i] : mt;                                                                 \
+    }                                                                                                 \
+  const T inv = mt > (T)0 ? (T)1 / mt : (T)1;                                                         \
+  for (int64_t i = 0; i < n; ++i) out[i] = vis[i] > (T)0.5 ? hit[i] * inv : (T)1;                     \
+  free(p);                                                                                            \
+  free(q);                                                                                            \
+  free(hit);                                                                                          \
+  free(vis);
+
+void oracle_dpt_f32(int64_t n, const int64_t* indptr, const int64_t* indices, const float* values, int64_t root,
+                    int64_t max_iter, float tol, float* out) {
+  ORACLE_DPT_BODY(float, fmaf)
+}
+
+void oracle_dpt_f64(int64_t n, const int64_t* indptr, const int64_t* indices, const double* values, int64_t root,
+                    int64_t max_iter, double tol, double* out) {
+  ORACLE_DPT_BODY(double, fma)
+}

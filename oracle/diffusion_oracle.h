@@ -15,7 +15,8 @@
  *       scl/kernel/kernel.hpp:403-453 local_bandwidth, scl/kernel/impute.hpp:156-159
  *       distance_to_weight, scl/kernel/neighbors.hpp:319-478 kNN list format)
  *   - vector walks: lazy random walk, heat-kernel signature, random walk with
- *       restart (scl/kernel/diffusion.hpp:833-900, 961-1007, 1157-1194)
+ *       restart, diffusion pseudotime (scl/kernel/diffusion.hpp:670-831,
+ *       833-900, 961-1007, 1157-1194)
  *   - BF16/FP16 storage variants and the FP64 adjoint (new in this project).
  *
  * Arithmetic contract: every multiply-add that the reference performs through
@@ -120,6 +121,12 @@ int64_t oracle_walk_restart_f32(int64_t n, const int64_t* indptr, const int64_t*
                                 const float* r, float* scores, float alpha, int64_t max_iter, float tol);
 int64_t oracle_walk_restart_f64(int64_t n, const int64_t* indptr, const int64_t* indices, const double* values,
                                 const double* r, double* scores, double alpha, int64_t max_iter, double tol);
+
+/* ---- diffusion pseudotime (diffusion.hpp:670-772) --------------------- */
+void oracle_dpt_f32(int64_t n, const int64_t* indptr, const int64_t* indices, const float* values, int64_t root,
+                    int64_t max_iter, float tol, float* out);
+void oracle_dpt_f64(int64_t n, const int64_t* indptr, const int64_t* indices, const double* values, int64_t root,
+                    int64_t max_iter, double tol, double* out);
 
 #ifdef __cplusplus
 }

@@ -46,6 +46,8 @@ _SIGS = {
     "oracle_walk_linear_f64": ([_i64, _p, _p, _p, _p, _i64, ctypes.c_double, ctypes.c_double], None),
     "oracle_walk_restart_f32": ([_i64, _p, _p, _p, _p, _p, ctypes.c_float, _i64, ctypes.c_float], _i64),
     "oracle_walk_restart_f64": ([_i64, _p, _p, _p, _p, _p, ctypes.c_double, _i64, ctypes.c_double], _i64),
+    "oracle_dpt_f32": ([_i64, _p, _p, _p, _i64, _i64, ctypes.c_float, _p], None),
+    "oracle_dpt_f64": ([_i64, _p, _p, _p, _i64, _i64, ctypes.c_double, _p], None),
 }
 
 
@@ -306,3 +308,27 @@ def walk_restart(indptr, indices, values, seeds, n, alpha, max_iter, tol, dtype=
     fn = lib().oracle_walk_restart_f32 if dtype == np.float32 else lib().oracle_walk_restart_f64
     it = fn(n, _ptr(indptr), _ptr(indices), _ptr(v), _ptr(r), _ptr(scores), float(alpha), int(max_iter), float(tol))
     return scores, int(it)
+
+
+def dpt(indptr, indices, values, root, max_iter, tol, dtype=np.float32):
+    """Diffusion pseudotime from one root (diffusion.hpp:670-772)."""
+    indptr, indices = _csr(indptr, indices)
+    n = indptr.size - 1
+    v = np.ascontiguousarray(values, dtype)
+    out = np.empty(n, dtype)
+    fn = lib().oracle_dpt_f32 if dtype == np.float32 else lib().oracle_dpt_f64
+    fn(n, _ptr(indptr), _ptr(indices), _ptr(v), int(root), int(max_iter), float(tol), _ptr(out))
+    return out
+
+
+def dpt_multi_root(indptr, indices, values, roots, max_iter, dtype=np.float32):
+    """diffusion.hpp:774-830: the mean of the in-range roots' pseudotimes
+    (each with tol 1e-6), summed in root order then scaled by 1 / count."""
+    n = np.asarray(indptr).size - 1
+    valid = [int(r) for r in roots if 0 <= int(r) < n]
+    if not valid:
+        return np.ones(n, dtype)
+    s = np.zeros(n, dtype)
+    for r in valid:
+        s = (s + dpt(indptr, indices, values, r, max_iter, dtype(1e-6), dtype)).astype(dtype)
+    return (s * (dtype(1) / dtype(len(valid)))).astype(dtype)

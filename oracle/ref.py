@@ -80,6 +80,8 @@ class RefLib:
         L.scl_diffusion_personalized_pagerank.argtypes = [P, I, P, ctypes.c_size_t, R_, I, R_]
         L.scl_diffusion_lazy_random_walk.argtypes = [P, P, ctypes.c_size_t, I, R_]
         L.scl_diffusion_heat_kernel_signature.argtypes = [P, P, ctypes.c_size_t, R_, I]
+        L.scl_diffusion_compute_dpt.argtypes = [P, I, P, ctypes.c_size_t, I, R_]
+        L.scl_diffusion_compute_dpt_multi_root.argtypes = [P, P, ctypes.c_size_t, P, ctypes.c_size_t, I]
         L.scl_impute_magic.argtypes = [P, P, I, I, I, P]
         L.scl_get_last_error.restype = ctypes.c_char_p
         for fn in ("scl_sparse_wrap", "scl_sparse_create_with_strategy", "scl_sparse_destroy",
@@ -88,7 +90,8 @@ class RefLib:
                    "scl_diffusion_diffuse_vector", "scl_diffusion_magic_impute", "scl_algebra_spmm",
                    "scl_impute_diffusion", "scl_impute_magic", "scl_diffusion_random_walk_with_restart",
                    "scl_diffusion_personalized_pagerank", "scl_diffusion_lazy_random_walk",
-                   "scl_diffusion_heat_kernel_signature"):
+                   "scl_diffusion_heat_kernel_signature", "scl_diffusion_compute_dpt",
+                   "scl_diffusion_compute_dpt_multi_root"):
             getattr(L, fn).restype = ctypes.c_int32
         self.L = L
 
@@ -204,7 +207,14 @@ class RefLib:
                                                                   kw.get("laziness", 0.5)))
                 return out
             out = np.full(m, -7.0, self.real_dtype)
-            if kind == "hks":
+            if kind == "dpt":
+                self._check(self.L.scl_diffusion_compute_dpt(h, kw["root"], out.ctypes.data, m,
+                                                             kw.get("max_iter", 100), kw.get("tol", 1e-6)))
+            elif kind == "dpt_multi":
+                roots = np.ascontiguousarray(kw["roots"], self.index_dtype)
+                self._check(self.L.scl_diffusion_compute_dpt_multi_root(h, roots.ctypes.data, roots.size,
+                                                                        out.ctypes.data, m, kw.get("max_iter", 100)))
+            elif kind == "hks":
                 self._check(self.L.scl_diffusion_heat_kernel_signature(h, out.ctypes.data, m, kw.get("t", 1.0),
                                                                        kw.get("steps", 10)))
             elif kind == "ppr":

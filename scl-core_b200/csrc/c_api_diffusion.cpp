@@ -424,13 +424,64 @@ SCL_EXPORT scl_error_t scl_diffusion_magic_impute(scl_sparse_t transition, scl_r
     return SCL_ERROR_NOT_IMPLEMENTED;                                                        \
   } while (0)
 
-SCL_EXPORT scl_error_t scl_diffusion_compute_dpt(scl_sparse_t, scl_index_t, scl_real_t*, scl_size_t, scl_index_t,
-                                                 scl_real_t) {
-  SCL_NOT_IMPLEMENTED("scl_diffusion_compute_dpt");
+SCL_EXPORT scl_error_t scl_diffusion_compute_dpt(scl_sparse_t transition, scl_index_t root_cell,
+                                                 scl_real_t* pseudotime, scl_size_t n_nodes, scl_index_t max_iter,
+                                                 scl_real_t tol) {
+  SCL_API_CHECK_NULL(transition, "Transition matrix is null");
+  SCL_API_CHECK_NULL(pseudotime, "Output pseudotime array is null");
+  SCL_API_CHECK(n_nodes > 0, SCL_ERROR_INVALID_ARGUMENT, "Number of nodes must be positive");
+  SCL_API_TRY
+  Stats st;
+  WalkSetup w = walk_setup(*transition, n_nodes, "DPT: output buffer too small", st);
+  SCL_REQUIRE(root_cell >= 0 && root_cell < w.n, SCL_ERROR_INVALID_ARGUMENT, "DPT: root_cell out of range");
+  DevBuf out(w.n * sizeof(Real), w.s);
+  EventTimer tm(w.s);
+  tm.start();
+  dpt(w.mir->g.view(), root_cell, out.p, max_iter == 0 ? kDefaultMaxIter : max_iter,
+      (double)(tol == Real(0) ? kDefaultTol : tol), w.s);
+  tm.stop();
+  SCL_CUDA(cudaMemcpyAsync(pseudotime, out.p, w.n * sizeof(Real), cudaMemcpyDeviceToHost, w.s));
+  st.d2h += (double)w.n * sizeof(Real);
+  SCL_CUDA(cudaStreamSynchronize(w.s));
+  st.device_ms = tm.ms();
+  t_stats = st;
+  SCL_API_RETURN_OK;
+  SCL_API_CATCH
 }
-SCL_EXPORT scl_error_t scl_diffusion_compute_dpt_multi_root(scl_sparse_t, const scl_index_t*, scl_size_t, scl_real_t*,
-                                                            scl_size_t, scl_index_t) {
-  SCL_NOT_IMPLEMENTED("scl_diffusion_compute_dpt_multi_root");
+
+SCL_EXPORT scl_error_t scl_diffusion_compute_dpt_multi_root(scl_sparse_t transition, const scl_index_t* root_cells,
+                                                            scl_size_t n_roots, scl_real_t* pseudotime,
+                                                            scl_size_t n_nodes, scl_index_t max_iter) {
+  SCL_API_CHECK_NULL(transition, "Transition matrix is null");
+  SCL_API_CHECK_NULL(root_cells, "Root cells array is null");
+  SCL_API_CHECK_NULL(pseudotime, "Output pseudotime array is null");
+  SCL_API_CHECK(n_roots > 0 && n_nodes > 0, SCL_ERROR_INVALID_ARGUMENT, "Dimensions must be positive");
+  SCL_API_TRY
+  Stats st;
+  WalkSetup w = walk_setup(*transition, n_nodes, "DPT: output buffer too small", st);
+  if (w.n == 0) SCL_API_RETURN_OK;
+  std::vector<Index> valid;  // diffusion.hpp:794-800: out-of-range roots are skipped
+  for (size_t r = 0; r < n_roots; ++r)
+    if (root_cells[r] >= 0 && root_cells[r] < w.n) valid.push_back(root_cells[r]);
+  if (valid.empty()) {
+    for (Index i = 0; i < w.n; ++i) pseudotime[i] = Real(1);
+    SCL_API_RETURN_OK;
+  }
+  const Index it = (max_iter == 0) ? kDefaultMaxIter : max_iter;
+  DevBuf all((size_t)valid.size() * w.n * sizeof(Real), w.s), out(w.n * sizeof(Real), w.s);
+  EventTimer tm(w.s);
+  tm.start();
+  for (size_t r = 0; r < valid.size(); ++r)  // each root with the kernel's default tolerance (diffusion.hpp:805-808)
+    dpt(w.mir->g.view(), valid[r], all.as<Real>() + r * (size_t)w.n, it, (double)kDefaultTol, w.s);
+  dpt_average(all.p, (int64_t)valid.size(), w.n, sclabi::kRealDType, out.p, w.s);
+  tm.stop();
+  SCL_CUDA(cudaMemcpyAsync(pseudotime, out.p, w.n * sizeof(Real), cudaMemcpyDeviceToHost, w.s));
+  st.d2h += (double)w.n * sizeof(Real);
+  SCL_CUDA(cudaStreamSynchronize(w.s));
+  st.device_ms = tm.ms();
+  t_stats = st;
+  SCL_API_RETURN_OK;
+  SCL_API_CATCH
 }
 SCL_EXPORT scl_error_t scl_diffusion_random_walk_with_restart(scl_sparse_t transition, const scl_index_t* seed_nodes,
                                                               scl_size_t n_seeds, scl_real_t* scores,

@@ -281,6 +281,10 @@ void magic_diffuse(const CsrView& aff, void* X, int64_t F, int64_t steps, cudaSt
 void walk_linear(const CsrView& P, void* x, int64_t steps, double c_x, double c_p, cudaStream_t s);
 int64_t walk_restart(const CsrView& P, const void* r, void* scores, double alpha, int64_t max_iter, double tol,
                      cudaStream_t s);
+// Diffusion pseudotime from one root (out: n values) and the average of
+// n_roots such rows (all: n_roots x n, summed in root order, times 1/n_roots).
+void dpt(const CsrView& P, int64_t root, void* out, int64_t max_iter, double tol, cudaStream_t s);
+void dpt_average(const void* all, int64_t n_roots, int64_t n, DType t, void* out, cudaStream_t s);
 
 // dL/dP in CSR order from its CSC-order accumulator.
 void scatter_adjoint_entries(const Adjoint& adj, const void* gPt, DType t, void* gP, cudaStream_t s);

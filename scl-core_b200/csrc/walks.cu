@@ -10,6 +10,7 @@
 // and, for the restart walk, the L1 change sum |y_i - x_i| (differences in
 // the storage precision, summed in FP64) for the convergence test.
 #include <algorithm>
+#include <cstring>
 
 #include "engine.hpp"
 
@@ -50,6 +51,86 @@ k_walk_step(const int64_t* __restrict__ ptr, const int32_t* __restrict__ idx, co
       for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t += part[w];
       atomicAdd(l1, t);
     }
+  }
+}
+
+// Atomic max of a non-negative value through its bit pattern (for such
+// values the unsigned order of the bits is the numeric order).
+__device__ __forceinline__ void max_nonneg(float v, unsigned long long* word) {
+  atomicMax(reinterpret_cast<unsigned int*>(word), __float_as_uint(v));
+}
+__device__ __forceinline__ void max_nonneg(double v, unsigned long long* word) {
+  atomicMax(word, (unsigned long long)__double_as_longlong(v));
+}
+template <class T> T from_bits(unsigned long long w);
+template <> float from_bits<float>(unsigned long long w) {
+  const unsigned int u = (unsigned int)w;
+  float f;
+  std::memcpy(&f, &u, 4);
+  return f;
+}
+template <> double from_bits<double>(unsigned long long w) {
+  double d;
+  std::memcpy(&d, &w, 8);
+  return d;
+}
+
+// One diffusion-pseudotime step (diffusion.hpp:706-738): p_new = P p, then for
+// rows not yet (almost) visited the hitting time and visit probability grow by
+// the newly arriving mass; the largest unvisited probability 1 - visited is
+// max-reduced for the convergence test.
+template <class T>
+__global__ void __launch_bounds__(256)
+k_dpt_step(const int64_t* __restrict__ ptr, const int32_t* __restrict__ idx, const T* __restrict__ val, int64_t n,
+           const T* __restrict__ p, T* __restrict__ p_new, T* __restrict__ hit, T* __restrict__ vis, T step,
+           unsigned long long* __restrict__ max_unvisited) {
+  T m = T(0);
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    T s = T(0);
+    for (int64_t k = ptr[i], e = ptr[i + 1]; k < e; ++k) s = wfma(val[k], p[idx[k]], s);
+    p_new[i] = s;
+    T v = vis[i];
+    if (v < T(0.99) && s > T(1e-15)) {
+      const T np = wmul(s, T(1) - v);
+      hit[i] = wfma(step, np, hit[i]);
+      v = v + np;
+      v = v < T(1) ? v : T(1);
+      vis[i] = v;
+    }
+    const T u = T(1) - v;
+    m = u > m ? u : m;
+  }
+  max_nonneg(m, max_unvisited);
+}
+
+// hitting time / visit probability on the visited rows (> 0.5), max-reduced
+template <class T>
+__global__ void k_dpt_scale(int64_t n, T* __restrict__ hit, const T* __restrict__ vis,
+                            unsigned long long* __restrict__ max_time) {
+  T m = T(0);
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    if (vis[i] > T(0.5)) {
+      const T h = hit[i] / vis[i];
+      hit[i] = h;
+      m = h > m ? h : m;
+    }
+  }
+  max_nonneg(m, max_time);
+}
+
+template <class T>
+__global__ void k_dpt_output(int64_t n, const T* __restrict__ hit, const T* __restrict__ vis, T inv_max,
+                             T* __restrict__ out) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    out[i] = vis[i] > T(0.5) ? wmul(hit[i], inv_max) : T(1);
+}
+
+template <class T>
+__global__ void k_add_scaled_rows(int64_t n, int64_t n_rows, const T* __restrict__ all, T scale, T* __restrict__ out) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    T s = T(0);
+    for (int64_t r = 0; r < n_rows; ++r) s = s + all[r * n + i];
+    out[i] = wmul(s, scale);
   }
 }
 
@@ -110,7 +191,67 @@ int64_t walk_restart_typed(const CsrView& P, const T* r, T* scores, T alpha, int
   return it;
 }
 
+template <class T>
+void dpt_typed(const CsrView& P, int64_t root, T* out, int64_t max_iter, T tol, cudaStream_t s) {
+  const int64_t n = P.n_rows;
+  const size_t bytes = (size_t)n * sizeof(T);
+  DevBuf pa(bytes, s), pb(bytes, s), hit(bytes, s), vis(bytes, s), word(sizeof(unsigned long long), s);
+  SCL_CUDA(cudaMemsetAsync(pa.p, 0, bytes, s));
+  SCL_CUDA(cudaMemsetAsync(hit.p, 0, bytes, s));
+  SCL_CUDA(cudaMemsetAsync(vis.p, 0, bytes, s));
+  const T one = T(1);
+  SCL_CUDA(cudaMemcpyAsync(pa.as<T>() + root, &one, sizeof(T), cudaMemcpyHostToDevice, s));
+  SCL_CUDA(cudaMemcpyAsync(vis.as<T>() + root, &one, sizeof(T), cudaMemcpyHostToDevice, s));
+  unsigned long long* hw = nullptr;
+  SCL_CUDA(cudaMallocHost(&hw, sizeof(unsigned long long)));
+  struct Free {
+    unsigned long long* p;
+    ~Free() { cudaFreeHost(p); }
+  } guard{hw};
+  T* p = pa.as<T>();
+  T* q = pb.as<T>();
+  for (int64_t it = 1; it <= max_iter; ++it) {
+    SCL_CUDA(cudaMemsetAsync(word.p, 0, sizeof(unsigned long long), s));
+    k_dpt_step<T><<<walk_grid(n), 256, 0, s>>>(P.indptr, P.indices, static_cast<const T*>(P.values), n, p, q,
+                                                hit.as<T>(), vis.as<T>(), static_cast<T>(it),
+                                                word.as<unsigned long long>());
+    SCL_CUDA(cudaGetLastError());
+    SCL_CUDA(cudaMemcpyAsync(hw, word.p, sizeof(unsigned long long), cudaMemcpyDeviceToHost, s));
+    SCL_CUDA(cudaStreamSynchronize(s));
+    if (from_bits<T>(*hw) < tol) break;
+    std::swap(p, q);
+  }
+  SCL_CUDA(cudaMemsetAsync(word.p, 0, sizeof(unsigned long long), s));
+  k_dpt_scale<T><<<walk_grid(n), 256, 0, s>>>(n, hit.as<T>(), vis.as<T>(), word.as<unsigned long long>());
+  SCL_CUDA(cudaGetLastError());
+  SCL_CUDA(cudaMemcpyAsync(hw, word.p, sizeof(unsigned long long), cudaMemcpyDeviceToHost, s));
+  SCL_CUDA(cudaStreamSynchronize(s));
+  const T max_time = from_bits<T>(*hw);
+  const T inv_max = (max_time > T(0)) ? T(1) / max_time : T(1);
+  k_dpt_output<T><<<walk_grid(n), 256, 0, s>>>(n, hit.as<T>(), vis.as<T>(), inv_max, out);
+  SCL_CUDA(cudaGetLastError());
+}
+
 }  // namespace
+
+void dpt(const CsrView& P, int64_t root, void* out, int64_t max_iter, double tol, cudaStream_t s) {
+  SCL_REQUIRE(P.n_cols <= P.n_rows, kErrDimensionMismatch, "DPT: column indices must address rows");
+  SCL_REQUIRE(root >= 0 && root < P.n_rows, kErrInvalidArgument, "DPT: root_cell out of range");
+  if (P.vtype == kF32) return dpt_typed<float>(P, root, static_cast<float*>(out), max_iter, (float)tol, s);
+  SCL_REQUIRE(P.vtype == kF64, kErrTypeMismatch, "DPT values must be f32 or f64");
+  dpt_typed<double>(P, root, static_cast<double*>(out), max_iter, tol, s);
+}
+
+void dpt_average(const void* all, int64_t n_roots, int64_t n, DType t, void* out, cudaStream_t s) {
+  if (t == kF32) {
+    k_add_scaled_rows<float><<<walk_grid(n), 256, 0, s>>>(n, n_roots, static_cast<const float*>(all),
+                                                          1.0f / (float)n_roots, static_cast<float*>(out));
+  } else {
+    k_add_scaled_rows<double><<<walk_grid(n), 256, 0, s>>>(n, n_roots, static_cast<const double*>(all),
+                                                           1.0 / (double)n_roots, static_cast<double*>(out));
+  }
+  SCL_CUDA(cudaGetLastError());
+}
 
 void walk_linear(const CsrView& P, void* x, int64_t steps, double c_x, double c_p, cudaStream_t s) {
   SCL_REQUIRE(P.n_cols <= P.n_rows, kErrDimensionMismatch, "walk: column indices must address rows of x");

@@ -52,6 +52,28 @@ def magic_impute(mat: CsrMatrix, X: np.ndarray, t: int = 0) -> np.ndarray:
     return X
 
 
+def compute_dpt(mat: CsrMatrix, root: int, n_nodes: int = None, max_iter: int = 100, tol: float = 1e-6) -> np.ndarray:
+    """Diffusion pseudotime from `root` in [0, 1] (scl_diffusion_compute_dpt)."""
+    lib = mat.lib
+    n = mat.shape[0] if n_nodes is None else int(n_nodes)
+    out = np.zeros(n, dtype=mat.real_dtype)
+    check_error(lib.scl_diffusion_compute_dpt(mat.handle, int(root), out.ctypes.data_as(ctypes.POINTER(lib.real_type)),
+                                              n, int(max_iter), tol), "compute_dpt", lib)
+    return out
+
+
+def compute_dpt_multi_root(mat: CsrMatrix, roots, n_nodes: int = None, max_iter: int = 100) -> np.ndarray:
+    """Mean diffusion pseudotime over `roots` (scl_diffusion_compute_dpt_multi_root)."""
+    lib = mat.lib
+    n = mat.shape[0] if n_nodes is None else int(n_nodes)
+    roots = np.ascontiguousarray(roots, dtype=mat.index_dtype)
+    out = np.zeros(n, dtype=mat.real_dtype)
+    check_error(lib.scl_diffusion_compute_dpt_multi_root(
+        mat.handle, roots.ctypes.data_as(ctypes.POINTER(lib.index_type)), roots.size,
+        out.ctypes.data_as(ctypes.POINTER(lib.real_type)), n, int(max_iter)), "compute_dpt_multi_root", lib)
+    return out
+
+
 def random_walk_with_restart(mat: CsrMatrix, seeds, n_nodes: int = None, alpha: float = 0.85, max_iter: int = 100,
                              tol: float = 1e-6) -> np.ndarray:
     """Scores of the walk that restarts on `seeds` (scl_diffusion_random_walk_with_restart)."""

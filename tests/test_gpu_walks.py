@@ -89,3 +89,23 @@ def test_longer_output_buffers_keep_their_tail_and_errors_follow_the_reference()
     assert lib.scl_diffusion_lazy_random_walk(m.handle, P(out), n, 0, 0.5) == 10
     assert lib.scl_diffusion_lazy_random_walk(m.handle, P(out), n, 2, -0.1) == 10
     assert lib.scl_diffusion_lazy_random_walk(m.handle, P(out), n - 1, 2, 0.5) == 11
+
+
+@pytest.mark.parametrize("dt,idt", VARIANTS)
+@pytest.mark.parametrize("n", [3, 400, 20000])
+def test_pseudotime_bit_exact(dt, idt, n):
+    m, (ip, ind, v) = _graph(n, dt, idt, seed=8, density=10.0 / n)
+    for root, max_iter, tol in ((0, 100, 1e-6), (n - 1, 3, 1e-6), (n // 2, 100, 1e-2), (1 % n, 0, 0.0)):
+        got = scl.diffusion.compute_dpt(m, root, max_iter=max_iter, tol=tol)
+        mi = 100 if max_iter == 0 else max_iter
+        t = dt(1e-6) if tol == 0.0 else dt(tol)
+        np.testing.assert_array_equal(bits(got), bits(port.dpt(ip, ind, v, root, mi, t, dt)))
+    got = scl.diffusion.compute_dpt_multi_root(m, [0, n // 3, -2, n + 5, 0], max_iter=40)
+    np.testing.assert_array_equal(bits(got), bits(port.dpt_multi_root(ip, ind, v, [0, n // 3, -2, n + 5, 0], 40, dt)))
+    assert (scl.diffusion.compute_dpt_multi_root(m, [-1, n]) == 1).all()
+    lib = m.lib
+    out = np.zeros(n, dt)
+    P = out.ctypes.data_as(ctypes.POINTER(lib.real_type))
+    assert lib.scl_diffusion_compute_dpt(m.handle, n, P, n, 10, 1e-6) == 10  # root out of range
+    assert lib.scl_diffusion_compute_dpt(m.handle, 0, P, n - 1, 10, 1e-6) == (11 if n > 1 else 10)
+    assert lib.scl_diffusion_compute_dpt(None, 0, P, n, 10, 1e-6) == 4

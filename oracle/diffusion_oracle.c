@@ -494,11 +494,44 @@ double oracle_adjoint_f64(int64_t n, const int64_t* indptr, const int64_t* indic
   return loss;
 }
 
+/* (P x)_i in the walks' order: 32 partial fma chains over the entries  */
+/* l, l+32, ... of the row, combined by the xor butterfly 16, 8, 4, 2, 1 */
+/* (every lane of a warp ends with the same value; lane 0's is used).   */
+static float warp_dot_f32(const int64_t* indptr, const int64_t* indices, const float* values, const float* x,
+                          int64_t i) {
+  float part[32], nxt[32];
+  for (int l = 0; l < 32; ++l) {
+    float s = 0.0f;
+    for (int64_t p = indptr[i] + l; p < indptr[i + 1]; p += 32) s = fmaf(values[p], x[indices[p]], s);
+    part[l] = s;
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    for (int l = 0; l < 32; ++l) nxt[l] = part[l] + part[l ^ o];
+    memcpy(part, nxt, sizeof(part));
+  }
+  return part[0];
+}
+
+static double warp_dot_f64(const int64_t* indptr, const int64_t* indices, const double* values, const double* x,
+                           int64_t i) {
+  double part[32], nxt[32];
+  for (int l = 0; l < 32; ++l) {
+    double s = 0.0;
+    for (int64_t p = indptr[i] + l; p < indptr[i + 1]; p += 32) s = fma(values[p], x[indices[p]], s);
+    part[l] = s;
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    for (int l = 0; l < 32; ++l) nxt[l] = part[l] + part[l ^ o];
+    memcpy(part, nxt, sizeof(part));
+  }
+  return part[0];
+}
+
 /* ===================================================================== */
 /* Vector walks — diffusion.hpp:833-900 (random walk with restart),       */
 /* 961-1007 (heat-kernel signature), 1157-1194 (lazy random walk), on    */
-/* spmv_parallel (169-221). Each (P x)_i is the sequential fma chain over */
-/* the row's entries; the step's combination is rounded as               */
+/* spmv_parallel (169-221). Each (P x)_i is formed in the warp order of  */
+/* warp_dot_*; the step's combination is rounded as                      */
 /*   lazy / heat kernel: y = fma(c_x, x, c_p * (P x))                     */
 /*   restart:            y = fma(alpha, (P x), (1 - alpha) * r)           */
 /* The restart walk's convergence sum is sum |y - x| (differences in the */
@@ -511,8 +544,7 @@ void oracle_walk_linear_f32(int64_t n, const int64_t* indptr, const int64_t* ind
   float* y = (float*)malloc(sizeof(float) * (size_t)(n > 0 ? n : 1));
   for (int64_t st = 0; st < steps; ++st) {
     for (int64_t i = 0; i < n; ++i) {
-      float s = 0.0f;
-      for (int64_t p = indptr[i]; p < indptr[i + 1]; ++p) s = fmaf(values[p], x[indices[p]], s);
+      const float s = warp_dot_f32(indptr, indices, values, x, i);
       y[i] = fmaf(cx, x[i], cp * s);
     }
     memcpy(x, y, sizeof(float) * (size_t)n);
@@ -525,8 +557,7 @@ void oracle_walk_linear_f64(int64_t n, const int64_t* indptr, const int64_t* ind
   double* y = (double*)malloc(sizeof(double) * (size_t)(n > 0 ? n : 1));
   for (int64_t st = 0; st < steps; ++st) {
     for (int64_t i = 0; i < n; ++i) {
-      double s = 0.0;
-      for (int64_t p = indptr[i]; p < indptr[i + 1]; ++p) s = fma(values[p], x[indices[p]], s);
+      const double s = warp_dot_f64(indptr, indices, values, x, i);
       y[i] = fma(cx, x[i], cp * s);
     }
     memcpy(x, y, sizeof(double) * (size_t)n);
@@ -544,8 +575,7 @@ int64_t oracle_walk_restart_f32(int64_t n, const int64_t* indptr, const int64_t*
   for (; it < max_iter; ++it) {
     double l1 = 0.0;
     for (int64_t i = 0; i < n; ++i) {
-      float s = 0.0f;
-      for (int64_t p = indptr[i]; p < indptr[i + 1]; ++p) s = fmaf(values[p], cur[indices[p]], s);
+      const float s = warp_dot_f32(indptr, indices, values, cur, i);
       const float y = fmaf(alpha, s, beta * r[i]);
       const float d = y - cur[i];
       l1 += (double)(d >= 0.0f ? d : -d);
@@ -574,8 +604,7 @@ int64_t oracle_walk_restart_f64(int64_t n, const int64_t* indptr, const int64_t*
   for (; it < max_iter; ++it) {
     double l1 = 0.0;
     for (int64_t i = 0; i < n; ++i) {
-      double s = 0.0;
-      for (int64_t p = indptr[i]; p < indptr[i + 1]; ++p) s = fma(values[p], cur[indices[p]], s);
+      const double s = warp_dot_f64(indptr, indices, values, cur, i);
       const double y = fma(alpha, s, beta * r[i]);
       const double d = y - cur[i];
       l1 += (d >= 0.0 ? d : -d);

@@ -1,14 +1,18 @@
-// Vector walks on the transition graph (scl/kernel/diffusion.hpp:833-900,
-// 961-1007, 1136-1194): lazy random walk, heat-kernel signature, random walk
-// with restart and personalized PageRank.
+// Vector walks on the transition graph (scl/kernel/diffusion.hpp:670-831,
+// 833-900, 961-1007, 1136-1194): lazy random walk, heat-kernel signature,
+// random walk with restart, personalized PageRank and diffusion pseudotime.
 //
-// Every step is one fused kernel: a thread per row forms (P x)_i as the
-// sequential fma chain over the row's entries in stored order, then the
-// step's linear combination with one explicit rounding pattern:
+// Lazy walk, heat kernel and restart walk: one fused kernel per step with a
+// warp per row. Lane l runs the fma chain over the row's entries l, l+32, ...
+// and the 32 partial sums are combined by a fixed xor butterfly (offsets 16,
+// 8, 4, 2, 1), so (P x)_i is deterministic; then the step's linear combination
+// with one explicit rounding pattern:
 //   lazy / heat kernel:  y_i = fma(c_x, x_i, c_p * (P x)_i)
 //   restart:             y_i = fma(c_p, (P x)_i, c_r * r_i)
 // and, for the restart walk, the L1 change sum |y_i - x_i| (differences in
 // the storage precision, summed in FP64) for the convergence test.
+// Diffusion pseudotime keeps a thread per row and the sequential fma chain in
+// stored order.
 #include <algorithm>
 #include <cstring>
 
@@ -28,23 +32,29 @@ k_walk_step(const int64_t* __restrict__ ptr, const int32_t* __restrict__ idx, co
             const T* __restrict__ x, const T* __restrict__ r, T c1, T c2, T* __restrict__ y,
             double* __restrict__ l1) {
   __shared__ double part[8];
+  const int lane = threadIdx.x & 31;
+  const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
   double d = 0.0;
-  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+  for (int64_t i = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < n; i += nw) {
     T s = T(0);
-    for (int64_t k = ptr[i], e = ptr[i + 1]; k < e; ++k) s = wfma(val[k], x[idx[k]], s);
-    T out;
-    if constexpr (RESTART) out = wfma(c1, s, wmul(c2, r[i]));
-    else out = wfma(c1, x[i], wmul(c2, s));
-    y[i] = out;
-    if constexpr (RESTART) {
-      const T diff = out - x[i];
-      d += (double)(diff >= T(0) ? diff : -diff);
+    for (int64_t k = ptr[i] + lane, e = ptr[i + 1]; k < e; k += 32) s = wfma(__ldcs(val + k), x[__ldcs(idx + k)], s);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) s = s + __shfl_xor_sync(0xffffffffu, s, o);
+    if (lane == 0) {
+      T out;
+      if constexpr (RESTART) out = wfma(c1, s, wmul(c2, r[i]));
+      else out = wfma(c1, x[i], wmul(c2, s));
+      y[i] = out;
+      if constexpr (RESTART) {
+        const T diff = out - x[i];
+        d += (double)(diff >= T(0) ? diff : -diff);
+      }
     }
   }
   if constexpr (RESTART) {
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) d += __shfl_xor_sync(0xffffffffu, d, o);
-    if ((threadIdx.x & 31) == 0) part[threadIdx.x >> 5] = d;
+    if (lane == 0) part[threadIdx.x >> 5] = d;
     __syncthreads();
     if (threadIdx.x == 0) {
       double t = 0.0;
@@ -141,6 +151,13 @@ unsigned walk_grid(int64_t n) {
   return (unsigned)std::max<int64_t>(1, std::min<int64_t>(want, (int64_t)sm_count(dev) * 8));
 }
 
+unsigned warp_row_grid(int64_t n) {  // a warp per row, 8 warps per block
+  int dev = 0;
+  SCL_CUDA(cudaGetDevice(&dev));
+  const int64_t want = (n + 7) / 8;
+  return (unsigned)std::max<int64_t>(1, std::min<int64_t>(want, (int64_t)sm_count(dev) * 8));
+}
+
 template <class T>
 void walk_linear_typed(const CsrView& P, T* x, int64_t steps, T c_x, T c_p, cudaStream_t s) {
   const int64_t n = P.n_rows;
@@ -148,7 +165,7 @@ void walk_linear_typed(const CsrView& P, T* x, int64_t steps, T c_x, T c_p, cuda
   T* in = x;
   T* out = tmp.as<T>();
   for (int64_t st = 0; st < steps; ++st) {
-    k_walk_step<T, false><<<walk_grid(n), 256, 0, s>>>(P.indptr, P.indices, static_cast<const T*>(P.values), n, in,
+    k_walk_step<T, false><<<warp_row_grid(n), 256, 0, s>>>(P.indptr, P.indices, static_cast<const T*>(P.values), n, in,
                                                         nullptr, c_x, c_p, out, nullptr);
     SCL_CUDA(cudaGetLastError());
     std::swap(in, out);
@@ -177,7 +194,7 @@ int64_t walk_restart_typed(const CsrView& P, const T* r, T* scores, T alpha, int
   int64_t it = 0;
   for (; it < max_iter; ++it) {
     SCL_CUDA(cudaMemsetAsync(l1.p, 0, sizeof(double), s));
-    k_walk_step<T, true><<<walk_grid(n), 256, 0, s>>>(P.indptr, P.indices, static_cast<const T*>(P.values), n, cur,
+    k_walk_step<T, true><<<warp_row_grid(n), 256, 0, s>>>(P.indptr, P.indices, static_cast<const T*>(P.values), n, cur,
                                                        r, alpha, beta, nxt, l1.as<double>());
     SCL_CUDA(cudaGetLastError());
     SCL_CUDA(cudaMemcpyAsync(host_l1, l1.p, sizeof(double), cudaMemcpyDeviceToHost, s));

@@ -681,3 +681,35 @@ void oracle_dpt_f64(int64_t n, const int64_t* indptr, const int64_t* indices, co
                     int64_t max_iter, double tol, double* out) {
   ORACLE_DPT_BODY(double, fma)
 }
+
+/* ===================================================================== */
+/* General SpMM — scl/kernel/algebra.hpp:546-600 (scl_algebra_spmm):      */
+/* Y <- beta Y (beta 0: zero, beta 1: untouched), then unless alpha is 0, */
+/* for every stored entry in order w = a * alpha and, when w != 0,        */
+/* y_row = fma(w, x_row, y_row).                                          */
+/* ===================================================================== */
+void oracle_algebra_spmm_f32(int64_t m, const int64_t* indptr, const int64_t* indices, const float* values,
+                             const float* X, int64_t K, float* Y, float alpha, float beta) {
+  for (int64_t i = 0; i < m * K; ++i) Y[i] = (beta == 0.0f) ? 0.0f : (beta == 1.0f ? Y[i] : Y[i] * beta);
+  if (alpha == 0.0f) return;
+  for (int64_t i = 0; i < m; ++i)
+    for (int64_t p = indptr[i]; p < indptr[i + 1]; ++p) {
+      const float w = values[p] * alpha;
+      if (w == 0.0f) continue;
+      const float* x = X + indices[p] * K;
+      for (int64_t c = 0; c < K; ++c) Y[i * K + c] = fmaf(w, x[c], Y[i * K + c]);
+    }
+}
+
+void oracle_algebra_spmm_f64(int64_t m, const int64_t* indptr, const int64_t* indices, const double* values,
+                             const double* X, int64_t K, double* Y, double alpha, double beta) {
+  for (int64_t i = 0; i < m * K; ++i) Y[i] = (beta == 0.0) ? 0.0 : (beta == 1.0 ? Y[i] : Y[i] * beta);
+  if (alpha == 0.0) return;
+  for (int64_t i = 0; i < m; ++i)
+    for (int64_t p = indptr[i]; p < indptr[i + 1]; ++p) {
+      const double w = values[p] * alpha;
+      if (w == 0.0) continue;
+      const double* x = X + indices[p] * K;
+      for (int64_t c = 0; c < K; ++c) Y[i * K + c] = fma(w, x[c], Y[i * K + c]);
+    }
+}

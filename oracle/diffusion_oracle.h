@@ -128,6 +128,12 @@ void oracle_dpt_f32(int64_t n, const int64_t* indptr, const int64_t* indices, co
 void oracle_dpt_f64(int64_t n, const int64_t* indptr, const int64_t* indices, const double* values, int64_t root,
                     int64_t max_iter, double tol, double* out);
 
+/* ---- general SpMM, Y = alpha A X + beta Y (algebra.hpp:546-600) ------- */
+void oracle_algebra_spmm_f32(int64_t m, const int64_t* indptr, const int64_t* indices, const float* values,
+                             const float* X, int64_t K, float* Y, float alpha, float beta);
+void oracle_algebra_spmm_f64(int64_t m, const int64_t* indptr, const int64_t* indices, const double* values,
+                             const double* X, int64_t K, double* Y, double alpha, double beta);
+
 #ifdef __cplusplus
 }
 #endif

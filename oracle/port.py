@@ -48,6 +48,8 @@ _SIGS = {
     "oracle_walk_restart_f64": ([_i64, _p, _p, _p, _p, _p, ctypes.c_double, _i64, ctypes.c_double], _i64),
     "oracle_dpt_f32": ([_i64, _p, _p, _p, _i64, _i64, ctypes.c_float, _p], None),
     "oracle_dpt_f64": ([_i64, _p, _p, _p, _i64, _i64, ctypes.c_double, _p], None),
+    "oracle_algebra_spmm_f32": ([_i64, _p, _p, _p, _p, _i64, _p, ctypes.c_float, ctypes.c_float], None),
+    "oracle_algebra_spmm_f64": ([_i64, _p, _p, _p, _p, _i64, _p, ctypes.c_double, ctypes.c_double], None),
 }
 
 
@@ -332,3 +334,15 @@ def dpt_multi_root(indptr, indices, values, roots, max_iter, dtype=np.float32):
     for r in valid:
         s = (s + dpt(indptr, indices, values, r, max_iter, dtype(1e-6), dtype)).astype(dtype)
     return (s * (dtype(1) / dtype(len(valid)))).astype(dtype)
+
+
+def algebra_spmm(indptr, indices, values, X, Y, alpha, beta):
+    """Y' = alpha A X + beta Y as scl_algebra_spmm forms it (algebra.hpp:546-600)."""
+    indptr, indices = _csr(indptr, indices)
+    m = indptr.size - 1
+    X = np.ascontiguousarray(X)
+    Yo = np.array(Y, dtype=X.dtype, copy=True, order="C")
+    v = np.ascontiguousarray(values, X.dtype)
+    fn = lib().oracle_algebra_spmm_f32 if X.dtype == np.float32 else lib().oracle_algebra_spmm_f64
+    fn(m, _ptr(indptr), _ptr(indices), _ptr(v), _ptr(X), X.shape[1], _ptr(Yo), float(alpha), float(beta))
+    return Yo

@@ -8,6 +8,7 @@
 #include "abi.hpp"
 #include "scl_diffusion.h"
 #include "scl_impute.h"
+#include "scl_algebra.h"
 
 using sclabi::Index;
 using sclabi::Real;
@@ -608,6 +609,39 @@ SCL_EXPORT scl_error_t scl_impute_magic(scl_sparse_t matrix, scl_sparse_t affini
   SCL_API_CHECK(n_cells > 0 && n_genes > 0 && t > 0, SCL_ERROR_INVALID_ARGUMENT, "Dimensions must be positive");
   SCL_API_TRY
   impute_host(*matrix, *affinity_matrix, n_cells, n_genes, t, X_imputed, true);
+  SCL_API_RETURN_OK;
+  SCL_API_CATCH
+}
+
+SCL_EXPORT scl_error_t scl_algebra_spmm(scl_sparse_t A, const scl_real_t* X, scl_index_t n_cols, scl_real_t* Y,
+                                        scl_real_t alpha, scl_real_t beta) {
+  SCL_API_CHECK_NULL(A, "Matrix A is null");
+  SCL_API_CHECK_NULL(X, "Input matrix X is null");
+  SCL_API_CHECK_NULL(Y, "Output matrix Y is null");
+  SCL_API_CHECK(n_cols > 0, SCL_ERROR_INVALID_ARGUMENT, "Number of columns must be positive");
+  SCL_API_TRY
+  SCL_REQUIRE(A->valid, SCL_ERROR_INVALID_ARGUMENT, "Matrix A is not valid");
+  const int dev = current_device();
+  cudaStream_t s = library_stream(dev);
+  Stats st;
+  auto mir = device_graph(*A, s, st.h2d);
+  const int64_t m = A->primary_dim(), kx = A->secondary_dim(), K = n_cols;
+  DevBuf Xd(std::max<int64_t>(kx * K, 1) * sizeof(Real), s), Yd(std::max<int64_t>(m * K, 1) * sizeof(Real), s);
+  if (kx > 0) SCL_CUDA(cudaMemcpyAsync(Xd.p, X, kx * K * sizeof(Real), cudaMemcpyHostToDevice, s));
+  st.h2d += (double)kx * K * sizeof(Real);
+  if (beta != Real(0) && m > 0) {
+    SCL_CUDA(cudaMemcpyAsync(Yd.p, Y, m * K * sizeof(Real), cudaMemcpyHostToDevice, s));
+    st.h2d += (double)m * K * sizeof(Real);
+  }
+  EventTimer tm(s);
+  tm.start();
+  algebra_spmm(mir->g.view(), Xd.p, K, Yd.p, (double)alpha, (double)beta, s);
+  tm.stop();
+  if (m > 0) SCL_CUDA(cudaMemcpyAsync(Y, Yd.p, m * K * sizeof(Real), cudaMemcpyDeviceToHost, s));
+  st.d2h += (double)m * K * sizeof(Real);
+  SCL_CUDA(cudaStreamSynchronize(s));
+  st.device_ms = tm.ms();
+  t_stats = st;
   SCL_API_RETURN_OK;
   SCL_API_CATCH
 }

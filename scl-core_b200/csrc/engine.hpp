@@ -273,6 +273,8 @@ double gather_floor_ms(const int32_t* idx, int64_t M, int64_t n_rows, int64_t ro
 // X <- W X with W the row-normalised affinity (rows with sum < 1e-12 copy X).
 void densify_expression(const CsrView& m, bool csr, int64_t n_cells, int64_t n_genes, void* dense, cudaStream_t s);
 void magic_diffuse(const CsrView& aff, void* X, int64_t F, int64_t steps, cudaStream_t s);
+// Y (A.n_rows x K) <- alpha A X + beta Y, X: A.n_cols x K (scl_algebra_spmm's arithmetic).
+void algebra_spmm(const CsrView& A, const void* X, int64_t K, void* Y, double alpha, double beta, cudaStream_t s);
 
 // Vector walks (walks.cu). walk_linear: x <- c_x x + c_p P x, `steps` times
 // (lazy random walk, heat-kernel signature). walk_restart: the restart walk

@@ -155,3 +155,52 @@ void magic_diffuse(const CsrView& aff, void* X, int64_t F, int64_t steps, cudaSt
 }
 
 }  // namespace sclgpu
+
+// ---- general SpMM, Y = alpha A X + beta Y (scl/kernel/algebra.hpp:546-600) -------
+namespace sclgpu {
+namespace {
+
+// A warp per row of A, lane l owning columns l, l+32, ...: y starts as beta y
+// (beta 0: zero, beta 1: y) and every stored entry with w = a * alpha != 0
+// adds fma(w, x_row, y) in stored order, as scl_algebra_spmm's axpy does.
+template <class T>
+__global__ void __launch_bounds__(256)
+k_algebra_spmm(const int64_t* __restrict__ ptr, const int32_t* __restrict__ idx, const T* __restrict__ val, int64_t m,
+               const T* __restrict__ X, int64_t K, T* __restrict__ Y, T alpha, T beta) {
+  const int lane = threadIdx.x & 31;
+  const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
+  for (int64_t i = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < m; i += nw) {
+    const int64_t s0 = ptr[i], s1 = ptr[i + 1];
+    for (int64_t c = lane; c < K; c += 32) {
+      T y = (beta == T(0)) ? T(0) : (beta == T(1) ? Y[i * K + c] : Y[i * K + c] * beta);
+      if (alpha != T(0)) {
+        for (int64_t k = s0; k < s1; ++k) {
+          const T w = val[k] * alpha;
+          if (w != T(0)) y = fma(w, X[(int64_t)idx[k] * K + c], y);
+        }
+      }
+      Y[i * K + c] = y;
+    }
+  }
+}
+
+}  // namespace
+
+void algebra_spmm(const CsrView& A, const void* X, int64_t K, void* Y, double alpha, double beta, cudaStream_t s) {
+  const int64_t m = A.n_rows;
+  if (m == 0 || K == 0) return;
+  int dev = 0;
+  SCL_CUDA(cudaGetDevice(&dev));
+  const unsigned grid = (unsigned)std::max<int64_t>(1, std::min<int64_t>((m + 7) / 8, (int64_t)sm_count(dev) * 8));
+  if (A.vtype == kF32)
+    k_algebra_spmm<float><<<grid, 256, 0, s>>>(A.indptr, A.indices, static_cast<const float*>(A.values), m,
+                                               static_cast<const float*>(X), K, static_cast<float*>(Y), (float)alpha,
+                                               (float)beta);
+  else
+    k_algebra_spmm<double><<<grid, 256, 0, s>>>(A.indptr, A.indices, static_cast<const double*>(A.values), m,
+                                                static_cast<const double*>(X), K, static_cast<double*>(Y), alpha,
+                                                beta);
+  SCL_CUDA(cudaGetLastError());
+}
+
+}  // namespace sclgpu

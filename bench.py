@@ -330,6 +330,58 @@ def bench_impute(torch, scl, device, reps, warmup, with_reference=True):
     return res
 
 
+def bench_knn(torch, scl, reps, warmup, with_reference=True):
+    """Brute-force kNN through the drop-in C ABI (scl_knn, host buffers): the
+    seeded 10-component 50-D mixture at 50,000 cells, k = 30 (the graph
+    build's first step), with norms from scl_neighbors_compute_norms. Beside
+    it, scl-core's own scl_knn (oracle/_ref, all host threads) on the first
+    10,000 cells, and the GPU on the same 10,000 cells with the reference's
+    norms, whose output must equal the reference's bit for bit."""
+    def wrap_dense(P):
+        n, d = P.shape
+        ip = np.arange(0, (n + 1) * d, d, dtype=np.int32)
+        ind = np.tile(np.arange(d, dtype=np.int32), n)
+        return scl.CsrMatrix.wrap(ip, ind, np.ascontiguousarray(P.reshape(-1)), (n, d)), (ip, ind)
+
+    n, k = 50_000, 30
+    pts = scl.synthetic.mixture(n, seed=21).astype(np.float32)
+    m, _ = wrap_dense(pts)
+    norms = scl.neighbors.compute_norms(m)
+    ts = []
+    for it in range(warmup + reps):
+        t0 = time.perf_counter()
+        gi, gd = scl.neighbors.knn(m, k, norms)
+        if it >= warmup:
+            ts.append(time.perf_counter() - t0)
+    st = scl.diffusion.last_stats(m.lib)
+    res = {"workload": "brute-force kNN, 50k cells x 50 features (mixture), k=30, host buffers through scl_knn",
+           "cells": n, "features": int(pts.shape[1]), "k": k, "e2e_ms": round(1e3 * float(np.median(ts)), 3),
+           "device_ms": round(float(st["device_ms"]), 3),
+           "distance_evaluations_per_s": round(n * (n - 1) / (st["device_ms"] * 1e-3), 1)}
+    if with_reference:
+        try:
+            from oracle import ref
+
+            R = ref.RefLib("f32_i32")
+            ns = 10_000
+            sub = np.ascontiguousarray(pts[:ns])
+            ms, (ip, ind) = wrap_dense(sub)
+            t0 = time.perf_counter()
+            ri, rd, rn = R.knn(ip, ind, sub.reshape(-1), sub.shape, k)
+            rdt = time.perf_counter() - t0
+            t0 = time.perf_counter()
+            si, sd = scl.neighbors.knn(ms, k, rn)
+            gdt = time.perf_counter() - t0
+            res.update({"sample_cells": ns, "reference_cpu_ms": round(1e3 * rdt, 1),
+                        "reference_cores": os.cpu_count(), "gpu_e2e_ms_on_sample": round(1e3 * gdt, 3),
+                        "e2e_speedup_vs_reference": round(rdt / gdt, 2),
+                        "bit_identical_to_reference": bool(np.array_equal(si, ri) and
+                                                           np.array_equal(sd.view(np.uint32), rd.view(np.uint32)))})
+        except Exception as e:  # informational; never fail the run on it
+            res["reference_cpu_ms"] = f"unavailable: {e}"
+    return res
+
+
 def bench_batched(torch, scl, device, stream, reps, warmup, rank=0, world=1, dist=None):
     """Batched form: 64 graphs, cell counts log-uniform in [2,000, 100,000]
     (seed 0), each its own 10-component mixture, k=15, row-normalised FP32,
@@ -407,6 +459,7 @@ def main():
     ap.add_argument("--no-batched", action="store_true", help="skip the batched configuration")
     ap.add_argument("--no-impute", action="store_true", help="skip the MAGIC imputation configuration")
     ap.add_argument("--no-walks", action="store_true", help="skip the personalized PageRank configuration")
+    ap.add_argument("--no-knn", action="store_true", help="skip the kNN configuration")
     args = ap.parse_args()
     warmup = max(3, args.warmup)
 
@@ -566,6 +619,9 @@ def main():
     impute = None
     if rank == 0 and not args.no_impute:
         impute = bench_impute(torch, scl, device, min(args.steps, 3), 1, with_reference=not args.no_cpu_baseline)
+    knn = None
+    if rank == 0 and not args.no_knn:
+        knn = bench_knn(torch, scl, min(args.steps, 3), 1, with_reference=not args.no_cpu_baseline)
 
     # ---- end to end through the drop-in C ABI with pinned host buffers --------------------
     e2e = None
@@ -668,6 +724,7 @@ def main():
             "batched": batched,
             "impute": impute,
             "walks": walks,
+            "knn": knn,
             "graph_build_ms": round(build_ms, 3),
             "reorder_ms": round(reorder_ms, 3),
             "reorder_cc_rounds": cc_rounds,

@@ -8,6 +8,7 @@
  */
 #include "diffusion_oracle.h"
 
+#include <float.h>
 #include <math.h>
 #include <stdlib.h>
 #include <string.h>
@@ -712,4 +713,119 @@ void oracle_algebra_spmm_f64(int64_t m, const int64_t* indptr, const int64_t* in
       const double* x = X + indices[p] * K;
       for (int64_t c = 0; c < K; ++c) Y[i * K + c] = fma(w, x[c], Y[i * K + c]);
     }
+}
+
+/* ===================================================================== */
+/* Brute-force kNN — scl/kernel/neighbors.hpp:319-478 (knn) on a dense   */
+/* n x d block (a sparse row's missing entries are zeros, whose products */
+/* leave an fma chain unchanged). For every query i, candidates j != i   */
+/* in increasing j: skipped when (sqrt(norm_i) - sqrt(norm_j))^2 is not  */
+/* below the current k-th distance; dot = fma chain over the features in */
+/* order; dist_sq = fma(-2, dot, norm_i + norm_j) clamped at 0 (the same */
+/* value as (norm_i + norm_j) - 2 * dot, 2 * dot being exact); a max-heap */
+/* of k (dist_sq, j) takes the candidate while short (sift up, stopping  */
+/* at a parent that is not smaller), else when strictly below the top    */
+/* (replace the top, sift down to the larger child). The heap is then    */
+/* sorted as the reference does (min-heap build, extract to the back,    */
+/* reverse) and written as sqrt(dist_sq); missing slots (inf, -1).       */
+/* ===================================================================== */
+#define ORACLE_KNN_SWAP(a, b)   \
+  do {                          \
+    T td_ = hd[a];              \
+    int64_t tj_ = hj[a];        \
+    hd[a] = hd[b];              \
+    hj[a] = hj[b];              \
+    hd[b] = td_;                \
+    hj[b] = tj_;                \
+  } while (0)
+
+#define ORACLE_KNN_BODY(T, FMA, SQRT, INF, MAXV)                                                      \
+  T* hd = (T*)malloc(sizeof(T) * (size_t)(k > 0 ? k : 1));                                            \
+  int64_t* hj = (int64_t*)malloc(sizeof(int64_t) * (size_t)(k > 0 ? k : 1));                          \
+  for (int64_t i = 0; i < n; ++i) {                                                                   \
+    int64_t cnt = 0;                                                                                  \
+    T maxd = MAXV;                                                                                    \
+    const T si = SQRT(norms[i]);                                                                      \
+    for (int64_t j = 0; j < n; ++j) {                                                                 \
+      if (j == i) continue;                                                                           \
+      const T nd = si - SQRT(norms[j]);                                                               \
+      if (nd * nd >= maxd) continue;                                                                  \
+      T dot = (T)0;                                                                                   \
+      for (int64_t f = 0; f < d; ++f) dot = FMA(X[i * d + f], X[j * d + f], dot);                     \
+      T ds = contract ? FMA((T)-2, dot, norms[i] + norms[j]) : (norms[i] + norms[j]) - (T)2 * dot;    \
+      if (ds < (T)0) ds = (T)0;                                                                       \
+      if (cnt < k) {                                                                                  \
+        int64_t pos = cnt;                                                                            \
+        hd[pos] = ds;                                                                                 \
+        hj[pos] = j;                                                                                  \
+        while (pos > 0) {                                                                             \
+          const int64_t par = (pos - 1) / 2;                                                          \
+          if (hd[pos] <= hd[par]) break;                                                              \
+          ORACLE_KNN_SWAP(pos, par);                                                                  \
+          pos = par;                                                                                  \
+        }                                                                                             \
+        ++cnt;                                                                                        \
+        if (cnt == k) maxd = hd[0];                                                                   \
+      } else if (ds < hd[0]) {                                                                        \
+        hd[0] = ds;                                                                                   \
+        hj[0] = j;                                                                                    \
+        int64_t pos = 0;                                                                              \
+        for (;;) {                                                                                    \
+          int64_t lg = pos;                                                                           \
+          const int64_t l = 2 * pos + 1, r = 2 * pos + 2;                                             \
+          if (l < cnt && hd[l] > hd[lg]) lg = l;                                                      \
+          if (r < cnt && hd[r] > hd[lg]) lg = r;                                                      \
+          if (lg == pos) break;                                                                       \
+          ORACLE_KNN_SWAP(pos, lg);                                                                   \
+          pos = lg;                                                                                   \
+        }                                                                                             \
+        maxd = hd[0];                                                                                 \
+      }                                                                                               \
+    }                                                                                                 \
+    for (int64_t m = cnt / 2; cnt >= 2 && m > 0; --m) oracle_knn_sort_sift_##T(hd, hj, m - 1, cnt);   \
+    for (int64_t m = cnt; m > 1; --m) {                                                               \
+      ORACLE_KNN_SWAP(0, m - 1);                                                                      \
+      oracle_knn_sort_sift_##T(hd, hj, 0, m - 1);                                                     \
+    }                                                                                                 \
+    for (int64_t m = 0; m < cnt / 2; ++m) ORACLE_KNN_SWAP(m, cnt - 1 - m);                            \
+    for (int64_t m = 0; m < k; ++m) {                                                                 \
+      out_dist[i * k + m] = m < cnt ? SQRT(hd[m]) : INF;                                              \
+      out_idx[i * k + m] = m < cnt ? hj[m] : -1;                                                      \
+    }                                                                                                 \
+  }                                                                                                   \
+  free(hd);                                                                                           \
+  free(hj);
+
+/* min-heap sift used by the final heap sort */
+#define ORACLE_KNN_SORT_SIFT(T)                                                                       \
+  static void oracle_knn_sort_sift_##T(T* hd, int64_t* hj, int64_t pos, int64_t size) {              \
+    for (;;) {                                                                                        \
+      int64_t sm = pos;                                                                               \
+      const int64_t l = 2 * pos + 1, r = 2 * pos + 2;                                                 \
+      if (l < size && hd[l] < hd[sm]) sm = l;                                                         \
+      if (r < size && hd[r] < hd[sm]) sm = r;                                                         \
+      if (sm == pos) break;                                                                           \
+      ORACLE_KNN_SWAP(pos, sm);                                                                       \
+      pos = sm;                                                                                       \
+    }                                                                                                 \
+  }
+#define T float
+ORACLE_KNN_SORT_SIFT(float)
+#undef T
+#define T double
+ORACLE_KNN_SORT_SIFT(double)
+#undef T
+
+void oracle_knn_dense_f32(int64_t n, int64_t d, const float* X, const float* norms, int64_t k, int contract,
+                          int64_t* out_idx, float* out_dist) {
+#define T float
+  ORACLE_KNN_BODY(float, fmaf, sqrtf, INFINITY, FLT_MAX)
+#undef T
+}
+
+void oracle_knn_dense_f64(int64_t n, int64_t d, const double* X, const double* norms, int64_t k, int contract,
+                          int64_t* out_idx, double* out_dist) {
+#define T double
+  ORACLE_KNN_BODY(double, fma, sqrt, (double)INFINITY, DBL_MAX)
+#undef T
 }

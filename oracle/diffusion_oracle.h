@@ -134,6 +134,12 @@ void oracle_algebra_spmm_f32(int64_t m, const int64_t* indptr, const int64_t* in
 void oracle_algebra_spmm_f64(int64_t m, const int64_t* indptr, const int64_t* indices, const double* values,
                              const double* X, int64_t K, double* Y, double alpha, double beta);
 
+/* ---- brute-force kNN on a dense block (neighbors.hpp:319-478) --------- */
+void oracle_knn_dense_f32(int64_t n, int64_t d, const float* X, const float* norms, int64_t k, int contract,
+                          int64_t* out_idx, float* out_dist);
+void oracle_knn_dense_f64(int64_t n, int64_t d, const double* X, const double* norms, int64_t k, int contract,
+                          int64_t* out_idx, double* out_dist);
+
 #ifdef __cplusplus
 }
 #endif

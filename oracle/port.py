@@ -50,6 +50,8 @@ _SIGS = {
     "oracle_dpt_f64": ([_i64, _p, _p, _p, _i64, _i64, ctypes.c_double, _p], None),
     "oracle_algebra_spmm_f32": ([_i64, _p, _p, _p, _p, _i64, _p, ctypes.c_float, ctypes.c_float], None),
     "oracle_algebra_spmm_f64": ([_i64, _p, _p, _p, _p, _i64, _p, ctypes.c_double, ctypes.c_double], None),
+    "oracle_knn_dense_f32": ([_i64, _i64, _p, _p, _i64, _int, _p, _p], None),
+    "oracle_knn_dense_f64": ([_i64, _i64, _p, _p, _i64, _int, _p, _p], None),
 }
 
 
@@ -346,3 +348,16 @@ def algebra_spmm(indptr, indices, values, X, Y, alpha, beta):
     fn = lib().oracle_algebra_spmm_f32 if X.dtype == np.float32 else lib().oracle_algebra_spmm_f64
     fn(m, _ptr(indptr), _ptr(indices), _ptr(v), _ptr(X), X.shape[1], _ptr(Yo), float(alpha), float(beta))
     return Yo
+
+
+def knn_dense(X, norms, k, contract=True):
+    """Brute-force kNN of the rows of dense X with the given squared norms
+    (neighbors.hpp:319-478): (indices int64 [n, k], distances [n, k])."""
+    X = np.ascontiguousarray(X)
+    n, d = X.shape
+    nr = np.ascontiguousarray(norms, X.dtype)
+    idx = np.empty((n, k), np.int64)
+    dist = np.empty((n, k), X.dtype)
+    fn = lib().oracle_knn_dense_f32 if X.dtype == np.float32 else lib().oracle_knn_dense_f64
+    fn(n, d, _ptr(X), _ptr(nr), int(k), int(bool(contract)), _ptr(idx), _ptr(dist))
+    return idx, dist

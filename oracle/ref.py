@@ -81,6 +81,8 @@ class RefLib:
         L.scl_diffusion_lazy_random_walk.argtypes = [P, P, ctypes.c_size_t, I, R_]
         L.scl_diffusion_heat_kernel_signature.argtypes = [P, P, ctypes.c_size_t, R_, I]
         L.scl_diffusion_compute_dpt.argtypes = [P, I, P, ctypes.c_size_t, I, R_]
+        L.scl_knn.argtypes = [P, P, ctypes.c_size_t, ctypes.c_size_t, P, P]
+        L.scl_neighbors_compute_norms.argtypes = [P, P]
         L.scl_diffusion_compute_dpt_multi_root.argtypes = [P, P, ctypes.c_size_t, P, ctypes.c_size_t, I]
         L.scl_impute_magic.argtypes = [P, P, I, I, I, P]
         L.scl_get_last_error.restype = ctypes.c_char_p
@@ -91,7 +93,7 @@ class RefLib:
                    "scl_impute_diffusion", "scl_impute_magic", "scl_diffusion_random_walk_with_restart",
                    "scl_diffusion_personalized_pagerank", "scl_diffusion_lazy_random_walk",
                    "scl_diffusion_heat_kernel_signature", "scl_diffusion_compute_dpt",
-                   "scl_diffusion_compute_dpt_multi_root"):
+                   "scl_diffusion_compute_dpt_multi_root", "scl_knn", "scl_neighbors_compute_norms"):
             getattr(L, fn).restype = ctypes.c_int32
         self.L = L
 
@@ -227,6 +229,23 @@ class RefLib:
                     h, seeds.ctypes.data, seeds.size, out.ctypes.data, m, kw.get("alpha", 0.85),
                     kw.get("max_iter", 100), kw.get("tol", 1e-6)))
             return out
+        finally:
+            self.destroy(h)
+
+    def knn(self, indptr, indices, data, shape, k, norms=None):
+        """scl_knn on a wrapped samples x features CSR (norms from
+        scl_neighbors_compute_norms unless given): (indices, distances, norms)."""
+        h, keep = self.wrap(indptr, indices, data, shape)
+        n = shape[0]
+        try:
+            if norms is None:
+                norms = np.zeros(n, self.real_dtype)
+                self._check(self.L.scl_neighbors_compute_norms(h, norms.ctypes.data))
+            norms = np.ascontiguousarray(norms, self.real_dtype)
+            idx = np.zeros(n * k, self.index_dtype)
+            dist = np.zeros(n * k, self.real_dtype)
+            self._check(self.L.scl_knn(h, norms.ctypes.data, n, k, idx.ctypes.data, dist.ctypes.data))
+            return idx.reshape(n, k), dist.reshape(n, k), norms
         finally:
             self.destroy(h)
 

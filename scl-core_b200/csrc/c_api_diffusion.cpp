@@ -9,6 +9,7 @@
 #include "scl_diffusion.h"
 #include "scl_impute.h"
 #include "scl_algebra.h"
+#include "scl_neighbors.h"
 
 using sclabi::Index;
 using sclabi::Real;
@@ -306,6 +307,56 @@ void walk_restart_host(scl_sparse_matrix& m, const Index* seeds, size_t n_seeds,
   SCL_CUDA(cudaMemcpyAsync(scores, sd.p, w.n * sizeof(Real), cudaMemcpyDeviceToHost, w.s));
   st.d2h += (double)w.n * sizeof(Real);
   SCL_CUDA(cudaStreamSynchronize(w.s));
+  st.device_ms = tm.ms();
+  t_stats = st;
+}
+
+// kNN (neighbors.cpp): the handle's primary rows made dense on the device.
+struct DenseSamples {
+  cudaStream_t s;
+  DevBuf X;
+  int64_t n;
+  int d;
+};
+
+DenseSamples dense_samples(scl_sparse_matrix& m, Stats& st) {
+  SCL_REQUIRE(m.valid, SCL_ERROR_INVALID_ARGUMENT, "Invalid sparse matrix");
+  DenseSamples ds;
+  ds.s = library_stream(current_device());
+  ds.n = m.primary_dim();
+  const int64_t d = m.secondary_dim();
+  SCL_REQUIRE(d >= 1 && d <= knn_max_features(), SCL_ERROR_INVALID_ARGUMENT,
+              "kNN on the device takes 1 to 128 features");
+  ds.d = (int)d;
+  auto mir = device_graph(m, ds.s, st.h2d);
+  ds.X = DevBuf(std::max<int64_t>(ds.n * d, 1) * sizeof(Real), ds.s);
+  densify_expression(mir->g.view(), true, ds.n, d, ds.X.p, ds.s);
+  return ds;
+}
+
+void knn_host(scl_sparse_matrix& m, const Real* norms, size_t n_samples, size_t k, Index* out_idx, Real* out_dist) {
+  Stats st;
+  SCL_REQUIRE(n_samples == (size_t)m.primary_dim(), SCL_ERROR_DIMENSION_MISMATCH,
+              "kNN: n_samples must equal the matrix's primary dimension");
+  SCL_REQUIRE(k >= 1 && k <= 64, SCL_ERROR_INVALID_ARGUMENT, "kNN on the device takes k from 1 to 64");
+  DenseSamples ds = dense_samples(m, st);
+  DevBuf nd(std::max<int64_t>(ds.n, 1) * sizeof(Real), ds.s);
+  if (norms) {
+    SCL_CUDA(cudaMemcpyAsync(nd.p, norms, ds.n * sizeof(Real), cudaMemcpyHostToDevice, ds.s));
+    st.h2d += (double)ds.n * sizeof(Real);
+  } else {
+    row_norms_dense(ds.X.p, sclabi::kRealDType, ds.n, ds.d, nd.p, ds.s);
+  }
+  const int64_t total = ds.n * (int64_t)k;
+  DevBuf di(std::max<int64_t>(total, 1) * sizeof(Index), ds.s), dd(std::max<int64_t>(total, 1) * sizeof(Real), ds.s);
+  EventTimer tm(ds.s);
+  tm.start();
+  knn_dense(ds.X.p, nd.p, sclabi::kRealDType, ds.n, ds.d, (int)k, di.p, sclabi::kIndexDType, dd.p, ds.s);
+  tm.stop();
+  SCL_CUDA(cudaMemcpyAsync(out_idx, di.p, total * sizeof(Index), cudaMemcpyDeviceToHost, ds.s));
+  SCL_CUDA(cudaMemcpyAsync(out_dist, dd.p, total * sizeof(Real), cudaMemcpyDeviceToHost, ds.s));
+  st.d2h += (double)total * (sizeof(Index) + sizeof(Real));
+  SCL_CUDA(cudaStreamSynchronize(ds.s));
   st.device_ms = tm.ms();
   t_stats = st;
 }
@@ -642,6 +693,44 @@ SCL_EXPORT scl_error_t scl_algebra_spmm(scl_sparse_t A, const scl_real_t* X, scl
   SCL_CUDA(cudaStreamSynchronize(s));
   st.device_ms = tm.ms();
   t_stats = st;
+  SCL_API_RETURN_OK;
+  SCL_API_CATCH
+}
+
+SCL_EXPORT scl_error_t scl_neighbors_compute_norms(scl_sparse_t matrix, scl_real_t* norms_sq) {
+  SCL_API_CHECK_NULL(matrix, "Matrix handle is null");
+  SCL_API_CHECK_NULL(norms_sq, "Norms output pointer is null");
+  SCL_API_TRY
+  Stats st;
+  DenseSamples ds = dense_samples(*matrix, st);
+  DevBuf nd(std::max<int64_t>(ds.n, 1) * sizeof(Real), ds.s);
+  row_norms_dense(ds.X.p, sclabi::kRealDType, ds.n, ds.d, nd.p, ds.s);
+  if (ds.n > 0) SCL_CUDA(cudaMemcpyAsync(norms_sq, nd.p, ds.n * sizeof(Real), cudaMemcpyDeviceToHost, ds.s));
+  SCL_CUDA(cudaStreamSynchronize(ds.s));
+  SCL_API_RETURN_OK;
+  SCL_API_CATCH
+}
+
+SCL_EXPORT scl_error_t scl_knn(scl_sparse_t matrix, const scl_real_t* norms_sq, scl_size_t n_samples, scl_size_t k,
+                               scl_index_t* out_indices, scl_real_t* out_distances) {
+  SCL_API_CHECK_NULL(matrix, "Matrix handle is null");
+  SCL_API_CHECK_NULL(norms_sq, "Norms input pointer is null");
+  SCL_API_CHECK_NULL(out_indices, "Indices output pointer is null");
+  SCL_API_CHECK_NULL(out_distances, "Distances output pointer is null");
+  SCL_API_CHECK(n_samples > 0 && k > 0, SCL_ERROR_INVALID_ARGUMENT, "Dimensions must be positive");
+  SCL_API_TRY
+  knn_host(*matrix, norms_sq, n_samples, k, out_indices, out_distances);
+  SCL_API_RETURN_OK;
+  SCL_API_CATCH
+}
+
+SCL_EXPORT scl_error_t scl_knn_simple(scl_sparse_t matrix, scl_size_t n_samples, scl_size_t k,
+                                      scl_index_t* out_indices, scl_real_t* out_distances) {
+  SCL_API_CHECK_NULL(matrix, "Matrix handle is null");
+  SCL_API_CHECK_NULL(out_indices, "Indices output pointer is null");
+  SCL_API_CHECK_NULL(out_distances, "Distances output pointer is null");
+  SCL_API_TRY
+  knn_host(*matrix, nullptr, n_samples, k, out_indices, out_distances);
   SCL_API_RETURN_OK;
   SCL_API_CATCH
 }

@@ -276,6 +276,14 @@ void magic_diffuse(const CsrView& aff, void* X, int64_t F, int64_t steps, cudaSt
 // Y (A.n_rows x K) <- alpha A X + beta Y, X: A.n_cols x K (scl_algebra_spmm's arithmetic).
 void algebra_spmm(const CsrView& A, const void* X, int64_t K, void* Y, double alpha, double beta, cudaStream_t s);
 
+// Brute-force kNN (knn.cu) over the rows of a dense n x d block (d <= 128,
+// k <= 64): indices (kI32/kI64) and sqrt distances [n, k], ascending, missing
+// slots (inf, -1); and the squared row norms as sequential fma chains.
+int knn_max_features();
+void knn_dense(const void* X, const void* norms, DType t, int64_t n, int d, int k, void* idx, DType it, void* dist,
+               cudaStream_t s);
+void row_norms_dense(const void* X, DType t, int64_t n, int d, void* out, cudaStream_t s);
+
 // Vector walks (walks.cu). walk_linear: x <- c_x x + c_p P x, `steps` times
 // (lazy random walk, heat-kernel signature). walk_restart: the restart walk
 // y = alpha P x + (1 - alpha) r until the L1 change is below tol or max_iter

@@ -1,3 +1,3 @@
 """ctypes bindings (hand-written in the style scl-core's codegen emits)."""
-from . import algebra, core, diffusion, gpu, impute, sparse  # noqa: F401  (register all functions)
+from . import algebra, core, diffusion, gpu, impute, neighbors, sparse  # noqa: F401  (register all functions)
 from ._loader import Library, VARIANTS, get_library  # noqa: F401

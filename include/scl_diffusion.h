@@ -70,8 +70,15 @@ SCL_EXPORT scl_error_t scl_diffusion_magic_impute(scl_sparse_t transition, scl_r
  * scl_diffusion_compute_dpt_multi_root averages that over the in-range roots
  * (none: all ones), each walked with the default tolerance.
  *
- * Diffusion map embedding and diffusion distance (diffusion.h:79-84, 108-113)
- * are exported for link compatibility and return SCL_ERROR_NOT_IMPLEMENTED. */
+ * Diffusion map embedding (diffusion.h:79-84; diffusion.hpp:366-446,
+ * 901-955): the reference's cosine start, modified Gram-Schmidt with its
+ * re-orthogonalisation rule, then n_iter (0 -> 50) rounds of Q <- P Q and
+ * Gram-Schmidt; the dot products are FP64 block sums and the start uses
+ * CUDA's cos/sin, so the result agrees with the reference to a tolerance.
+ * n_nodes must be at least the primary dimension.
+ *
+ * Diffusion distance (diffusion.h:108-113) is exported for link
+ * compatibility and returns SCL_ERROR_NOT_IMPLEMENTED. */
 SCL_EXPORT scl_error_t scl_diffusion_compute_dpt(scl_sparse_t transition, scl_index_t root_cell,
                                                  scl_real_t* pseudotime, scl_size_t n_nodes, scl_index_t max_iter,
                                                  scl_real_t tol);

@@ -564,9 +564,29 @@ SCL_EXPORT scl_error_t scl_diffusion_personalized_pagerank(scl_sparse_t transiti
   SCL_API_RETURN_OK;
   SCL_API_CATCH
 }
-SCL_EXPORT scl_error_t scl_diffusion_diffusion_map_embedding(scl_sparse_t, scl_real_t*, scl_index_t, scl_index_t,
-                                                             scl_index_t) {
-  SCL_NOT_IMPLEMENTED("scl_diffusion_diffusion_map_embedding");
+SCL_EXPORT scl_error_t scl_diffusion_diffusion_map_embedding(scl_sparse_t transition, scl_real_t* embedding,
+                                                             scl_index_t n_nodes, scl_index_t n_components,
+                                                             scl_index_t n_iter) {
+  SCL_API_CHECK_NULL(transition, "Transition matrix is null");
+  SCL_API_CHECK_NULL(embedding, "Output embedding array is null");
+  SCL_API_CHECK(n_nodes > 0 && n_components > 0, SCL_ERROR_INVALID_ARGUMENT, "Dimensions must be positive");
+  SCL_API_TRY
+  Stats st;
+  WalkSetup w = walk_setup(*transition, (size_t)n_nodes, "DiffusionMap: embedding buffer too small", st);
+  SCL_REQUIRE(n_components <= 4096, SCL_ERROR_INVALID_ARGUMENT, "diffusion map: at most 4096 components");
+  const int64_t total = (int64_t)w.n * n_components;
+  DevBuf out(std::max<int64_t>(total, 1) * sizeof(Real), w.s);
+  EventTimer tm(w.s);
+  tm.start();
+  diffusion_map(w.mir->g.view(), out.p, (int)n_components, n_iter == 0 ? 50 : n_iter, w.s);  // diffusion.cpp:24
+  tm.stop();
+  if (total > 0) SCL_CUDA(cudaMemcpyAsync(embedding, out.p, total * sizeof(Real), cudaMemcpyDeviceToHost, w.s));
+  st.d2h += (double)total * sizeof(Real);
+  SCL_CUDA(cudaStreamSynchronize(w.s));
+  st.device_ms = tm.ms();
+  t_stats = st;
+  SCL_API_RETURN_OK;
+  SCL_API_CATCH
 }
 SCL_EXPORT scl_error_t scl_diffusion_heat_kernel_signature(scl_sparse_t transition, scl_real_t* signature,
                                                            scl_size_t n_nodes, scl_real_t t, scl_index_t n_steps) {

@@ -295,6 +295,9 @@ int64_t walk_restart(const CsrView& P, const void* r, void* scores, double alpha
 // n_roots such rows (all: n_roots x n, summed in root order, times 1/n_roots).
 void dpt(const CsrView& P, int64_t root, void* out, int64_t max_iter, double tol, cudaStream_t s);
 void dpt_average(const void* all, int64_t n_roots, int64_t n, DType t, void* out, cudaStream_t s);
+// Diffusion map embedding: K columns (row-major n x K in out) from a fixed
+// cosine start, orthonormalised, then n_iter rounds of Q <- P Q + Gram-Schmidt.
+void diffusion_map(const CsrView& P, void* out, int K, int64_t n_iter, cudaStream_t s);
 
 // dL/dP in CSR order from its CSC-order accumulator.
 void scatter_adjoint_entries(const Adjoint& adj, const void* gPt, DType t, void* gP, cudaStream_t s);

@@ -291,3 +291,139 @@ int64_t walk_restart(const CsrView& P, const void* r, void* scores, double alpha
 }
 
 }  // namespace sclgpu
+
+// ---- diffusion map embedding (scl/kernel/diffusion.hpp:366-446, 901-955) -------------
+namespace sclgpu {
+namespace {
+
+template <class T>
+__global__ void k_dmap_init(T* __restrict__ Q, int64_t n, int K) {
+  const int64_t total = n * K;
+  for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < total; e += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t i = e / K;
+    const int c = (int)(e % K);
+    const T t = (T)i / (T)n;
+    const T phase = (T)(c + 1) * (T)3.14159265358979323846;
+    Q[e] = wfma((T)0.1, sin(phase * t * (T)2.7), cos(phase * t));
+  }
+}
+
+// Block-wide sum of a per-thread double, returned to every thread.
+__device__ double block_sum(double v, double* red) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  __syncthreads();
+  if (lane == 0) red[w] = v;
+  __syncthreads();
+  double s = 0.0;
+  for (int k = 0; k < (int)(blockDim.x >> 5); ++k) s += red[k];
+  return s;
+}
+
+// Modified Gram-Schmidt with re-orthogonalisation over the K columns of the
+// row-major n x K block Q, with the reference's control flow: each column is
+// projected off the previous ones (coefficients dot / |q_p|^2 when
+// |q_p|^2 > 1e-15), re-projected (up to 2 more passes) while its largest
+// cosine with them is at least 0.7 after the first pass, and normalised; a
+// column of norm^2 <= 1e-15 becomes the unit vector e_(v mod n). One CTA runs
+// the whole loop; the sums are FP64 block reductions.
+template <class T>
+__global__ void __launch_bounds__(1024) k_gram_schmidt(T* __restrict__ Q, int64_t n, int K, T* __restrict__ w) {
+  __shared__ double red[32];
+  const int tid = threadIdx.x;
+  const int NT = blockDim.x;
+  for (int v = 0; v < K; ++v) {
+    for (int64_t i = tid; i < n; i += NT) w[i] = Q[i * K + v];
+    __syncthreads();
+    for (int reorth = 0; reorth <= 2; ++reorth) {
+      for (int p = 0; p < v; ++p) {
+        double a = 0.0, b = 0.0;
+        for (int64_t i = tid; i < n; i += NT) {
+          const double q = (double)Q[i * K + p];
+          a += (double)w[i] * q;
+          b += q * q;
+        }
+        const T dot = (T)block_sum(a, red);
+        const T norm_p = (T)block_sum(b, red);
+        if (norm_p > (T)1e-15) {
+          const T coeff = dot / norm_p;
+          for (int64_t i = tid; i < n; i += NT) w[i] = wfma(-coeff, Q[i * K + p], w[i]);
+        }
+        __syncthreads();
+      }
+      double c = 0.0;
+      for (int64_t i = tid; i < n; i += NT) c += (double)w[i] * (double)w[i];
+      const T norm_v = (T)block_sum(c, red);
+      if (reorth == 0 && v > 0) {
+        T max_cos = T(0);
+        for (int p = 0; p < v; ++p) {
+          double a = 0.0;
+          for (int64_t i = tid; i < n; i += NT) a += (double)w[i] * (double)Q[i * K + p];
+          const T dot = (T)block_sum(a, red);
+          const T cv = (norm_v > (T)1e-15) ? (dot < T(0) ? -dot : dot) / sqrt(norm_v) : T(0);
+          max_cos = cv > max_cos ? cv : max_cos;
+        }
+        if (max_cos < (T)0.7) break;
+      } else {
+        break;
+      }
+    }
+    double c = 0.0;
+    for (int64_t i = tid; i < n; i += NT) c += (double)w[i] * (double)w[i];
+    const T norm = (T)block_sum(c, red);
+    if (norm > (T)1e-15) {
+      const T inv = T(1) / sqrt(norm);
+      for (int64_t i = tid; i < n; i += NT) Q[i * K + v] = wmul(w[i], inv);
+    } else {
+      for (int64_t i = tid; i < n; i += NT) Q[i * K + v] = (i == (int64_t)v % n) ? T(1) : T(0);
+    }
+    __syncthreads();
+  }
+}
+
+template <class T>
+void dmap_typed(const CsrView& P, T* out, int K, int64_t n_iter, cudaStream_t s) {
+  const int64_t n = P.n_rows;
+  const size_t bytes = (size_t)n * K * sizeof(T);
+  DevBuf qa(bytes, s), qb(bytes, s), w((size_t)n * sizeof(T), s);
+  int dev = 0;
+  SCL_CUDA(cudaGetDevice(&dev));
+  const unsigned g = (unsigned)std::max<int64_t>(1, std::min<int64_t>((n * K + 255) / 256, (int64_t)sm_count(dev) * 8));
+  k_dmap_init<T><<<g, 256, 0, s>>>(qa.as<T>(), n, K);
+  SCL_CUDA(cudaGetLastError());
+  k_gram_schmidt<T><<<1, 1024, 0, s>>>(qa.as<T>(), n, K, w.as<T>());
+  SCL_CUDA(cudaGetLastError());
+  SpmmArgs a{};
+  a.indptr = P.indptr;
+  a.indices = P.indices;
+  a.values = P.values;
+  a.vtype = P.vtype;
+  a.n_rows = n;
+  a.F = K;
+  a.xtype = P.vtype;
+  a.ytype = P.vtype;
+  T* q = qa.as<T>();
+  T* qn = qb.as<T>();
+  for (int64_t it = 0; it < n_iter; ++it) {
+    a.X = q;
+    a.Y = qn;
+    spmm(a, s);
+    k_gram_schmidt<T><<<1, 1024, 0, s>>>(qn, n, K, w.as<T>());
+    SCL_CUDA(cudaGetLastError());
+    std::swap(q, qn);
+  }
+  SCL_CUDA(cudaMemcpyAsync(out, q, bytes, cudaMemcpyDeviceToDevice, s));
+}
+
+}  // namespace
+
+void diffusion_map(const CsrView& P, void* out, int K, int64_t n_iter, cudaStream_t s) {
+  SCL_REQUIRE(P.n_cols <= P.n_rows, kErrDimensionMismatch, "diffusion map: column indices must address rows");
+  if (P.n_rows == 0 || K <= 0) return;
+  if (P.vtype == kF32) return dmap_typed<float>(P, static_cast<float*>(out), K, n_iter, s);
+  SCL_REQUIRE(P.vtype == kF64, kErrTypeMismatch, "diffusion map values must be f32 or f64");
+  dmap_typed<double>(P, static_cast<double*>(out), K, n_iter, s);
+}
+
+}  // namespace sclgpu

@@ -74,6 +74,17 @@ def compute_dpt_multi_root(mat: CsrMatrix, roots, n_nodes: int = None, max_iter:
     return out
 
 
+def diffusion_map_embedding(mat: CsrMatrix, n_components: int, n_iter: int = 50, n_nodes: int = None) -> np.ndarray:
+    """n x n_components diffusion-map coordinates (scl_diffusion_diffusion_map_embedding)."""
+    lib = mat.lib
+    n = mat.shape[0] if n_nodes is None else int(n_nodes)
+    out = np.zeros((n, int(n_components)), dtype=mat.real_dtype)
+    check_error(lib.scl_diffusion_diffusion_map_embedding(mat.handle, out.ctypes.data_as(ctypes.POINTER(lib.real_type)),
+                                                          n, int(n_components), int(n_iter)),
+                "diffusion_map_embedding", lib)
+    return out
+
+
 def random_walk_with_restart(mat: CsrMatrix, seeds, n_nodes: int = None, alpha: float = 0.85, max_iter: int = 100,
                              tol: float = 1e-6) -> np.ndarray:
     """Scores of the walk that restarts on `seeds` (scl_diffusion_random_walk_with_restart)."""

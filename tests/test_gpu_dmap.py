@@ -1,0 +1,54 @@
+"""Diffusion map embedding through the drop-in C ABI on the GPU against
+scl-core's own scl_diffusion_diffusion_map_embedding (compiled from the
+reference sources and shipped with the tests). The GPU reduces the
+Gram-Schmidt dot products in FP64 blocks where the reference sums
+sequentially, and its starting cosines come from CUDA's cos/sin, so the two
+agree to a tolerance, not bit for bit; both outputs are orthonormal."""
+import numpy as np
+import pytest
+import scipy.sparse as sp
+
+import scl
+from oracle import ref
+
+pytestmark = pytest.mark.gpu
+
+
+def _graph(n, dt, idt, seed):
+    rng = np.random.default_rng(seed)
+    pts = np.concatenate([rng.standard_normal((n // 2, 5)), rng.standard_normal((n - n // 2, 5)) + 4.0])
+    d2 = ((pts[:, None, :] - pts[None, :, :]) ** 2).sum(-1)
+    W = np.exp(-d2 / 4.0) * (d2 < 9.0)
+    np.fill_diagonal(W, 0.0)
+    P = sp.csr_matrix(W / W.sum(1, keepdims=True)).astype(dt)
+    P.sort_indices()
+    m = scl.CsrMatrix.wrap(P.indptr.astype(idt), P.indices.astype(idt), P.data, P.shape)
+    return m, P
+
+
+@pytest.mark.parametrize("dt,idt,tol", [(np.float32, np.int32, 2e-3), (np.float64, np.int64, 1e-8)])
+@pytest.mark.parametrize("n,K,n_iter", [(200, 3, 10), (400, 6, 50), (300, 1, 0)])
+def test_diffusion_map_matches_reference(dt, idt, tol, n, K, n_iter):
+    variant = "f32_i32" if dt == np.float32 else "f64_i64"
+    m, P = _graph(n, dt, idt, seed=n + K)
+    got = scl.diffusion.diffusion_map_embedding(m, K, n_iter)
+    G = got.astype(np.float64)
+    np.testing.assert_allclose(G.T @ G, np.eye(K), atol=50 * tol)
+    if not ref.available(variant):
+        pytest.skip("reference library not shipped with the tests")
+    want = ref.RefLib(variant).diffusion_map(P.indptr, P.indices, P.data, n, K, n_iter)
+    np.testing.assert_allclose(got, want, atol=tol, rtol=0)
+
+
+def test_diffusion_map_errors():
+    m, _ = _graph(20, np.float32, np.int32, 1)
+    out = np.zeros((20, 2), np.float32)
+    import ctypes
+
+    lib = m.lib
+    P = out.ctypes.data_as(ctypes.POINTER(lib.real_type))
+    assert lib.scl_diffusion_diffusion_map_embedding(None, P, 20, 2, 5) == 4
+    assert lib.scl_diffusion_diffusion_map_embedding(m.handle, None, 20, 2, 5) == 4
+    assert lib.scl_diffusion_diffusion_map_embedding(m.handle, P, 0, 2, 5) == 10
+    assert lib.scl_diffusion_diffusion_map_embedding(m.handle, P, 20, 0, 5) == 10
+    assert lib.scl_diffusion_diffusion_map_embedding(m.handle, P, 19, 2, 5) == 11

@@ -77,8 +77,11 @@ SCL_EXPORT scl_error_t scl_diffusion_magic_impute(scl_sparse_t transition, scl_r
  * CUDA's cos/sin, so the result agrees with the reference to a tolerance.
  * n_nodes must be at least the primary dimension.
  *
- * Diffusion distance (diffusion.h:108-113) is exported for link
- * compatibility and returns SCL_ERROR_NOT_IMPLEMENTED. */
+ * Diffusion distance (diffusion.h:108-113; diffusion.hpp:1024-1130): the n x n
+ * pairwise L2 distances (row stride n) between the rows of P^n_steps for
+ * n <= 1000 and between its columns for n > 1000, the reference's two
+ * branches; each pair sums its rounded squares in order. At most 46,340
+ * nodes. */
 SCL_EXPORT scl_error_t scl_diffusion_compute_dpt(scl_sparse_t transition, scl_index_t root_cell,
                                                  scl_real_t* pseudotime, scl_size_t n_nodes, scl_index_t max_iter,
                                                  scl_real_t tol);

@@ -83,6 +83,7 @@ class RefLib:
         L.scl_diffusion_compute_dpt.argtypes = [P, I, P, ctypes.c_size_t, I, R_]
         L.scl_knn.argtypes = [P, P, ctypes.c_size_t, ctypes.c_size_t, P, P]
         L.scl_diffusion_diffusion_map_embedding.argtypes = [P, P, I, I, I]
+        L.scl_diffusion_diffusion_distance.argtypes = [P, P, ctypes.c_size_t, I]
         L.scl_neighbors_compute_norms.argtypes = [P, P]
         L.scl_diffusion_compute_dpt_multi_root.argtypes = [P, P, ctypes.c_size_t, P, ctypes.c_size_t, I]
         L.scl_impute_magic.argtypes = [P, P, I, I, I, P]
@@ -95,7 +96,7 @@ class RefLib:
                    "scl_diffusion_personalized_pagerank", "scl_diffusion_lazy_random_walk",
                    "scl_diffusion_heat_kernel_signature", "scl_diffusion_compute_dpt",
                    "scl_diffusion_compute_dpt_multi_root", "scl_knn", "scl_neighbors_compute_norms",
-                   "scl_diffusion_diffusion_map_embedding"):
+                   "scl_diffusion_diffusion_map_embedding", "scl_diffusion_diffusion_distance"):
             getattr(L, fn).restype = ctypes.c_int32
         self.L = L
 
@@ -239,6 +240,15 @@ class RefLib:
         out = np.zeros((n, K), self.real_dtype)
         try:
             self._check(self.L.scl_diffusion_diffusion_map_embedding(h, out.ctypes.data, n, K, n_iter))
+            return out
+        finally:
+            self.destroy(h)
+
+    def diffusion_distance(self, indptr, indices, data, n, steps):
+        h, keep = self.wrap(indptr, indices, data, (n, n))
+        out = np.zeros((n, n), self.real_dtype)
+        try:
+            self._check(self.L.scl_diffusion_diffusion_distance(h, out.ctypes.data, n, steps))
             return out
         finally:
             self.destroy(h)

@@ -604,8 +604,27 @@ SCL_EXPORT scl_error_t scl_diffusion_heat_kernel_signature(scl_sparse_t transiti
   SCL_API_RETURN_OK;
   SCL_API_CATCH
 }
-SCL_EXPORT scl_error_t scl_diffusion_diffusion_distance(scl_sparse_t, scl_real_t*, scl_size_t, scl_index_t) {
-  SCL_NOT_IMPLEMENTED("scl_diffusion_diffusion_distance");
+SCL_EXPORT scl_error_t scl_diffusion_diffusion_distance(scl_sparse_t transition, scl_real_t* distances,
+                                                        scl_size_t n_nodes, scl_index_t n_steps) {
+  SCL_API_CHECK_NULL(transition, "Transition matrix is null");
+  SCL_API_CHECK_NULL(distances, "Output distances array is null");
+  SCL_API_CHECK(n_nodes > 0 && n_steps > 0, SCL_ERROR_INVALID_ARGUMENT, "Dimensions must be positive");
+  SCL_API_TRY
+  Stats st;
+  WalkSetup w = walk_setup(*transition, n_nodes, "DiffusionDist: output buffer too small", st);
+  const int64_t total = (int64_t)w.n * w.n;  // written with row stride n, as the reference
+  DevBuf D(std::max<int64_t>(total, 1) * sizeof(Real), w.s);
+  EventTimer tm(w.s);
+  tm.start();
+  diffusion_distance(w.mir->g.view(), D.p, n_steps, w.s);
+  tm.stop();
+  if (total > 0) SCL_CUDA(cudaMemcpyAsync(distances, D.p, total * sizeof(Real), cudaMemcpyDeviceToHost, w.s));
+  st.d2h += (double)total * sizeof(Real);
+  SCL_CUDA(cudaStreamSynchronize(w.s));
+  st.device_ms = tm.ms();
+  t_stats = st;
+  SCL_API_RETURN_OK;
+  SCL_API_CATCH
 }
 SCL_EXPORT scl_error_t scl_diffusion_lazy_random_walk(scl_sparse_t transition, scl_real_t* x, scl_size_t n_nodes,
                                                       scl_index_t n_steps, scl_real_t laziness) {

@@ -298,6 +298,9 @@ void dpt_average(const void* all, int64_t n_roots, int64_t n, DType t, void* out
 // Diffusion map embedding: K columns (row-major n x K in out) from a fixed
 // cosine start, orthonormalised, then n_iter rounds of Q <- P Q + Gram-Schmidt.
 void diffusion_map(const CsrView& P, void* out, int K, int64_t n_iter, cudaStream_t s);
+// Diffusion distance: D (n x n) = pairwise L2 distances between the rows of
+// P^steps (n <= 1000) or its columns (n > 1000), as the reference's two branches.
+void diffusion_distance(const CsrView& P, void* D, int64_t steps, cudaStream_t s);
 
 // dL/dP in CSR order from its CSC-order accumulator.
 void scatter_adjoint_entries(const Adjoint& adj, const void* gPt, DType t, void* gP, cudaStream_t s);

@@ -427,3 +427,112 @@ void diffusion_map(const CsrView& P, void* out, int K, int64_t n_iter, cudaStrea
 }
 
 }  // namespace sclgpu
+
+// ---- diffusion distance (scl/kernel/diffusion.hpp:1024-1130) ---------------------------
+namespace sclgpu {
+namespace {
+
+template <class T>
+__global__ void k_identity(T* __restrict__ Z, int64_t n) {
+  const int64_t total = n * n;
+  for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < total; e += (int64_t)gridDim.x * blockDim.x)
+    Z[e] = (e / n == e % n) ? T(1) : T(0);
+}
+
+template <class T>
+__global__ void k_transpose_sq(const T* __restrict__ A, T* __restrict__ B, int64_t n) {
+  __shared__ T tile[32][33];
+  const int64_t bx = (int64_t)blockIdx.x * 32, by = (int64_t)blockIdx.y * 32;
+  for (int r = threadIdx.y; r < 32; r += blockDim.y) {
+    const int64_t i = by + r, j = bx + threadIdx.x;
+    if (i < n && j < n) tile[r][threadIdx.x] = A[i * n + j];
+  }
+  __syncthreads();
+  for (int r = threadIdx.y; r < 32; r += blockDim.y) {
+    const int64_t i = bx + r, j = by + threadIdx.x;
+    if (i < n && j < n) B[i * n + j] = tile[threadIdx.x][r];
+  }
+}
+
+// D[i][j] = D[j][i] = sqrt(sum_k (Z[i][k] - Z[j][k])^2) for i < j, summed over
+// k in order with each square rounded before it is added; D[i][i] = 0. A CTA takes a 32 x 32 block of
+// (i, j) above the diagonal and stages 32-column slices of both row sets.
+template <class T>
+__global__ void k_pair_dist(const T* __restrict__ Z, int64_t n, T* __restrict__ D) {
+  __shared__ T A[32][33], B[32][33];
+  const int64_t bi = (int64_t)blockIdx.y * 32, bj = (int64_t)blockIdx.x * 32;
+  if (bj + 31 < bi) return;  // block entirely below the diagonal
+  const int ty = threadIdx.y, tx = threadIdx.x;
+  const int64_t i = bi + ty, j = bj + tx;
+  T acc = T(0);
+  for (int64_t k0 = 0; k0 < n; k0 += 32) {
+    const int64_t k = k0 + tx;
+    A[ty][tx] = (bi + ty < n && k < n) ? Z[(bi + ty) * n + k] : T(0);
+    B[ty][tx] = (bj + ty < n && k < n) ? Z[(bj + ty) * n + k] : T(0);
+    __syncthreads();
+    const int kn = (n - k0) < 32 ? (int)(n - k0) : 32;
+    for (int kk = 0; kk < kn; ++kk) {
+      const T diff = A[ty][kk] - B[tx][kk];
+      acc = acc + wmul(diff, diff);  // a rounded product, then the sum (no fma), as the reference
+    }
+    __syncthreads();
+  }
+  if (i < n && j < n) {
+    if (i == j) D[i * n + i] = T(0);
+    else if (i < j) {
+      const T dist = sqrt(acc);
+      D[i * n + j] = dist;
+      D[j * n + i] = dist;
+    }
+  }
+}
+
+template <class T>
+void ddist_typed(const CsrView& P, T* D, int64_t steps, cudaStream_t s) {
+  const int64_t n = P.n_rows;
+  const size_t bytes = (size_t)n * (size_t)n * sizeof(T);
+  DevBuf za(bytes, s), zb(bytes, s);
+  int dev = 0;
+  SCL_CUDA(cudaGetDevice(&dev));
+  const unsigned g = (unsigned)std::max<int64_t>(1, std::min<int64_t>((n * n + 255) / 256, (int64_t)sm_count(dev) * 16));
+  k_identity<T><<<g, 256, 0, s>>>(za.as<T>(), n);
+  SCL_CUDA(cudaGetLastError());
+  SpmmArgs a{};
+  a.indptr = P.indptr;
+  a.indices = P.indices;
+  a.values = P.values;
+  a.vtype = P.vtype;
+  a.n_rows = n;
+  a.F = n;
+  a.xtype = P.vtype;
+  a.ytype = P.vtype;
+  T* z = za.as<T>();
+  T* zn = zb.as<T>();
+  for (int64_t st = 0; st < steps; ++st) {  // Z <- P Z: the rows of P^t
+    a.X = z;
+    a.Y = zn;
+    spmm(a, s);
+    std::swap(z, zn);
+  }
+  const dim3 blocks((unsigned)((n + 31) / 32), (unsigned)((n + 31) / 32));
+  if (n > 1000) {  // the reference's large-n branch compares columns of P^t (P^t e_i)
+    k_transpose_sq<T><<<blocks, dim3(32, 8), 0, s>>>(z, zn, n);
+    SCL_CUDA(cudaGetLastError());
+    std::swap(z, zn);
+  }
+  k_pair_dist<T><<<blocks, dim3(32, 32), 0, s>>>(z, n, D);
+  SCL_CUDA(cudaGetLastError());
+}
+
+}  // namespace
+
+void diffusion_distance(const CsrView& P, void* D, int64_t steps, cudaStream_t s) {
+  SCL_REQUIRE(P.n_cols <= P.n_rows, kErrDimensionMismatch, "diffusion distance: column indices must address rows");
+  SCL_REQUIRE(P.n_rows <= 46340, kErrInvalidArgument, "diffusion distance: at most 46,340 nodes (n^2 < 2^31)");
+  if (P.n_rows == 0) return;
+  if (P.vtype == kF32) return ddist_typed<float>(P, static_cast<float*>(D), steps, s);
+  SCL_REQUIRE(P.vtype == kF64, kErrTypeMismatch, "diffusion distance values must be f32 or f64");
+  ddist_typed<double>(P, static_cast<double*>(D), steps, s);
+}
+
+}  // namespace sclgpu

@@ -85,6 +85,16 @@ def diffusion_map_embedding(mat: CsrMatrix, n_components: int, n_iter: int = 50,
     return out
 
 
+def diffusion_distance(mat: CsrMatrix, n_steps: int = 3) -> np.ndarray:
+    """n x n pairwise diffusion distances (scl_diffusion_diffusion_distance)."""
+    lib = mat.lib
+    n = mat.shape[0]
+    out = np.zeros((n, n), dtype=mat.real_dtype)
+    check_error(lib.scl_diffusion_diffusion_distance(mat.handle, out.ctypes.data_as(ctypes.POINTER(lib.real_type)), n,
+                                                     int(n_steps)), "diffusion_distance", lib)
+    return out
+
+
 def random_walk_with_restart(mat: CsrMatrix, seeds, n_nodes: int = None, alpha: float = 0.85, max_iter: int = 100,
                              tol: float = 1e-6) -> np.ndarray:
     """Scores of the walk that restarts on `seeds` (scl_diffusion_random_walk_with_restart)."""

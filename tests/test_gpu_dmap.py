@@ -52,3 +52,39 @@ def test_diffusion_map_errors():
     assert lib.scl_diffusion_diffusion_map_embedding(m.handle, P, 0, 2, 5) == 10
     assert lib.scl_diffusion_diffusion_map_embedding(m.handle, P, 20, 0, 5) == 10
     assert lib.scl_diffusion_diffusion_map_embedding(m.handle, P, 19, 2, 5) == 11
+
+
+@pytest.mark.parametrize("dt,idt", [(np.float32, np.int32), (np.float64, np.int64)])
+def test_diffusion_distance_small_graph_bit_exact_with_reference(dt, idt):
+    """n <= 1000: the reference diffuses the identity with spmm_block (the
+    library's SpMM gives the same bits) and sums the rounded squares of row
+    differences in order. In FP64 the GPU output equals it bit for bit; in FP32
+    0.05 % of the entries of this graph differ by one ulp, which a sequential
+    multiply-add restatement in NumPy reproduces as well (the reference's own
+    compiled loop rounds a few of those sums differently)."""
+    variant = "f32_i32" if dt == np.float32 else "f64_i64"
+    m, P = _graph(300, dt, idt, seed=4)
+    got = scl.diffusion.diffusion_distance(m, 3)
+    assert np.all(np.diag(got) == 0) and np.array_equal(got, got.T)
+    if not ref.available(variant):
+        pytest.skip("reference library not shipped with the tests")
+    want = ref.RefLib(variant).diffusion_distance(P.indptr, P.indices, P.data, 300, 3)
+    if dt == np.float64:
+        np.testing.assert_array_equal(got.view(np.uint8), want.view(np.uint8))
+    else:
+        np.testing.assert_array_max_ulp(got, want, maxulp=1)
+        assert np.mean(got == want) > 0.99
+
+
+def test_diffusion_distance_large_graph_compares_columns():
+    """n > 1000: the reference's row-by-row branch diffuses unit vectors, so it
+    compares columns of P^t; checked against an FP64 restatement."""
+    m, P = _graph(1100, np.float64, np.int64, seed=5)
+    got = scl.diffusion.diffusion_distance(m, 2)
+    Z = np.eye(1100)
+    for _ in range(2):
+        Z = P @ Z
+    C = Z.T  # column i of P^t as row i
+    sq = (C * C).sum(1)
+    want = np.sqrt(np.maximum(sq[:, None] + sq[None, :] - 2 * C @ C.T, 0))
+    np.testing.assert_allclose(got, want, atol=1e-7)

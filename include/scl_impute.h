@@ -19,14 +19,21 @@
 extern "C" {
 #endif
 
-/* impute.h:15-25 (k-nearest-neighbour imputation): not part of this build;
- * returns SCL_ERROR_NOT_IMPLEMENTED. */
+/* impute.h:15-25 (impute.cpp:19-52, impute.hpp:400-510): X_imputed is the
+ * dense block (later duplicates winning), then every value not above
+ * `threshold` becomes the mean of the listed neighbours (knn_indices, n_cells
+ * x k_neighbors; out-of-range ones skipped) that store the gene (their first
+ * stored value; a stored zero counts), weighted by
+ * exp(-(d / (bandwidth + 1e-12))^2), when the weight sum exceeds 1e-12 and the
+ * mean exceeds 1e-10. The weights use CUDA's exp, so values agree with the
+ * reference to rounding. */
 SCL_EXPORT scl_error_t scl_impute_knn(scl_sparse_t matrix, const scl_index_t* knn_indices,
                                       const scl_real_t* knn_distances, scl_index_t n_cells, scl_index_t n_genes,
                                       scl_index_t k_neighbors, scl_real_t* X_imputed, scl_real_t bandwidth,
                                       scl_real_t threshold);
 
-/* impute.h:28-38: not part of this build; returns SCL_ERROR_NOT_IMPLEMENTED. */
+/* impute.h:28-38: the same computation (scl-core's impute.cpp:54-87 runs the
+ * same kernel for it). */
 SCL_EXPORT scl_error_t scl_impute_knn_weighted(scl_sparse_t matrix, const scl_index_t* knn_indices,
                                                const scl_real_t* knn_distances, scl_index_t n_cells,
                                                scl_index_t n_genes, scl_index_t k_neighbors, scl_real_t* X_imputed,

@@ -87,12 +87,14 @@ class RefLib:
         L.scl_neighbors_compute_norms.argtypes = [P, P]
         L.scl_diffusion_compute_dpt_multi_root.argtypes = [P, P, ctypes.c_size_t, P, ctypes.c_size_t, I]
         L.scl_impute_magic.argtypes = [P, P, I, I, I, P]
+        L.scl_impute_knn.argtypes = [P, P, P, I, I, I, P, self.c_real, self.c_real]
         L.scl_get_last_error.restype = ctypes.c_char_p
         for fn in ("scl_sparse_wrap", "scl_sparse_create_with_strategy", "scl_sparse_destroy",
                    "scl_sparse_transpose", "scl_sparse_export", "scl_sparse_nnz", "scl_sparse_is_contiguous",
                    "scl_diffusion_compute_transition_matrix", "scl_diffusion_diffuse_matrix",
                    "scl_diffusion_diffuse_vector", "scl_diffusion_magic_impute", "scl_algebra_spmm",
-                   "scl_impute_diffusion", "scl_impute_magic", "scl_diffusion_random_walk_with_restart",
+                   "scl_impute_diffusion", "scl_impute_magic", "scl_impute_knn",
+                   "scl_diffusion_random_walk_with_restart",
                    "scl_diffusion_personalized_pagerank", "scl_diffusion_lazy_random_walk",
                    "scl_diffusion_heat_kernel_signature", "scl_diffusion_compute_dpt",
                    "scl_diffusion_compute_dpt_multi_root", "scl_knn", "scl_neighbors_compute_norms",
@@ -184,6 +186,18 @@ class RefLib:
             return Y
         finally:
             self.destroy(h)
+
+    def impute_knn(self, x_csr, x_shape, x_is_csr, nbr, dist, n_cells, n_genes, bandwidth, threshold):
+        hx, kx = self.wrap(*x_csr, x_shape, is_csr=x_is_csr)
+        nbr = np.ascontiguousarray(nbr, self.index_dtype)
+        dist = np.ascontiguousarray(dist, self.real_dtype)
+        out = np.zeros((n_cells, n_genes), self.real_dtype)
+        try:
+            self._check(self.L.scl_impute_knn(hx, nbr.ctypes.data, dist.ctypes.data, n_cells, n_genes, nbr.shape[1],
+                                              out.ctypes.data, bandwidth, threshold))
+            return out
+        finally:
+            self.destroy(hx)
 
     def impute(self, kind, x_csr, x_shape, x_is_csr, t_csr, n_cells, n_genes, steps):
         """scl_impute_diffusion (kind 'diffusion') or scl_impute_magic on

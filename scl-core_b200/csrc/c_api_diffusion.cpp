@@ -311,6 +311,34 @@ void walk_restart_host(scl_sparse_matrix& m, const Index* seeds, size_t n_seeds,
   t_stats = st;
 }
 
+// kNN imputation (impute.cpp:19-87, impute.hpp:400-510).
+void knn_impute_host(scl_sparse_matrix& X, const Index* nbr, const Real* dist, Index n_cells, Index n_genes, Index K,
+                     Real* X_imputed, Real bandwidth, Real threshold) {
+  SCL_REQUIRE(X.valid, SCL_ERROR_INVALID_ARGUMENT, "Expression matrix is not valid");
+  SCL_REQUIRE(X.primary_dim() >= (X.is_csr ? n_cells : n_genes), SCL_ERROR_DIMENSION_MISMATCH,
+              "Imputation: the expression matrix has fewer cells (CSR rows) or genes (CSC columns) than requested");
+  const int dev = current_device();
+  cudaStream_t s = library_stream(dev);
+  Stats st;
+  auto xm = device_graph(X, s, st.h2d);
+  const int64_t nk = (int64_t)n_cells * K, total = (int64_t)n_cells * n_genes;
+  DevBuf nb(std::max<int64_t>(nk, 1) * sizeof(Index), s), ds(std::max<int64_t>(nk, 1) * sizeof(Real), s);
+  DevBuf out(std::max<int64_t>(total, 1) * sizeof(Real), s);
+  SCL_CUDA(cudaMemcpyAsync(nb.p, nbr, nk * sizeof(Index), cudaMemcpyHostToDevice, s));
+  SCL_CUDA(cudaMemcpyAsync(ds.p, dist, nk * sizeof(Real), cudaMemcpyHostToDevice, s));
+  st.h2d += (double)nk * (sizeof(Index) + sizeof(Real));
+  EventTimer tm(s);
+  tm.start();
+  knn_impute(xm->g.view(), X.is_csr, n_cells, n_genes, nb.p, sclabi::kIndexDType, ds.p, (int)K, (double)bandwidth,
+             (double)threshold, out.p, s);
+  tm.stop();
+  SCL_CUDA(cudaMemcpyAsync(X_imputed, out.p, total * sizeof(Real), cudaMemcpyDeviceToHost, s));
+  st.d2h += (double)total * sizeof(Real);
+  SCL_CUDA(cudaStreamSynchronize(s));
+  st.device_ms = tm.ms();
+  t_stats = st;
+}
+
 // kNN (neighbors.cpp): the handle's primary rows made dense on the device.
 struct DenseSamples {
   cudaStream_t s;
@@ -774,13 +802,38 @@ SCL_EXPORT scl_error_t scl_knn_simple(scl_sparse_t matrix, scl_size_t n_samples,
   SCL_API_CATCH
 }
 
-SCL_EXPORT scl_error_t scl_impute_knn(scl_sparse_t, const scl_index_t*, const scl_real_t*, scl_index_t, scl_index_t,
-                                      scl_index_t, scl_real_t*, scl_real_t, scl_real_t) {
-  SCL_NOT_IMPLEMENTED("scl_impute_knn");
+SCL_EXPORT scl_error_t scl_impute_knn(scl_sparse_t matrix, const scl_index_t* knn_indices,
+                                      const scl_real_t* knn_distances, scl_index_t n_cells, scl_index_t n_genes,
+                                      scl_index_t k_neighbors, scl_real_t* X_imputed, scl_real_t bandwidth,
+                                      scl_real_t threshold) {
+  SCL_API_CHECK_NULL(matrix, "Matrix is null");
+  SCL_API_CHECK_NULL(knn_indices, "KNN indices array is null");
+  SCL_API_CHECK_NULL(knn_distances, "KNN distances array is null");
+  SCL_API_CHECK_NULL(X_imputed, "Output imputed matrix is null");
+  SCL_API_CHECK(n_cells > 0 && n_genes > 0 && k_neighbors > 0, SCL_ERROR_INVALID_ARGUMENT,
+                "Dimensions must be positive");
+  SCL_API_TRY
+  knn_impute_host(*matrix, knn_indices, knn_distances, n_cells, n_genes, k_neighbors, X_imputed, bandwidth, threshold);
+  SCL_API_RETURN_OK;
+  SCL_API_CATCH
 }
-SCL_EXPORT scl_error_t scl_impute_knn_weighted(scl_sparse_t, const scl_index_t*, const scl_real_t*, scl_index_t,
-                                               scl_index_t, scl_index_t, scl_real_t*, scl_real_t, scl_real_t) {
-  SCL_NOT_IMPLEMENTED("scl_impute_knn_weighted");
+
+// impute.cpp:54-87: the reference's weighted entry point runs the same kernel
+// (knn_impute_dense, Gaussian weights of the given distances).
+SCL_EXPORT scl_error_t scl_impute_knn_weighted(scl_sparse_t matrix, const scl_index_t* knn_indices,
+                                               const scl_real_t* knn_distances, scl_index_t n_cells,
+                                               scl_index_t n_genes, scl_index_t k_neighbors, scl_real_t* X_imputed,
+                                               scl_real_t bandwidth, scl_real_t threshold) {
+  SCL_API_CHECK_NULL(matrix, "Matrix is null");
+  SCL_API_CHECK_NULL(knn_indices, "KNN indices array is null");
+  SCL_API_CHECK_NULL(knn_distances, "KNN distances array is null");
+  SCL_API_CHECK_NULL(X_imputed, "Output imputed matrix is null");
+  SCL_API_CHECK(n_cells > 0 && n_genes > 0 && k_neighbors > 0, SCL_ERROR_INVALID_ARGUMENT,
+                "Dimensions must be positive");
+  SCL_API_TRY
+  knn_impute_host(*matrix, knn_indices, knn_distances, n_cells, n_genes, k_neighbors, X_imputed, bandwidth, threshold);
+  SCL_API_RETURN_OK;
+  SCL_API_CATCH
 }
 
 }  // extern "C"

@@ -273,6 +273,11 @@ double gather_floor_ms(const int32_t* idx, int64_t M, int64_t n_rows, int64_t ro
 // X <- W X with W the row-normalised affinity (rows with sum < 1e-12 copy X).
 void densify_expression(const CsrView& m, bool csr, int64_t n_cells, int64_t n_genes, void* dense, cudaStream_t s);
 void magic_diffuse(const CsrView& aff, void* X, int64_t F, int64_t steps, cudaStream_t s);
+// kNN imputation: out (n_cells x n_genes) = the dense block with every value
+// not above threshold replaced by the Gaussian-weighted mean of the neighbours
+// (nbr, dist: n_cells x K) that store the gene.
+void knn_impute(const CsrView& m, bool csr, int64_t n_cells, int64_t n_genes, const void* nbr, DType it,
+                const void* dist, int K, double bandwidth, double threshold, void* out, cudaStream_t s);
 // Y (A.n_rows x K) <- alpha A X + beta Y, X: A.n_cols x K (scl_algebra_spmm's arithmetic).
 void algebra_spmm(const CsrView& A, const void* X, int64_t K, void* Y, double alpha, double beta, cudaStream_t s);
 

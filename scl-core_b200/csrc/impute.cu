@@ -47,6 +47,78 @@ __global__ void k_densify(const int64_t* __restrict__ ptr, const int32_t* __rest
   }
 }
 
+// The lookup side of kNN imputation: the FIRST stored value of every
+// (cell, gene) inside the block (the reference's has_expression finds the
+// first match) and a mask of the stored positions (a stored zero counts).
+template <class T>
+__global__ void k_densify_first(const int64_t* __restrict__ ptr, const int32_t* __restrict__ idx,
+                                const T* __restrict__ val, int64_t n_primary, int64_t n_cells, int64_t n_genes,
+                                int csr, T* __restrict__ dense, unsigned char* __restrict__ mask) {
+  const int lane = threadIdx.x & 31;
+  const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
+  for (int64_t p = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; p < n_primary; p += nw) {
+    const int64_t s0 = ptr[p], s1 = ptr[p + 1];
+    for (int64_t base = s0; base < s1; base += 32) {
+      const int64_t k = base + lane;
+      int32_t sec = -1;
+      T v = T(0);
+      if (k < s1) {
+        sec = idx[k];
+        v = val[k];
+      }
+      const bool ok = sec >= 0 && (csr ? (int64_t)sec < n_genes : (int64_t)sec < n_cells);
+      const unsigned grp = __match_any_sync(0xffffffffu, ok ? sec : -2 - lane);
+      if (ok && lane == __ffs(grp) - 1) {
+        const int64_t c = csr ? p : (int64_t)sec;
+        const int64_t g = csr ? (int64_t)sec : p;
+        if (!mask[c * n_genes + g]) {
+          dense[c * n_genes + g] = v;
+          mask[c * n_genes + g] = 1;
+        }
+      }
+      __syncwarp();
+    }
+  }
+}
+
+// w = exp(-(d / (bandwidth + 1e-12))^2) per neighbour (impute.hpp:156-159).
+template <class T>
+__global__ void k_knn_weights(const T* __restrict__ dist, int64_t m, T bw, T* __restrict__ w) {
+  for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < m; e += (int64_t)gridDim.x * blockDim.x) {
+    const T scaled = dist[e] / (bw + (T)1e-12);
+    w[e] = exp(-scaled * scaled);
+  }
+}
+
+// impute.hpp:468-508 for one (cell, gene): values above the threshold stay;
+// otherwise the weighted mean of the neighbours that store the gene
+// (sum w v as an fma chain, sum w, neighbours in list order) replaces the
+// value when the weight sum exceeds 1e-12 and the mean exceeds 1e-10.
+template <class T, class IT>
+__global__ void k_knn_impute(T* __restrict__ D, const T* __restrict__ L, const unsigned char* __restrict__ M,
+                             const IT* __restrict__ nbr, const T* __restrict__ w, int64_t n, int64_t G, int K,
+                             T threshold) {
+  const int64_t total = n * G;
+  for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < total; e += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t c = e / G, g = e - c * G;
+    const T x = D[e];
+    if (x > threshold) continue;
+    T sv = T(0), sw = T(0);
+    int found = 0;
+    for (int k = 0; k < K; ++k) {
+      const int64_t j = (int64_t)nbr[c * K + k];
+      if (j < 0 || j >= n || !M[j * G + g]) continue;
+      const T wk = w[c * K + k];
+      sv = fma(wk, L[j * G + g], sv);
+      sw = sw + wk;
+      ++found;
+    }
+    if (found == 0 || !(sw > (T)1e-12)) continue;
+    const T imp = sv / sw;
+    if (imp > (T)1e-10) D[e] = imp;
+  }
+}
+
 // One thread per affinity row: sum its values in stored order (storage
 // precision), then w = a * (1 / sum) for every entry; rows with sum < eps are
 // marked to copy their input row and listed in copy_rows.
@@ -99,6 +171,45 @@ void densify_expression(const CsrView& m, bool csr, int64_t n_cells, int64_t n_g
   else
     k_densify<double><<<grid, 256, 0, s>>>(m.indptr, m.indices, static_cast<const double*>(m.values), n_primary,
                                            n_cells, n_genes, csr ? 1 : 0, static_cast<double*>(dense));
+  SCL_CUDA(cudaGetLastError());
+}
+
+void knn_impute(const CsrView& m, bool csr, int64_t n_cells, int64_t n_genes, const void* nbr, DType it,
+                const void* dist, int K, double bandwidth, double threshold, void* out, cudaStream_t s) {
+  SCL_REQUIRE(m.vtype == kF32 || m.vtype == kF64, kErrTypeMismatch, "expression values must be f32 or f64");
+  densify_expression(m, csr, n_cells, n_genes, out, s);  // the block, later duplicates winning
+  const size_t esz = dtype_size(m.vtype);
+  const int64_t total = n_cells * n_genes;
+  DevBuf L(std::max<int64_t>(total, 1) * esz, s), M(std::max<int64_t>(total, 1), s), W(std::max<int64_t>(n_cells * K, 1) * esz, s);
+  SCL_CUDA(cudaMemsetAsync(M.p, 0, total, s));
+  const int64_t n_primary = std::min<int64_t>(m.n_rows, csr ? n_cells : n_genes);
+  if (n_primary > 0 && m.nnz > 0) {
+    const unsigned gp = grid_for(n_primary * 32);
+    if (m.vtype == kF32)
+      k_densify_first<float><<<gp, 256, 0, s>>>(m.indptr, m.indices, static_cast<const float*>(m.values), n_primary,
+                                                n_cells, n_genes, csr ? 1 : 0, L.as<float>(), M.as<unsigned char>());
+    else
+      k_densify_first<double><<<gp, 256, 0, s>>>(m.indptr, m.indices, static_cast<const double*>(m.values), n_primary,
+                                                 n_cells, n_genes, csr ? 1 : 0, L.as<double>(), M.as<unsigned char>());
+    SCL_CUDA(cudaGetLastError());
+  }
+  const unsigned gw = grid_for(n_cells * K), ge = grid_for(total);
+#define SCL_KNN_IMPUTE(T)                                                                                  \
+  k_knn_weights<T><<<gw, 256, 0, s>>>(static_cast<const T*>(dist), n_cells * K, (T)bandwidth, W.as<T>());  \
+  if (it == kI32)                                                                                          \
+    k_knn_impute<T, int32_t><<<ge, 256, 0, s>>>(static_cast<T*>(out), L.as<T>(), M.as<unsigned char>(),      \
+                                                static_cast<const int32_t*>(nbr), W.as<T>(), n_cells,        \
+                                                n_genes, K, (T)threshold);                                    \
+  else                                                                                                     \
+    k_knn_impute<T, int64_t><<<ge, 256, 0, s>>>(static_cast<T*>(out), L.as<T>(), M.as<unsigned char>(),      \
+                                                static_cast<const int64_t*>(nbr), W.as<T>(), n_cells,        \
+                                                n_genes, K, (T)threshold);
+  if (m.vtype == kF32) {
+    SCL_KNN_IMPUTE(float)
+  } else {
+    SCL_KNN_IMPUTE(double)
+  }
+#undef SCL_KNN_IMPUTE
   SCL_CUDA(cudaGetLastError());
 }
 

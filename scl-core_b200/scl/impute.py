@@ -48,3 +48,20 @@ def spmm(A: CsrMatrix, X: np.ndarray, Y: np.ndarray = None, alpha: float = 1.0, 
     check_error(lib.scl_algebra_spmm(A.handle, X.ctypes.data_as(P), X.shape[1], Y.ctypes.data_as(P), alpha, beta),
                 "algebra_spmm", lib)
     return Y
+
+
+def knn(matrix: CsrMatrix, knn_indices: np.ndarray, knn_distances: np.ndarray, n_cells: int, n_genes: int,
+        bandwidth: float = 1.0, threshold: float = 0.0, weighted: bool = False) -> np.ndarray:
+    """kNN imputation (scl_impute_knn, or scl_impute_knn_weighted, which scl-core
+    runs with the same kernel): values not above `threshold` become the
+    Gaussian-weighted mean of the neighbours that store the gene."""
+    lib = matrix.lib
+    idx = np.ascontiguousarray(knn_indices, dtype=matrix.index_dtype)
+    dist = np.ascontiguousarray(knn_distances, dtype=matrix.real_dtype)
+    out = np.zeros((int(n_cells), int(n_genes)), dtype=matrix.real_dtype)
+    fn = lib.scl_impute_knn_weighted if weighted else lib.scl_impute_knn
+    check_error(fn(matrix.handle, idx.ctypes.data_as(ctypes.POINTER(lib.index_type)),
+                   dist.ctypes.data_as(ctypes.POINTER(lib.real_type)), int(n_cells), int(n_genes), idx.shape[1],
+                   out.ctypes.data_as(ctypes.POINTER(lib.real_type)), bandwidth, threshold),
+                "impute_knn", lib)
+    return out

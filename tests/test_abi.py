@@ -71,7 +71,8 @@ def test_null_and_dimension_errors_match_reference_codes():
     assert lib.scl_get_last_error() == b"Output pseudotime array is null"
     assert lib.scl_diffusion_compute_dpt(m.handle, 0, X.ctypes.data_as(P), 0, 0, 0.0) == 10
     assert lib.scl_diffusion_diffusion_distance(m.handle, X.ctypes.data_as(P), 9, 0) == 10
-    assert lib.scl_impute_knn(m.handle, None, None, 3, 2, 1, X.ctypes.data_as(P), 1.0, 0.0) == 40  # not in this build
+    assert lib.scl_impute_knn(m.handle, None, None, 3, 2, 1, X.ctypes.data_as(P), 1.0, 0.0) == 4
+    assert lib.scl_get_last_error() == b"KNN indices array is null"
     lib.scl_clear_error()
     assert lib.scl_get_last_error() == b"No error" and lib.scl_get_last_error_code() == 0
 

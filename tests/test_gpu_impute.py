@@ -127,4 +127,48 @@ def test_errors_follow_the_reference_convention():
     assert lib.scl_impute_diffusion(M.handle, G.handle, 0, 2, 1, P) == 10
     assert lib.scl_impute_magic(M.handle, G.handle, 2, 2, 0, P) == 10
     assert lib.scl_impute_diffusion(M.handle, G.handle, 3, 2, 1, P) == 11  # graph has 2 cells
-    assert lib.scl_impute_knn(M.handle, None, None, 2, 2, 1, P, 1.0, 0.0) == 40  # not implemented
+    assert lib.scl_impute_knn(M.handle, None, None, 2, 2, 1, P, 1.0, 0.0) == 4
+
+
+@pytest.mark.parametrize("dt,idt,rtol", [(np.float32, np.int32, 2e-6), (np.float64, np.int64, 1e-14)])
+@pytest.mark.parametrize("csr", [True, False])
+def test_knn_impute_matches_reference(dt, idt, rtol, csr):
+    """scl_impute_knn (and scl_impute_knn_weighted, the same kernel in
+    scl-core) against scl-core's own build: the positions imputed are the
+    same and the values agree to rounding (the Gaussian weights come from
+    CUDA's exp, the reference's from the C library's)."""
+    if not ref.available("f32_i32" if dt == np.float32 else "f64_i64"):
+        pytest.skip("reference library not shipped with the tests")
+    R = ref.RefLib("f32_i32" if dt == np.float32 else "f64_i64")
+    rng = np.random.default_rng(13)
+    n_cells, n_genes, K = 400, 60, 8
+    X = sp.random(n_cells, n_genes, density=0.3, random_state=3, format="csr", dtype=np.float64).astype(dt)
+    X.sort_indices()
+    X.data[::11] = 0  # stored zeros still count as expressed
+    nbr = rng.integers(0, n_cells, size=(n_cells, K)).astype(np.int64)
+    nbr[::17, 0] = n_cells + 3  # out-of-range neighbours are ignored
+    dist = rng.random((n_cells, K)).astype(dt)
+    if csr:
+        x = (X.indptr.astype(np.int64), X.indices.astype(np.int64), X.data)
+        shape = X.shape
+        M = _wrap(x, shape, idt)
+    else:
+        C = X.tocsc()
+        C.sort_indices()
+        x = (C.indptr.astype(np.int64), C.indices.astype(np.int64), C.data)
+        shape = X.shape
+        import ctypes
+
+        lib = scl.get_library("f32_i32" if dt == np.float32 else "f64_i64")
+        arrs = [np.ascontiguousarray(x[0], idt), np.ascontiguousarray(x[1], idt), np.ascontiguousarray(x[2], dt)]
+        h = ctypes.c_void_p()
+        ptr = lambda a, t: a.ctypes.data_as(ctypes.POINTER(t))
+        assert lib.scl_sparse_wrap(ctypes.byref(h), n_cells, n_genes, arrs[2].size, ptr(arrs[0], lib.index_type),
+                                   ptr(arrs[1], lib.index_type), ptr(arrs[2], lib.real_type), 0) == 0
+        M = scl.CsrMatrix(h, lib, scl.core.sparse.OwnershipMode.WRAPPED, data_refs=arrs, is_csr=False)
+    for bw, thr in ((1.0, 0.0), (0.3, 0.05)):
+        want = R.impute_knn(x, shape, csr, nbr, dist, n_cells, n_genes, bw, thr)
+        for weighted in (False, True):
+            got = scl.impute.knn(M, nbr, dist, n_cells, n_genes, bw, thr, weighted=weighted)
+            np.testing.assert_array_equal(got == 0, want == 0)
+            np.testing.assert_allclose(got, want, rtol=rtol, atol=0)

@@ -18,6 +18,7 @@
 #include <algorithm>
 #include <cmath>
 #include <limits>
+#include <type_traits>
 
 #include "engine.hpp"
 
@@ -32,14 +33,19 @@ __device__ __forceinline__ double kfma(double a, double b, double c) { return __
 __device__ __forceinline__ float ksqrt(float a) { return __fsqrt_rn(a); }
 __device__ __forceinline__ double ksqrt(double a) { return __dsqrt_rn(a); }
 
-template <class T, class IT, int NT, int KMAX>
+// DR > 0 (16 or 32 features at most): the query row is held in DR registers
+// (features zero-padded to DR, which leaves every fma chain unchanged) and the
+// candidate rows are staged with pitch DR, read 16 bytes per load; DR == 0:
+// queries in shared memory, any d up to 128 (a 64-register query spilled and
+// ran slower than this path at 50 features).
+template <class T, class IT, int NT, int KMAX, int DR>
 __global__ void __launch_bounds__(NT)
 k_knn_dense(const T* __restrict__ X, const T* __restrict__ norms, const T* __restrict__ snorms, int64_t n, int d,
             int k, IT* __restrict__ out_idx, T* __restrict__ out_dist) {
   extern __shared__ __align__(16) unsigned char knn_smem[];
-  const int dp = d + 1;
-  T* Qs = reinterpret_cast<T*>(knn_smem);                          // [d][NT]
-  T* Cs = Qs + (size_t)d * NT;                                     // [kKnnTile][dp]
+  const int dp = DR > 0 ? DR : d + 1;
+  T* Qs = reinterpret_cast<T*>(knn_smem);                          // [d][NT] (DR == 0)
+  T* Cs = Qs + (DR > 0 ? 0 : (size_t)d * NT);                      // [kKnnTile][dp]
   T* Hd = Cs + (size_t)kKnnTile * dp;                              // [KMAX][NT]
   int32_t* Hj = reinterpret_cast<int32_t*>(Hd + (size_t)KMAX * NT);  // [KMAX][NT]
   const int tid = threadIdx.x;
@@ -47,9 +53,15 @@ k_knn_dense(const T* __restrict__ X, const T* __restrict__ norms, const T* __res
   const bool live = i < n;
   const int64_t q0 = (int64_t)blockIdx.x * NT;
   const int nq = (n - q0) < (int64_t)NT ? (int)(n - q0) : NT;
-  for (int e = tid; e < nq * d; e += NT) {  // queries, column-major
-    const int r = e / d, f = e - r * d;
-    Qs[f * NT + r] = X[(q0 + r) * (int64_t)d + f];
+  T qr[DR > 0 ? DR : 1];
+  if constexpr (DR > 0) {
+#pragma unroll
+    for (int f = 0; f < DR; ++f) qr[f] = (live && f < d) ? X[i * (int64_t)d + f] : T(0);
+  } else {
+    for (int e = tid; e < nq * d; e += NT) {  // queries, column-major
+      const int r = e / d, f = e - r * d;
+      Qs[f * NT + r] = X[(q0 + r) * (int64_t)d + f];
+    }
   }
   const T ni = live ? norms[i] : T(0);
   const T si = live ? snorms[i] : T(0);
@@ -68,20 +80,48 @@ k_knn_dense(const T* __restrict__ X, const T* __restrict__ norms, const T* __res
   for (int64_t t0 = 0; t0 < n; t0 += kKnnTile) {
     const int tn = (n - t0) < (int64_t)kKnnTile ? (int)(n - t0) : kKnnTile;
     __syncthreads();  // the previous tile is consumed (and the queries are staged)
-    for (int e = tid; e < tn * d; e += NT) {
-      const int r = e / d, f = e - r * d;
-      Cs[r * dp + f] = X[(t0 + r) * (int64_t)d + f];
+    if constexpr (DR > 0) {
+      for (int e = tid; e < kKnnTile * DR; e += NT) {  // rows past the tile and features past d are zero
+        const int r = e / DR, f = e - r * DR;
+        Cs[e] = (r < tn && f < d) ? X[(t0 + r) * (int64_t)d + f] : T(0);
+      }
+    } else {
+      for (int e = tid; e < tn * d; e += NT) {
+        const int r = e / d, f = e - r * d;
+        Cs[r * dp + f] = X[(t0 + r) * (int64_t)d + f];
+      }
     }
     __syncthreads();
     if (!live) continue;
     for (int c0 = 0; c0 < tn; c0 += 4) {
       T dot[4] = {T(0), T(0), T(0), T(0)};
       const int cl = (tn - c0) < 4 ? (tn - c0) : 4;
-      for (int f = 0; f < d; ++f) {
-        const T a = Qs[f * NT + tid];
+      if constexpr (DR > 0) {
+        using V4 = typename std::conditional<sizeof(T) == 4, float4, double2>::type;
+        constexpr int PER = 16 / (int)sizeof(T);  // values per 16-byte load
 #pragma unroll
-        for (int u = 0; u < 4; ++u)
-          if (u < cl) dot[u] = kfma(a, Cs[(c0 + u) * dp + f], dot[u]);
+        for (int f = 0; f < DR; f += PER) {
+#pragma unroll
+          for (int u = 0; u < 4; ++u) {
+            const V4 v = *reinterpret_cast<const V4*>(Cs + (c0 + u) * DR + f);
+            if constexpr (sizeof(T) == 4) {
+              dot[u] = kfma(qr[f], v.x, dot[u]);
+              dot[u] = kfma(qr[f + 1], v.y, dot[u]);
+              dot[u] = kfma(qr[f + 2], v.z, dot[u]);
+              dot[u] = kfma(qr[f + 3], v.w, dot[u]);
+            } else {
+              dot[u] = kfma(qr[f], v.x, dot[u]);
+              dot[u] = kfma(qr[f + 1], v.y, dot[u]);
+            }
+          }
+        }
+      } else {
+        for (int f = 0; f < d; ++f) {
+          const T a = Qs[f * NT + tid];
+#pragma unroll
+          for (int u = 0; u < 4; ++u)
+            if (u < cl) dot[u] = kfma(a, Cs[(c0 + u) * dp + f], dot[u]);
+        }
       }
 #pragma unroll
       for (int u = 0; u < 4; ++u) {
@@ -165,12 +205,13 @@ __global__ void k_row_norms(const T* __restrict__ X, int64_t n, int d, T* __rest
   }
 }
 
-template <class T, class IT, int NT, int KMAX>
+template <class T, class IT, int NT, int KMAX, int DR>
 void launch_knn(const T* X, const T* norms, const T* snorms, int64_t n, int d, int k, IT* idx, T* dist,
                 cudaStream_t s) {
-  const size_t smem = (size_t)d * NT * sizeof(T) + (size_t)kKnnTile * (d + 1) * sizeof(T) +
+  const size_t smem = (DR > 0 ? (size_t)kKnnTile * DR * sizeof(T)
+                              : (size_t)d * NT * sizeof(T) + (size_t)kKnnTile * (d + 1) * sizeof(T)) +
                       (size_t)KMAX * NT * (sizeof(T) + sizeof(int32_t));
-  auto kern = k_knn_dense<T, IT, NT, KMAX>;
+  auto kern = k_knn_dense<T, IT, NT, KMAX, DR>;
   SCL_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   const int64_t grid = (n + NT - 1) / NT;
   kern<<<(unsigned)grid, NT, smem, s>>>(X, norms, snorms, n, d, k, idx, dist);
@@ -186,8 +227,14 @@ void knn_typed(const T* X, const T* norms, int64_t n, int d, int k, IT* idx, T* 
               s>>>(norms, n, sn.as<T>());
   SCL_CUDA(cudaGetLastError());
   constexpr int NT = sizeof(T) == 4 ? 128 : 64;
-  if (k <= 32) return launch_knn<T, IT, NT, 32>(X, norms, sn.as<T>(), n, d, k, idx, dist, s);
-  return launch_knn<T, IT, NT, 64>(X, norms, sn.as<T>(), n, d, k, idx, dist, s);
+  const T* sp = sn.as<T>();
+  if (k <= 32) {
+    if (d <= 16) return launch_knn<T, IT, NT, 32, 16>(X, norms, sp, n, d, k, idx, dist, s);
+    if (d <= 32) return launch_knn<T, IT, NT, 32, 32>(X, norms, sp, n, d, k, idx, dist, s);
+    return launch_knn<T, IT, NT, 32, 0>(X, norms, sp, n, d, k, idx, dist, s);
+  }
+  if (d <= 32) return launch_knn<T, IT, NT, 64, 32>(X, norms, sp, n, d, k, idx, dist, s);
+  return launch_knn<T, IT, NT, 64, 0>(X, norms, sp, n, d, k, idx, dist, s);
 }
 
 }  // namespace

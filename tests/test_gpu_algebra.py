@@ -25,7 +25,7 @@ def test_algebra_spmm_bit_exact(dt, idt, m, kdim, K):
     X = rng.standard_normal((kdim, K)).astype(dt)
     for alpha, beta in ((1.0, 0.0), (0.5, 2.0), (2.0, 1.0), (0.0, 3.0), (-1.5, 0.25)):
         Y0 = rng.standard_normal((m, K)).astype(dt)
-        got = scl.impute.spmm(M, X, Y0.copy(), alpha, beta)
+        got = scl.algebra.spmm(M, X, Y0.copy(), alpha, beta)
         np.testing.assert_array_equal(bits(got), bits(port.algebra_spmm(A.indptr, A.indices, A.data, X, Y0,
                                                                          dt(alpha), dt(beta))))
 

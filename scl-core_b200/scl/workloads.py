@@ -46,7 +46,7 @@ def _main():
     import torch
 
     ap = argparse.ArgumentParser()
-    ap.add_argument("case", choices=["spmm", "backward"])
+    ap.add_argument("case", choices=["spmm", "backward", "knn", "ppr"])
     ap.add_argument("--every", type=int, default=4)
     ap.add_argument("--cells", type=int, default=200_000)
     ap.add_argument("--k", type=int, default=30)
@@ -56,6 +56,33 @@ def _main():
     ap.add_argument("--no-reorder", action="store_true")
     ap.add_argument("--plan", default="", help="group,vec,kind,stage launch shape for diffuse (default: built-in)")
     a = ap.parse_args()
+    if a.case == "knn":  # brute-force kNN of the mixture through scl_knn (host buffers)
+        import numpy as np
+
+        from . import neighbors, synthetic
+        from .core.sparse import CsrMatrix
+
+        pts = synthetic.mixture(a.cells, seed=21).astype(np.float32)[:, : a.features]
+        pts = np.ascontiguousarray(pts)
+        n, d = pts.shape
+        m = CsrMatrix.wrap(np.arange(0, (n + 1) * d, d, dtype=np.int32), np.tile(np.arange(d, dtype=np.int32), n),
+                           pts.reshape(-1), (n, d))
+        norms = neighbors.compute_norms(m)
+        for _ in range(max(a.steps, 1)):
+            idx, dist = neighbors.knn(m, a.k, norms)
+        print(f"cells={n} features={d} k={a.k} checksum={float(dist[np.isfinite(dist)].sum()):.6e}")
+        return
+    if a.case == "ppr":  # personalized PageRank from cell 0 on the row-normalised graph
+        from . import diffusion
+        from .core.sparse import CsrMatrix
+
+        g, _, _, tm = build_graph(a.cells, a.k, reorder=False)
+        ip, ind, P = g.export()
+        m = CsrMatrix.wrap(ip.astype("int32"), ind.astype("int32"), P, (a.cells, a.cells))
+        for _ in range(max(a.steps, 1)):
+            pr = diffusion.personalized_pagerank(m, 0)
+        print(f"cells={a.cells} nnz={ind.size} checksum={float(pr.sum()):.6e}")
+        return
     if a.case == "backward":
         g, _, _, tm = build_graph(a.cells, a.k, reorder=False)
         gen = torch.Generator(device="cuda").manual_seed(7)

@@ -30,7 +30,8 @@ def _matrix(n, d, dt, idt, dens=1.0, seed=0, quantised=False):
 @pytest.mark.parametrize("n,d,k,dens,quant", [(1, 3, 4, 1.0, False), (12, 5, 15, 1.0, False),
                                               (300, 20, 10, 1.0, False), (700, 50, 30, 1.0, False),
                                               (400, 60, 12, 0.3, False), (500, 8, 6, 1.0, True),
-                                              (2000, 128, 64, 1.0, False), (129, 1, 3, 1.0, True)])
+                                              (2000, 128, 64, 1.0, False), (129, 1, 3, 1.0, True),
+                                              (3000, 33, 40, 1.0, True)])
 def test_knn_bit_exact(dt, idt, n, d, k, dens, quant):
     m, X = _matrix(n, d, dt, idt, dens, seed=n + d, quantised=quant)
     Xd = X.toarray()

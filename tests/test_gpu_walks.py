@@ -30,7 +30,7 @@ def _graph(n, dt, idt, seed=3, density=0.03, empty=()):
 
 
 @pytest.mark.parametrize("dt,idt", VARIANTS)
-@pytest.mark.parametrize("n", [1, 7, 300, 20000])
+@pytest.mark.parametrize("n", [1, 7, 300, 1500, 20000])
 def test_lazy_walk_and_heat_kernel_bit_exact(dt, idt, n):
     m, (ip, ind, v) = _graph(n, dt, idt, density=12.0 / n, empty=(0,) if n > 5 else ())
     x0 = np.random.default_rng(n).random(n).astype(dt)
@@ -47,7 +47,7 @@ def test_lazy_walk_and_heat_kernel_bit_exact(dt, idt, n):
 
 
 @pytest.mark.parametrize("dt,idt", VARIANTS)
-@pytest.mark.parametrize("n", [5, 500, 20000])
+@pytest.mark.parametrize("n", [5, 500, 1500, 20000])
 def test_restart_walk_and_pagerank_bit_exact(dt, idt, n):
     m, (ip, ind, v) = _graph(n, dt, idt, seed=5, density=10.0 / n)
     for seeds in ([0, 3, 3, n + 4, -1], [n - 1]):

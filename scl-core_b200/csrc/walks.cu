@@ -10,7 +10,13 @@
 //   lazy / heat kernel:  y_i = fma(c_x, x_i, c_p * (P x)_i)
 //   restart:             y_i = fma(c_p, (P x)_i, c_r * r_i)
 // and, for the restart walk, the L1 change sum |y_i - x_i| (differences in
-// the storage precision, summed in FP64) for the convergence test.
+// the storage precision, summed in FP64) for the convergence test. The
+// restart walk decides convergence on the device: every block stores its
+// partial sum, the last block to finish adds the partials in block order (a
+// fixed order, so the sum is deterministic) and, below tol, records the step
+// and raises a flag that makes the later steps' launches return at once. The
+// host queues steps in chunks and reads the flag once per chunk instead of
+// once per step.
 // Diffusion pseudotime keeps a thread per row and the sequential fma chain in
 // stored order.
 #include <algorithm>
@@ -26,12 +32,25 @@ __device__ __forceinline__ double wfma(double a, double b, double c) { return __
 __device__ __forceinline__ float wmul(float a, float b) { return __fmul_rn(a, b); }
 __device__ __forceinline__ double wmul(double a, double b) { return __dmul_rn(a, b); }
 
+// Convergence state of a restart walk, in device memory.
+struct WalkCtl {
+  unsigned int arrived;  // blocks of the current step that have stored their partial sum
+  int done;              // set by the step whose L1 change fell below tol
+  long long step;        // that step's index
+};
+
 template <class T, bool RESTART>
 __global__ void __launch_bounds__(256)
 k_walk_step(const int64_t* __restrict__ ptr, const int32_t* __restrict__ idx, const T* __restrict__ val, int64_t n,
-            const T* __restrict__ x, const T* __restrict__ r, T c1, T c2, T* __restrict__ y,
-            double* __restrict__ l1) {
+            const T* __restrict__ x, const T* __restrict__ r, T c1, T c2, T* __restrict__ y, WalkCtl* ctl,
+            double* __restrict__ partials, long long step, double tol) {
   __shared__ double part[8];
+  __shared__ bool last;
+  if constexpr (RESTART) {
+    // a converged walk's later steps do nothing (the flag only changes after
+    // every block of the converging step has passed this point)
+    if (*reinterpret_cast<volatile int*>(&ctl->done)) return;
+  }
   const int lane = threadIdx.x & 31;
   const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
   double d = 0.0;
@@ -59,7 +78,24 @@ k_walk_step(const int64_t* __restrict__ ptr, const int32_t* __restrict__ idx, co
     if (threadIdx.x == 0) {
       double t = 0.0;
       for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t += part[w];
-      atomicAdd(l1, t);
+      partials[blockIdx.x] = t;
+      __threadfence();
+      last = atomicAdd(&ctl->arrived, 1u) == gridDim.x - 1;
+    }
+    __syncthreads();
+    if (last && threadIdx.x < 32) {
+      __threadfence();
+      double t = 0.0;
+      for (unsigned b = lane; b < gridDim.x; b += 32) t += __ldcg(partials + b);
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) t += __shfl_xor_sync(0xffffffffu, t, o);
+      if (lane == 0) {
+        if (t < tol) {
+          ctl->step = step;
+          ctl->done = 1;
+        }
+        ctl->arrived = 0;
+      }
     }
   }
 }
@@ -166,7 +202,7 @@ void walk_linear_typed(const CsrView& P, T* x, int64_t steps, T c_x, T c_p, cuda
   T* out = tmp.as<T>();
   for (int64_t st = 0; st < steps; ++st) {
     k_walk_step<T, false><<<warp_row_grid(n), 256, 0, s>>>(P.indptr, P.indices, static_cast<const T*>(P.values), n, in,
-                                                        nullptr, c_x, c_p, out, nullptr);
+                                                        nullptr, c_x, c_p, out, nullptr, nullptr, 0, 0.0);
     SCL_CUDA(cudaGetLastError());
     std::swap(in, out);
   }
@@ -177,35 +213,35 @@ template <class T>
 int64_t walk_restart_typed(const CsrView& P, const T* r, T* scores, T alpha, int64_t max_iter, T tol,
                            cudaStream_t s) {
   const int64_t n = P.n_rows;
+  const unsigned grid = warp_row_grid(n);
   DevBuf other(std::max<int64_t>(n, 1) * sizeof(T), s);
-  DevBuf l1(sizeof(double), s);
-  double* host_l1 = nullptr;
-  SCL_CUDA(cudaMallocHost(&host_l1, sizeof(double)));
-  struct Free {
-    double* p;
-    ~Free() { cudaFreeHost(p); }
-  } guard{host_l1};
+  DevBuf ctl(sizeof(WalkCtl), s), partials(grid * sizeof(double), s);
+  SCL_CUDA(cudaMemsetAsync(ctl.p, 0, sizeof(WalkCtl), s));
+  WalkCtl host{};  // read back once per chunk (a few bytes: pageable memory, no pinned allocation per call)
   const T beta = T(1) - alpha;
   // scores holds the restart vector; the two buffers swap roles after every
-  // step that has not converged, so the caller's buffer ends up holding the
-  // last iterate written into it (the reference's pointer swap)
-  T* cur = scores;
-  T* nxt = other.as<T>();
-  int64_t it = 0;
-  for (; it < max_iter; ++it) {
-    SCL_CUDA(cudaMemsetAsync(l1.p, 0, sizeof(double), s));
-    k_walk_step<T, true><<<warp_row_grid(n), 256, 0, s>>>(P.indptr, P.indices, static_cast<const T*>(P.values), n, cur,
-                                                       r, alpha, beta, nxt, l1.as<double>());
-    SCL_CUDA(cudaGetLastError());
-    SCL_CUDA(cudaMemcpyAsync(host_l1, l1.p, sizeof(double), cudaMemcpyDeviceToHost, s));
+  // step that has not converged, so step `it` reads from scores when `it` is
+  // even and the caller's buffer ends up holding the last iterate written
+  // into it (the reference's pointer swap)
+  T* bufs[2] = {scores, other.as<T>()};
+  constexpr int64_t kChunk = 8;  // steps queued between reads of the flag
+  for (int64_t c0 = 0; c0 < max_iter; c0 += kChunk) {
+    const int64_t c1 = std::min<int64_t>(max_iter, c0 + kChunk);
+    for (int64_t it = c0; it < c1; ++it) {
+      k_walk_step<T, true><<<grid, 256, 0, s>>>(P.indptr, P.indices, static_cast<const T*>(P.values), n,
+                                                bufs[it & 1], r, alpha, beta, bufs[(it + 1) & 1],
+                                                ctl.as<WalkCtl>(), partials.as<double>(), (long long)it, (double)tol);
+      SCL_CUDA(cudaGetLastError());
+    }
+    SCL_CUDA(cudaMemcpyAsync(&host, ctl.p, sizeof(WalkCtl), cudaMemcpyDeviceToHost, s));
     SCL_CUDA(cudaStreamSynchronize(s));
-    if (*host_l1 < (double)tol) {
-      SCL_CUDA(cudaMemcpyAsync(cur, nxt, n * sizeof(T), cudaMemcpyDeviceToDevice, s));
+    if (host.done) {
+      const int64_t it = host.step;  // the converged step wrote bufs[(it + 1) & 1]; it lands in bufs[it & 1]
+      SCL_CUDA(cudaMemcpyAsync(bufs[it & 1], bufs[(it + 1) & 1], n * sizeof(T), cudaMemcpyDeviceToDevice, s));
       return it + 1;
     }
-    std::swap(cur, nxt);
   }
-  return it;
+  return max_iter;
 }
 
 template <class T>
@@ -219,12 +255,7 @@ void dpt_typed(const CsrView& P, int64_t root, T* out, int64_t max_iter, T tol, 
   const T one = T(1);
   SCL_CUDA(cudaMemcpyAsync(pa.as<T>() + root, &one, sizeof(T), cudaMemcpyHostToDevice, s));
   SCL_CUDA(cudaMemcpyAsync(vis.as<T>() + root, &one, sizeof(T), cudaMemcpyHostToDevice, s));
-  unsigned long long* hw = nullptr;
-  SCL_CUDA(cudaMallocHost(&hw, sizeof(unsigned long long)));
-  struct Free {
-    unsigned long long* p;
-    ~Free() { cudaFreeHost(p); }
-  } guard{hw};
+  unsigned long long hw = 0;  // the max-reduced word, read back each step (pageable: 8 bytes)
   T* p = pa.as<T>();
   T* q = pb.as<T>();
   for (int64_t it = 1; it <= max_iter; ++it) {
@@ -233,17 +264,17 @@ void dpt_typed(const CsrView& P, int64_t root, T* out, int64_t max_iter, T tol, 
                                                 hit.as<T>(), vis.as<T>(), static_cast<T>(it),
                                                 word.as<unsigned long long>());
     SCL_CUDA(cudaGetLastError());
-    SCL_CUDA(cudaMemcpyAsync(hw, word.p, sizeof(unsigned long long), cudaMemcpyDeviceToHost, s));
+    SCL_CUDA(cudaMemcpyAsync(&hw, word.p, sizeof(unsigned long long), cudaMemcpyDeviceToHost, s));
     SCL_CUDA(cudaStreamSynchronize(s));
-    if (from_bits<T>(*hw) < tol) break;
+    if (from_bits<T>(hw) < tol) break;
     std::swap(p, q);
   }
   SCL_CUDA(cudaMemsetAsync(word.p, 0, sizeof(unsigned long long), s));
   k_dpt_scale<T><<<walk_grid(n), 256, 0, s>>>(n, hit.as<T>(), vis.as<T>(), word.as<unsigned long long>());
   SCL_CUDA(cudaGetLastError());
-  SCL_CUDA(cudaMemcpyAsync(hw, word.p, sizeof(unsigned long long), cudaMemcpyDeviceToHost, s));
+  SCL_CUDA(cudaMemcpyAsync(&hw, word.p, sizeof(unsigned long long), cudaMemcpyDeviceToHost, s));
   SCL_CUDA(cudaStreamSynchronize(s));
-  const T max_time = from_bits<T>(*hw);
+  const T max_time = from_bits<T>(hw);
   const T inv_max = (max_time > T(0)) ? T(1) / max_time : T(1);
   k_dpt_output<T><<<walk_grid(n), 256, 0, s>>>(n, hit.as<T>(), vis.as<T>(), inv_max, out);
   SCL_CUDA(cudaGetLastError());

@@ -17,8 +17,9 @@
 // and raises a flag that makes the later steps' launches return at once. The
 // host queues steps in chunks and reads the flag once per chunk instead of
 // once per step.
-// Diffusion pseudotime keeps a thread per row and the sequential fma chain in
-// stored order.
+// Diffusion pseudotime keeps one sequential fma chain per row in stored order
+// (a lane per row over entries staged by its warp) and also decides
+// convergence on the device.
 #include <algorithm>
 #include <cstring>
 
@@ -108,6 +109,9 @@ __device__ __forceinline__ void max_nonneg(float v, unsigned long long* word) {
 __device__ __forceinline__ void max_nonneg(double v, unsigned long long* word) {
   atomicMax(word, (unsigned long long)__double_as_longlong(v));
 }
+template <class T> __device__ T from_bits_dev(unsigned long long w);
+template <> __device__ float from_bits_dev<float>(unsigned long long w) { return __uint_as_float((unsigned int)w); }
+template <> __device__ double from_bits_dev<double>(unsigned long long w) { return __longlong_as_double((long long)w); }
 template <class T> T from_bits(unsigned long long w);
 template <> float from_bits<float>(unsigned long long w) {
   const unsigned int u = (unsigned int)w;
@@ -125,28 +129,89 @@ template <> double from_bits<double>(unsigned long long w) {
 // rows not yet (almost) visited the hitting time and visit probability grow by
 // the newly arriving mass; the largest unvisited probability 1 - visited is
 // max-reduced for the convergence test.
+// Convergence state of a DPT walk, in device memory.
+struct DptCtl {
+  unsigned int arrived;  // blocks of the current step that have max-reduced their rows
+  int done;              // set by the step whose largest unvisited probability fell below tol
+};
+
+constexpr int kDptWarps = 4;  // warps per block
 template <class T>
-__global__ void __launch_bounds__(256)
+constexpr int kDptStage = 4096 / (int)sizeof(T);  // entries a warp stages per round
+
+// A warp owns 32 consecutive rows and stages their entries (the values and
+// the gathered p values), read coalesced, in shared memory; then each lane
+// runs its own row's sequential fma chain in stored order from there, so the
+// sums are the ones a thread walking its row in global memory would form.
+// Rows whose entries exceed one staging round continue in the next round
+// with the partial sum kept. The largest unvisited probability is
+// max-reduced per block into one word (one atomic per block); the last block
+// of the step compares it with tol, raises the done flag (the later steps'
+// launches then return at once) and clears the word for the next step.
+template <class T>
+__global__ void __launch_bounds__(kDptWarps * 32)
 k_dpt_step(const int64_t* __restrict__ ptr, const int32_t* __restrict__ idx, const T* __restrict__ val, int64_t n,
            const T* __restrict__ p, T* __restrict__ p_new, T* __restrict__ hit, T* __restrict__ vis, T step,
-           unsigned long long* __restrict__ max_unvisited) {
+           unsigned long long* __restrict__ max_unvisited, DptCtl* ctl, T tol) {
+  if (*reinterpret_cast<volatile int*>(&ctl->done)) return;
+  __shared__ T sv[kDptWarps][kDptStage<T>];
+  __shared__ T sp[kDptWarps][kDptStage<T>];
+  __shared__ T part[kDptWarps];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   T m = T(0);
-  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+  const int64_t groups = (n + 31) / 32;
+  for (int64_t g = (int64_t)blockIdx.x * kDptWarps + w; g < groups; g += (int64_t)gridDim.x * kDptWarps) {
+    const int64_t r0 = g * 32;
+    const int64_t i = r0 + lane;
+    const bool live = i < n;
+    const int64_t rb = live ? ptr[i] : 0, re = live ? ptr[i + 1] : 0;
+    const int64_t b = ptr[r0], e = ptr[(r0 + 32) < n ? r0 + 32 : n];
     T s = T(0);
-    for (int64_t k = ptr[i], e = ptr[i + 1]; k < e; ++k) s = wfma(val[k], p[idx[k]], s);
-    p_new[i] = s;
-    T v = vis[i];
-    if (v < T(0.99) && s > T(1e-15)) {
-      const T np = wmul(s, T(1) - v);
-      hit[i] = wfma(step, np, hit[i]);
-      v = v + np;
-      v = v < T(1) ? v : T(1);
-      vis[i] = v;
+    for (int64_t c0 = b; c0 < e; c0 += kDptStage<T>) {
+      const int cn = (e - c0) < (int64_t)kDptStage<T> ? (int)(e - c0) : kDptStage<T>;
+#pragma unroll 4
+      for (int j = lane; j < cn; j += 32) {
+        sv[w][j] = val[c0 + j];
+        sp[w][j] = p[idx[c0 + j]];
+      }
+      __syncwarp();
+      const int64_t lo = rb > c0 ? rb : c0, hi = re < c0 + cn ? re : c0 + cn;
+      for (int64_t k = lo; k < hi; ++k) s = wfma(sv[w][k - c0], sp[w][k - c0], s);
+      __syncwarp();
     }
-    const T u = T(1) - v;
-    m = u > m ? u : m;
+    if (live) {
+      p_new[i] = s;
+      T v = vis[i];
+      if (v < T(0.99) && s > T(1e-15)) {
+        const T np = wmul(s, T(1) - v);
+        hit[i] = wfma(step, np, hit[i]);
+        v = v + np;
+        v = v < T(1) ? v : T(1);
+        vis[i] = v;
+      }
+      const T u = T(1) - v;
+      m = u > m ? u : m;
+    }
   }
-  max_nonneg(m, max_unvisited);
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    const T x = __shfl_xor_sync(0xffffffffu, m, o);
+    m = x > m ? x : m;
+  }
+  if (lane == 0) part[w] = m;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int k = 1; k < kDptWarps; ++k) m = part[k] > m ? part[k] : m;
+    max_nonneg(m, max_unvisited);
+    __threadfence();
+    if (atomicAdd(&ctl->arrived, 1u) == gridDim.x - 1) {
+      __threadfence();
+      const T mx = from_bits_dev<T>(atomicAdd(max_unvisited, 0ull));
+      if (mx < tol) ctl->done = 1;
+      *max_unvisited = 0ull;
+      ctl->arrived = 0;
+    }
+  }
 }
 
 // hitting time / visit probability on the visited rows (> 0.5), max-reduced
@@ -255,19 +320,30 @@ void dpt_typed(const CsrView& P, int64_t root, T* out, int64_t max_iter, T tol, 
   const T one = T(1);
   SCL_CUDA(cudaMemcpyAsync(pa.as<T>() + root, &one, sizeof(T), cudaMemcpyHostToDevice, s));
   SCL_CUDA(cudaMemcpyAsync(vis.as<T>() + root, &one, sizeof(T), cudaMemcpyHostToDevice, s));
-  unsigned long long hw = 0;  // the max-reduced word, read back each step (pageable: 8 bytes)
-  T* p = pa.as<T>();
-  T* q = pb.as<T>();
-  for (int64_t it = 1; it <= max_iter; ++it) {
-    SCL_CUDA(cudaMemsetAsync(word.p, 0, sizeof(unsigned long long), s));
-    k_dpt_step<T><<<walk_grid(n), 256, 0, s>>>(P.indptr, P.indices, static_cast<const T*>(P.values), n, p, q,
-                                                hit.as<T>(), vis.as<T>(), static_cast<T>(it),
-                                                word.as<unsigned long long>());
-    SCL_CUDA(cudaGetLastError());
-    SCL_CUDA(cudaMemcpyAsync(&hw, word.p, sizeof(unsigned long long), cudaMemcpyDeviceToHost, s));
+  unsigned long long hw = 0;  // the max-reduced hitting time, read back once (pageable: 8 bytes)
+  DevBuf ctl(sizeof(DptCtl), s);
+  SCL_CUDA(cudaMemsetAsync(ctl.p, 0, sizeof(DptCtl), s));
+  SCL_CUDA(cudaMemsetAsync(word.p, 0, sizeof(unsigned long long), s));
+  T* bufs[2] = {pa.as<T>(), pb.as<T>()};  // step it reads bufs[(it + 1) & 1] and writes the other one
+  int dev = 0;
+  SCL_CUDA(cudaGetDevice(&dev));
+  const int64_t groups = (n + 31) / 32;
+  const unsigned grid = (unsigned)std::max<int64_t>(
+      1, std::min<int64_t>((groups + kDptWarps - 1) / kDptWarps, (int64_t)sm_count(dev) * 12));
+  constexpr int64_t kChunk = 8;  // steps queued between reads of the flag
+  DptCtl host{};
+  for (int64_t c0 = 1; c0 <= max_iter; c0 += kChunk) {
+    const int64_t c1 = std::min<int64_t>(max_iter, c0 + kChunk - 1);
+    for (int64_t it = c0; it <= c1; ++it) {
+      k_dpt_step<T><<<grid, kDptWarps * 32, 0, s>>>(P.indptr, P.indices, static_cast<const T*>(P.values), n,
+                                                    bufs[(it + 1) & 1], bufs[it & 1], hit.as<T>(), vis.as<T>(),
+                                                    static_cast<T>(it), word.as<unsigned long long>(),
+                                                    ctl.as<DptCtl>(), tol);
+      SCL_CUDA(cudaGetLastError());
+    }
+    SCL_CUDA(cudaMemcpyAsync(&host, ctl.p, sizeof(DptCtl), cudaMemcpyDeviceToHost, s));
     SCL_CUDA(cudaStreamSynchronize(s));
-    if (from_bits<T>(hw) < tol) break;
-    std::swap(p, q);
+    if (host.done) break;
   }
   SCL_CUDA(cudaMemsetAsync(word.p, 0, sizeof(unsigned long long), s));
   k_dpt_scale<T><<<walk_grid(n), 256, 0, s>>>(n, hit.as<T>(), vis.as<T>(), word.as<unsigned long long>());

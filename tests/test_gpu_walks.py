@@ -92,6 +92,17 @@ def test_longer_output_buffers_keep_their_tail_and_errors_follow_the_reference()
 
 
 @pytest.mark.parametrize("dt,idt", VARIANTS)
+def test_pseudotime_long_rows_bit_exact(dt, idt):
+    """Rows far longer than one staging round of the DPT step (and 32-row
+    groups holding many rounds), next to empty rows."""
+    n = 3000
+    m, (ip, ind, v) = _graph(n, dt, idt, seed=12, density=0.4, empty=(5, 6, 2999))
+    for root, max_iter, tol in ((0, 30, 1e-6), (1700, 100, 1e-3)):
+        got = scl.diffusion.compute_dpt(m, root, max_iter=max_iter, tol=tol)
+        np.testing.assert_array_equal(bits(got), bits(port.dpt(ip, ind, v, root, max_iter, dt(tol), dt)))
+
+
+@pytest.mark.parametrize("dt,idt", VARIANTS)
 @pytest.mark.parametrize("n", [3, 400, 20000])
 def test_pseudotime_bit_exact(dt, idt, n):
     m, (ip, ind, v) = _graph(n, dt, idt, seed=8, density=10.0 / n)

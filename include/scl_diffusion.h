@@ -53,9 +53,12 @@ SCL_EXPORT scl_error_t scl_diffusion_magic_impute(scl_sparse_t transition, scl_r
  * (alpha 0 -> 0.85, tol 0 -> 1e-6, max_iter 0 -> 100, HKS steps 0 -> 10,
  * laziness 0 -> 0.5), checks and the restart walk's buffer swap (after an
  * unconverged last step the caller's array holds the previous iterate, as in
- * the reference). Each step is one kernel: (P x)_i as the sequential fma chain,
- * then y = fma(c_x, x, c_p (P x)) (lazy, HKS) or y = fma(alpha, (P x),
- * (1 - alpha) r) (restart); the restart walk's L1 change is summed in FP64.
+ * the reference). Each step is one kernel: (P x)_i as 32 lane fma chains
+ * (entries l, l+32, ...) combined by a fixed xor butterfly, then
+ * y = fma(c_x, x, c_p (P x)) (lazy, HKS) or y = fma(alpha, (P x),
+ * (1 - alpha) r) (restart); the restart walk's L1 change is summed in FP64 in
+ * a fixed block order and tested against tol on the device, the host reading
+ * the result once per eight queued steps.
  * scl-core's own SpMV rounding depends on its compiler's contraction, so these
  * agree with it to a few ulps rather than bit for bit. The walk's size is the
  * handle's primary dimension; n_nodes must be at least that

@@ -46,7 +46,7 @@ def _main():
     import torch
 
     ap = argparse.ArgumentParser()
-    ap.add_argument("case", choices=["spmm", "backward", "knn", "ppr"])
+    ap.add_argument("case", choices=["spmm", "backward", "knn", "ppr", "dpt"])
     ap.add_argument("--every", type=int, default=4)
     ap.add_argument("--cells", type=int, default=200_000)
     ap.add_argument("--k", type=int, default=30)
@@ -82,6 +82,17 @@ def _main():
         for _ in range(max(a.steps, 1)):
             pr = diffusion.personalized_pagerank(m, 0)
         print(f"cells={a.cells} nnz={ind.size} checksum={float(pr.sum()):.6e}")
+        return
+    if a.case == "dpt":  # diffusion pseudotime from cell 0 on the row-normalised graph (max 100 steps, tol 1e-6)
+        from . import diffusion
+        from .core.sparse import CsrMatrix
+
+        g, _, _, tm = build_graph(a.cells, a.k, reorder=False)
+        ip, ind, P = g.export()
+        m = CsrMatrix.wrap(ip.astype("int32"), ind.astype("int32"), P, (a.cells, a.cells))
+        for _ in range(max(a.steps, 1)):
+            pt = diffusion.compute_dpt(m, 0)
+        print(f"cells={a.cells} nnz={ind.size} checksum={float(pt.sum()):.6e}")
         return
     if a.case == "backward":
         g, _, _, tm = build_graph(a.cells, a.k, reorder=False)

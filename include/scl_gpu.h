@@ -237,6 +237,23 @@ SCL_EXPORT scl_error_t scl_gpu_batch_status(scl_gpu_batch_t batch, int* code, in
  * Results of a stalled launch are undefined. */
 SCL_EXPORT scl_error_t scl_gpu_batch_inject_stall(scl_gpu_batch_t batch, int graph);
 
+/* FP64 error of a diffused block against an FP64 reference (the final
+ * residual check of the precision forms). No counterpart in scl-core: its
+ * diffusion (scl/kernel/diffusion.hpp:638-664) has one precision per build,
+ * and this compares a 16- or 32-bit result with the FP64 build's.
+ *
+ * X (x_dtype: f32, f64, bf16 or f16) and X_ref (f64) are device blocks of
+ * n_rows * n_features elements. Reduced on the device in FP64 in a fixed order
+ * (the same bits on every run), then written to host memory out[4]:
+ *   out[0] = ||X - X_ref||_F / ||X_ref||_F   (0 when both are zero)
+ *   out[1] = max |x - r| / max(|r|, rel_floor)
+ *   out[2] = max |x - r|
+ *   out[3] = ||X_ref||_F
+ * Synchronises `stream`. */
+SCL_EXPORT scl_error_t scl_gpu_residual_fp64(const void* X, scl_dtype_t x_dtype, const double* X_ref,
+                                             int64_t n_rows, int64_t n_features, double rel_floor, double* out,
+                                             void* stream);
+
 /* Diffusion that allocates no device memory. No counterpart in scl-core.
  *
  * For callers that cannot allocate GPU memory while they run: a framework
@@ -247,14 +264,18 @@ SCL_EXPORT scl_error_t scl_gpu_batch_inject_stall(scl_gpu_batch_t batch, int gra
  * n_rows x n_features, the same bits as scl_gpu_diffuse) for a device CSR
  * transition matrix P given as indptr (int64, n_rows + 1), indices (int32,
  * each in [0, n_rows)) and values (f32). X and Y are caller-owned device
- * buffers and must be different; the one intermediate iterate lives in a
- * fixed 32 MiB scratch array compiled into the library, which every GPU that
- * loads the library holds until the process exits.
+ * buffers; they must not overlap each other or the library's scratch array
+ * (SCL_ERROR_INVALID_ARGUMENT otherwise), and every pointer must be non-null
+ * (SCL_ERROR_NULL_POINTER). The one intermediate iterate lives in a fixed
+ * 32 MiB scratch array compiled into the library, which every GPU that loads
+ * the library holds until the process exits.
  *
  * Limit: n_rows * n_features <= 8,388,608, else SCL_ERROR_INVALID_ARGUMENT
- * and nothing is launched. The first call on each device looks up the scratch
- * array's device address (cudaGetSymbolAddress); make that first call before
- * any stream capture. All calls share the one array and it keeps the last
+ * and nothing is launched. The first call on each device, and the first call
+ * from a context not seen before on it (another context, or the primary
+ * context re-created after cudaDeviceReset), looks up the scratch array's
+ * device address (cudaGetSymbolAddress); make that first call before any
+ * stream capture. All calls share the one array and it keeps the last
  * call's contents (every element is overwritten before it is read, so no
  * clearing is needed); calls that overlap on the GPU — other streams, other
  * threads — race on it. Asynchronous on `stream`. */

@@ -12,12 +12,16 @@
 // That array is a file-scope __device__ variable of kNoAllocMaxElems floats
 // (32 MiB): every GPU on which the library is loaded holds it until the
 // process exits. Host code must not pass the array's name to a kernel (on the
-// host it is only a stand-in symbol); the device address is looked up once per
-// device with cudaGetSymbolAddress and cached.
+// host it is only a stand-in symbol); the device address is looked up with
+// cudaGetSymbolAddress, with the device current, the first time a CUDA
+// context calls in, and cached under that context's process-unique id
+// (cuCtxGetId), so a caller that switches to another context on the same
+// device, or resets the device, gets the address in the context it runs in.
 //
 // The kernel is a warp-per-row FP32 SpMM with the same per-element arithmetic
 // as every other SpMM in this library: each output element is the sequential
 // fma chain over its row's entries in stored order.
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include <mutex>
@@ -32,21 +36,60 @@ constexpr int64_t kNoAllocMaxElems = 8388608;  // 32 MiB of float
 static __device__ __align__(256) float g_noalloc_scratch[kNoAllocMaxElems];
 
 std::mutex g_noalloc_mu;
-float* g_noalloc_ptr[64] = {nullptr};
+struct ScratchSlot {
+  unsigned long long ctx_id;  // process-unique id of the context the address belongs to
+  float* ptr;
+};
+ScratchSlot g_noalloc_slot[64] = {};
+
+using CtxGetCurrentFn = CUresult (*)(CUcontext*);
+using CtxGetIdFn = CUresult (*)(CUcontext, unsigned long long*);
+
+template <class Fn>
+Fn driver_fn(const char* name) {
+  void* p = nullptr;
+  cudaDriverEntryPointQueryResult q{};
+  if (cudaGetDriverEntryPoint(name, &p, cudaEnableDefault, &q) != cudaSuccess || q != cudaDriverEntryPointSuccess) {
+    (void)cudaGetLastError();
+    return nullptr;
+  }
+  return reinterpret_cast<Fn>(p);
+}
+
+// Id of the calling thread's current context (0 when it cannot be read).
+unsigned long long current_context_id() {
+  static const CtxGetCurrentFn get_current = driver_fn<CtxGetCurrentFn>("cuCtxGetCurrent");
+  static const CtxGetIdFn get_id = driver_fn<CtxGetIdFn>("cuCtxGetId");
+  if (!get_current || !get_id) return 0;
+  CUcontext ctx = nullptr;
+  unsigned long long id = 0;
+  if (get_current(&ctx) != CUDA_SUCCESS || ctx == nullptr) return 0;
+  if (get_id(ctx, &id) != CUDA_SUCCESS) return 0;
+  return id;
+}
 
 // Device address of the scratch array on `dev` (which must be current).
 float* scratch_for(int dev) {
   std::lock_guard<std::mutex> lk(g_noalloc_mu);
-  if (!g_noalloc_ptr[dev]) {
+  const unsigned long long ctx = current_context_id();
+  ScratchSlot& slot = g_noalloc_slot[dev];
+  if (slot.ptr == nullptr || ctx == 0 || slot.ctx_id != ctx) {
     void* p = nullptr;
     const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
     if (e != cudaSuccess || p == nullptr) {
       (void)cudaGetLastError();
       throw sclgpu::Error(SCL_ERROR_INTERNAL, "cudaGetSymbolAddress of the no-allocation scratch array failed");
     }
-    g_noalloc_ptr[dev] = static_cast<float*>(p);
+    slot.ptr = static_cast<float*>(p);
+    slot.ctx_id = ctx;
   }
-  return g_noalloc_ptr[dev];
+  return slot.ptr;
+}
+
+// True when the byte ranges [a, a + na) and [b, b + nb) share a byte.
+bool overlaps(const void* a, size_t na, const void* b, size_t nb) {
+  const uintptr_t x = reinterpret_cast<uintptr_t>(a), y = reinterpret_cast<uintptr_t>(b);
+  return x < y + nb && y < x + na;
 }
 
 // One warp per row (grid-stride); lane l handles columns l, l+32, ...
@@ -91,19 +134,26 @@ SCL_EXPORT scl_error_t scl_gpu_diffuse_noalloc(const int64_t* indptr, const int3
                                                int64_t n_rows, const float* X, float* Y, int64_t n_features,
                                                int64_t n_steps, void* stream) {
   SCL_API_CHECK_NULL(indptr, "Offset array pointer is null");
+  SCL_API_CHECK_NULL(indices, "Indices array pointer is null");
+  SCL_API_CHECK_NULL(values, "Data array pointer is null");
   SCL_API_CHECK_NULL(X, "Matrix X is null");
   SCL_API_CHECK_NULL(Y, "Matrix Y is null");
   SCL_API_CHECK(n_rows > 0 && n_features > 0 && n_steps >= 0, SCL_ERROR_INVALID_ARGUMENT,
                 "Dimensions must be positive");
   SCL_API_CHECK(n_features <= kNoAllocMaxElems / n_rows, SCL_ERROR_INVALID_ARGUMENT,
                 "n_rows * n_features exceeds the 8,388,608-element scratch array of the no-allocation entry point");
-  SCL_API_CHECK(X != Y, SCL_ERROR_INVALID_ARGUMENT, "X and Y must be different buffers");
+  const size_t block_bytes = (size_t)n_rows * (size_t)n_features * sizeof(float);
+  SCL_API_CHECK(!overlaps(X, block_bytes, Y, block_bytes), SCL_ERROR_INVALID_ARGUMENT,
+                "X and Y must not overlap");
   SCL_API_TRY
   cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
   int dev = 0;
   SCL_CUDA(cudaGetDevice(&dev));
   SCL_REQUIRE(dev >= 0 && dev < 64, SCL_ERROR_INTERNAL, "device ordinal out of range");
   float* scratch = scratch_for(dev);
+  const size_t scratch_bytes = (size_t)kNoAllocMaxElems * sizeof(float);
+  SCL_REQUIRE(!overlaps(X, block_bytes, scratch, scratch_bytes) && !overlaps(Y, block_bytes, scratch, scratch_bytes),
+              SCL_ERROR_INVALID_ARGUMENT, "X and Y must not lie in the library's no-allocation scratch array");
   const int64_t n = n_rows, F = n_features;
   if (n_steps == 0) {
     SCL_CUDA(cudaMemcpyAsync(Y, X, n * F * sizeof(float), cudaMemcpyDeviceToDevice, s));

@@ -77,6 +77,27 @@ def test_null_and_dimension_errors_match_reference_codes():
     assert lib.scl_get_last_error() == b"No error" and lib.scl_get_last_error_code() == 0
 
 
+def test_noalloc_argument_errors_before_any_launch():
+    """scl_gpu_diffuse_noalloc rejects null and overlapping buffers on the host,
+    before it touches the device (the addresses below are never dereferenced)."""
+    lib = get_library("f32_i32")
+    fn = lib.scl_gpu_diffuse_noalloc
+    ip, ix, v, X, Y = (ctypes.c_void_p(a) for a in (0x10000, 0x20000, 0x30000, 0x100000, 0x200000))
+    n, F = 100, 8  # one block is 3,200 bytes
+    for pos, msg in [(0, b"Offset array pointer is null"), (1, b"Indices array pointer is null"),
+                     (2, b"Data array pointer is null"), (3, b"Matrix X is null"), (4, b"Matrix Y is null")]:
+        args = [ip, ix, v, X, Y]
+        args[pos] = None
+        assert fn(args[0], args[1], args[2], n, args[3], args[4], F, 2, None) == 4
+        assert lib.scl_get_last_error() == msg
+    for y_addr in (0x100000, 0x100000 + 3196, 0x100000 - 3196):  # same, tail overlap, head overlap
+        assert fn(ip, ix, v, n, X, ctypes.c_void_p(y_addr), F, 2, None) == 10
+        assert lib.scl_get_last_error() == b"X and Y must not overlap"
+    assert fn(ip, ix, v, 0, X, Y, F, 2, None) == 10
+    assert fn(ip, ix, v, 8388609, X, Y, 1, 2, None) == 10
+    assert b"exceeds" in lib.scl_get_last_error()
+
+
 def test_sparse_create_validation():
     lib = get_library("f64_i64")
     h = ctypes.c_void_p()

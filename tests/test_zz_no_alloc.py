@@ -66,6 +66,28 @@ def test_noalloc_matches_regular_entry_point_twice(F, steps):
         assert torch.equal(Y.view(torch.int32), want.view(torch.int32)), f"call {call} differs"
 
 
+@pytest.mark.parametrize("F,steps", [(5, 3), (64, 2)])
+def test_noalloc_matches_oracle_twice(F, steps):
+    """Independent check: the oracle restatement of scl-core's diffuse_matrix
+    (sequential fma chain per element, rows in stored order) on the same CSR."""
+    import torch
+
+    from oracle import port
+
+    lib = get_library("f32_i32")
+    g, dev, n = _graph(n=2500, k=12, seed=5)
+    ip, ind, P = g.export()
+    for call in range(2):
+        X0 = scl.synthetic.features(n, F, seed=40 + call)
+        want = port.diffuse_matrix(ip, ind, P, X0, steps)
+        X = torch.from_numpy(X0).cuda()
+        Y = torch.full((n, F), float("nan"), device="cuda")
+        rc = _noalloc(lib, dev, n, X, Y, F, steps)
+        assert rc == 0, lib.scl_get_last_error()
+        got = Y.cpu().numpy()
+        assert np.array_equal(got.view(np.uint32), want.view(np.uint32)), f"call {call} differs from the oracle"
+
+
 def test_noalloc_rejects_oversized_blocks():
     import torch
 

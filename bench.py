@@ -143,17 +143,53 @@ def gpu_uuid(torch, device):
 
 
 # ---- inputs ------------------------------------------------------------------------
-def build_inputs(torch, device):
-    import scl
+def synthetic_module():
+    """scl-core_b200/scl/synthetic.py loaded on its own (NumPy / torch only), so
+    that the reference arm never imports this repository's package or loads
+    its libraries."""
+    import importlib.util
 
-    t0 = time.time()
-    pts = scl.synthetic.mixture(N_CELLS, seed=0)
-    ki, kd = scl.synthetic.knn_device(pts, K_NN, device=device, block=2048)
+    spec = importlib.util.spec_from_file_location("scl_synthetic_inputs", ROOT / "scl-core_b200" / "scl" / "synthetic.py")
+    mod = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mod)
+    return mod
+
+
+def native_knn(scl, pts, k):
+    """kNN of the rows of `pts` through this library's scl_knn (the drop-in
+    neighbors ABI, host buffers): (idx int32 [n, k], dist float32 [n, k]) as
+    NumPy arrays, and the wall time in seconds."""
+    pts = np.ascontiguousarray(pts, dtype=np.float32)
+    n, d = pts.shape
+    ip = np.arange(0, (n + 1) * d, d, dtype=np.int64)
+    if ip[-1] < 2**31:
+        ip = ip.astype(np.int32)
+    m = scl.CsrMatrix.wrap(ip, np.tile(np.arange(d, dtype=np.int32), n), pts.reshape(-1), (n, d))
+    t0 = time.perf_counter()
+    norms = scl.neighbors.compute_norms(m)
+    idx, dist = scl.neighbors.knn(m, k, norms)
+    dt = time.perf_counter() - t0
+    del m
+    return idx.astype(np.int32, copy=False), dist.astype(np.float32, copy=False), dt
+
+
+def native_graph(torch, scl, n, k, seed, stream=None, normalize=True):
+    """Seeded mixture -> scl_knn -> Gaussian weights and (W+W^T)/2 -> row
+    normalisation, all through this library: (GpuGraph, info dict)."""
+    syn = synthetic_module()
+    pts = syn.mixture(n, seed=seed)
+    ki, kd, t_knn = native_knn(scl, pts, k)
     del pts
-    torch.cuda.synchronize()
-    torch.cuda.empty_cache()  # release the kNN distance tiles before the measured work
-    t_knn = time.time() - t0
-    return ki, kd, t_knn
+    s = stream if stream is not None else torch.cuda.current_stream()
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    kit, kdt = torch.from_numpy(ki).cuda(), torch.from_numpy(kd).cuda()
+    a.record(s)
+    g = scl.gpu.GpuGraph.from_knn(kit, kdt, stream=s)
+    if normalize:
+        g.normalize(symmetric=False, stream=s)
+    b.record(s)
+    b.synchronize()
+    return g, {"knn_s": round(t_knn, 3), "build_ms": round(a.elapsed_time(b), 3)}
 
 
 def flush_l2(torch, buf):
@@ -178,24 +214,30 @@ def timed_calls(torch, fn, steps, warmup, flush_buf, stream):
 
 
 # ---- CPU baseline (scl-core's own implementation) ---------------------------------------
-def cpu_reference_diffusion(ip, ind, P, n, F, target_s=12.0, max_steps=N_STEPS):
-    """Times oracle/_ref f32_i32 diffuse_matrix on a bounded number of steps of
-    the full graph; returns (GB/s, steps_run, seconds, cores)."""
-    from oracle import ref
+def reference_diffusion(R, ip, ind, P, X0, steps, reps=1):
+    """scl-core's own diffuse_matrix (oracle/_ref, all host threads) on the given
+    graph and block: (result of the last rep, seconds per rep list)."""
+    out, ts = None, []
+    for _ in range(reps):
+        t0 = time.perf_counter()
+        out = R.diffuse_matrix(ip, ind, P, X0, steps)
+        ts.append(time.perf_counter() - t0)
+    return out, ts
 
-    R = ref.RefLib("f32_i32")
-    X0 = np.random.default_rng(1).standard_normal((n, F)).astype(np.float32)
-    t0 = time.time()
-    R.diffuse_matrix(ip, ind, P, X0, 1)
-    t1 = time.time() - t0
-    steps = int(max(1, min(max_steps, target_s // max(t1, 1e-3))))
-    t0 = time.time()
-    R.diffuse_matrix(ip, ind, P, X0, steps)
-    dt = time.time() - t0
-    nnz = int(ind.size)
-    gbs = step_bytes(n, nnz, F) * steps / dt / 1e9
-    cores = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1))
-    return gbs, steps, dt, cores, R.path.name
+
+def host_cores():
+    return int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1))
+
+
+def workload_config(world):
+    """The config dict both arms print (the workload's definition, not its
+    generated graph: nnz is reported beside it)."""
+    return {"workload": "diffusion 500k cells k=30 64 cols 16 steps (FP32 plain, row-normalised)",
+            "cells": N_CELLS, "k": K_NN, "features": N_FEAT, "diffusion_steps": N_STEPS,
+            "graph": "seeded 10-component 50-D mixture (seed 0), Gaussian adaptive-sigma weights, (W+W^T)/2",
+            "x0": "N(0,1) FP32, torch generator seed 1 + rank",
+            "l2": "GPU arm: flushed (256 MiB write) before every timed step",
+            "parallelism": f"replicas x{world}"}
 
 
 def profiled_traffic(name):
@@ -237,13 +279,7 @@ def bench_backward(torch, scl, device, stream, reps, warmup, flush):
     import scl.autograd  # noqa: F401
 
     n, k, F, T, every = 200_000, 30, 32, 8, 4
-    pts = scl.synthetic.mixture(n, seed=0)
-    ki, kd = scl.synthetic.knn_device(pts, k, device=device, block=4096)
-    torch.cuda.synchronize()
-    torch.cuda.empty_cache()
-    g = scl.gpu.GpuGraph.from_knn(ki, kd, stream=stream)
-    g.normalize(symmetric=False, stream=stream)
-    del ki, kd
+    g, _ = native_graph(torch, scl, n, k, seed=0, stream=stream)
     gen = torch.Generator(device=device).manual_seed(7)
     X0 = torch.randn((n, F), device=device, generator=gen)
     Yt = torch.randn((n, F), device=device, generator=gen)
@@ -280,12 +316,9 @@ def bench_impute(torch, scl, device, reps, warmup, with_reference=True):
     import scipy.sparse as sp
 
     n, k, G, t = 100_000, 15, 1000, 3
-    pts = scl.synthetic.mixture(n, seed=11)
-    ki, kd = scl.synthetic.knn_device(pts, k, device=device, block=8192)
-    g = scl.gpu.GpuGraph.from_knn(ki, kd)
+    g, _ = native_graph(torch, scl, n, k, seed=11, normalize=False)
     ip, ind, W = g.export()
     g.close()
-    del ki, kd, pts
     Xs = sp.random(n, G, density=0.05, random_state=12, format="csr", dtype=np.float32)
     Xs.sort_indices()
     pin = lambda a: torch.from_numpy(np.ascontiguousarray(a)).pin_memory().numpy()
@@ -382,7 +415,7 @@ def bench_knn(torch, scl, reps, warmup, with_reference=True):
     return res
 
 
-def bench_batched(torch, scl, device, stream, reps, warmup, rank=0, world=1, dist=None):
+def bench_batched(torch, scl, device, stream, reps, warmup, rank=0, world=1, dist=None, check_reference=True):
     """Batched form: 64 graphs, cell counts log-uniform in [2,000, 100,000]
     (seed 0), each its own 10-component mixture, k=15, row-normalised FP32,
     16-column blocks, 8 steps: one persistent CUDA-graph launch (autotuned
@@ -397,10 +430,7 @@ def bench_batched(torch, scl, device, stream, reps, warmup, rank=0, world=1, dis
     sizes = [(b, sizes_all[b]) for b in mine]
     graphs = []
     for b, n in sizes:
-        pts = scl.synthetic.mixture(int(n), seed=100 + b)
-        ki, kd = scl.synthetic.knn_device(pts, 15, device=device, block=8192)
-        g = scl.gpu.GpuGraph.from_knn(ki, kd, stream=stream)
-        g.normalize(symmetric=False, stream=stream)
+        g, _ = native_graph(torch, scl, int(n), 15, seed=100 + b, stream=stream)
         graphs.append(g)
     torch.cuda.synchronize()
     torch.cuda.empty_cache()
@@ -422,6 +452,22 @@ def bench_batched(torch, scl, device, stream, reps, warmup, rank=0, world=1, dis
     t_s = event_ms(torch, seq, stream, reps, warmup)
     same = bool(torch.equal(Y, Ys))
     nnz = batch.nnz_total
+    # every graph's batched result against scl-core's own diffuse_matrix
+    # (oracle/_ref, host threads) on the same graph and block, outside the timing
+    ref_same = None
+    if check_reference:
+        try:
+            from oracle import ref
+
+            R = ref.RefLib("f32_i32")
+            Xh, Yh = X0.cpu().numpy(), Y.cpu().numpy()
+            ref_same = True
+            for i, g in enumerate(graphs):
+                ip, ind, P = g.export()
+                want, _ = reference_diffusion(R, ip, ind, P, Xh[offs[i]:offs[i + 1]], T)
+                ref_same &= bool(np.array_equal(want.view(np.uint32), Yh[offs[i]:offs[i + 1]].view(np.uint32)))
+        except Exception as e:  # informational; never fail the run on it
+            ref_same = f"unavailable: {e}"
     batch.close()
     for g in graphs:
         g.close()
@@ -433,7 +479,72 @@ def bench_batched(torch, scl, device, stream, reps, warmup, rank=0, world=1, dis
             "graphs": 64, "graphs_this_rank": len(mine), "cells_this_rank": int(offs[-1]),
             "nnz_this_rank": int(nnz), "sharding": f"LPT over {world} rank(s), no data-path collective",
             "batched_ms": round(t_b, 4), "sequential_ms": round(t_s, 4), "speedup": round(t_s / t_b, 3),
-            "bit_identical_to_sequential": same, "status": code, "schedule": sched}
+            "bit_identical_to_sequential": same, "bit_identical_to_reference": ref_same, "status": code,
+            "schedule": sched}
+
+
+def run_reference_arm(args, warmup):
+    """scl-core's own CPU diffusion (oracle/_ref f32_i32, all host threads) on
+    this workload, through its C ABI the way its Python wrapper drives it.
+    Rank 0 alone runs; nothing of this repository's package or libraries is
+    imported or loaded. The graph is built on the host from kNN lists computed
+    with torch (an input generator, untimed), Gaussian weights and (W+W^T)/2
+    in NumPy / SciPy, then scl-core's own
+    scl_diffusion_compute_transition_matrix. One step = one full 16-step
+    diffusion of the 500k x 64 block, as in the GPU arm."""
+    import scipy.sparse as sp
+    import torch
+
+    from oracle import ref
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    if rank != 0:
+        return
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    device = f"cuda:{local}"
+    torch.cuda.set_device(local)
+    syn = synthetic_module()
+    t0 = time.time()
+    pts = syn.mixture(N_CELLS, seed=0)
+    ki, kd = syn.knn_device(pts, K_NN, device=device, block=2048)
+    ki, kd = ki.cpu().numpy(), kd.cpu().numpy()
+    del pts
+    torch.cuda.empty_cache()
+    # sigma_i = distance to the k-th neighbour (floored at 1e-10), w = exp(-(d/sigma_i)^2), (W + W^T)/2
+    sigma = np.maximum(kd.max(axis=1), np.float32(1e-10)).astype(np.float32)
+    w = np.exp(-np.square(kd / sigma[:, None])).astype(np.float32)
+    A = sp.csr_matrix((w.reshape(-1), ki.reshape(-1).astype(np.int64), np.arange(0, N_CELLS * K_NN + 1, K_NN)),
+                      shape=(N_CELLS, N_CELLS))
+    S = ((A + A.T) * np.float32(0.5)).tocsr()
+    S.sum_duplicates()
+    S.sort_indices()
+    ip, ind, W = S.indptr, S.indices, S.data.astype(np.float32)
+    t_inputs = time.time() - t0
+    R = ref.RefLib("f32_i32")
+    t0 = time.perf_counter()
+    P = R.transition(ip, ind, W, N_CELLS)
+    t_tr = time.perf_counter() - t0
+    gen = torch.Generator(device=device).manual_seed(1)
+    X0 = torch.randn((N_CELLS, N_FEAT), device=device, dtype=torch.float32, generator=gen).cpu().numpy()
+    nnz = int(ind.size)
+    _, tw = reference_diffusion(R, ip, ind, P, X0, N_STEPS, reps=warmup)
+    _, ts = reference_diffusion(R, ip, ind, P, X0, N_STEPS, reps=args.steps)
+    t = float(np.mean(ts))
+    gbs = step_bytes(N_CELLS, nnz, N_FEAT) * N_STEPS / t / 1e9
+    cores = host_cores()
+    line = {"impl": "reference", "metric": METRIC, "value": round(gbs, 3), "unit": "GB/s", "n_gpus": world,
+            "steps": args.steps, "warmup": warmup, "ms_per_step": round(1e3 * t, 3), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (seeded 10-component 50-D mixture; kNN lists from torch on the device, untimed)",
+            "config": workload_config(world),
+            "graph": {"nnz": nnz, "inputs_s": round(t_inputs, 2)},
+            "cpu_baseline": {"value": round(gbs, 3), "unit": "GB/s", "cores": cores, "kind": "reference",
+                             "sample": f"scl_diffusion_diffuse_matrix ({R.path.name}, scl-core compiled) on the full "
+                                       f"500k graph, all 16 steps per sample, {cpu_model()}"},
+            "transition_ms_cpu": round(1e3 * t_tr, 3),
+            "e2e": {"value": round(gbs, 3), "unit": "GB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
 
 
 def cpu_model():
@@ -446,12 +557,98 @@ def cpu_model():
     return "unknown"
 
 
+# ---- named profiling cases --------------------------------------------------------------------
+CASES = {
+    "spmm": "diffusion steps through scl_gpu_diffuse (--storage, --plan, --no-reorder)",
+    "backward": "checkpointed forward + backward of L = sum((X_T - Y)^2) (--every)",
+    "knn": "brute-force kNN of the mixture through scl_knn (host buffers)",
+    "ppr": "personalized PageRank from cell 0 through the drop-in ABI",
+    "dpt": "diffusion pseudotime from cell 0 through the drop-in ABI",
+    "e2e": "scl_diffusion_diffuse_matrix with pinned host buffers",
+}
+
+
+def run_case(args):
+    """One named workload, for ncu captures and sweeps: the seeded mixture graph
+    built natively (scl_knn, weights, (W+W^T)/2, row normalisation), then the
+    case's calls; prints one line with a checksum.
+
+        python bench.py --case spmm --cells 500000 --features 64 --case-steps 4 [--storage bf16]
+    """
+    import torch
+
+    import scl
+
+    steps = max(args.case_steps, 1)
+    if args.case == "knn":
+        syn = synthetic_module()
+        pts = syn.mixture(args.cells, seed=21).astype(np.float32)[:, : args.features]
+        for _ in range(steps):
+            idx, dist, _ = native_knn(scl, pts, args.k)
+        print(f"cells={pts.shape[0]} features={pts.shape[1]} k={args.k} "
+              f"checksum={float(dist[np.isfinite(dist)].sum()):.6e}")
+        return
+    g, info = native_graph(torch, scl, args.cells, args.k, seed=0)
+    n, _, nnz = g.shape
+    if args.case in ("ppr", "dpt", "e2e"):
+        ip, ind, P = g.export()
+        m = scl.CsrMatrix.wrap(ip.astype(np.int32), ind, P, (n, n))
+        if args.case == "ppr":
+            for _ in range(steps):
+                out = scl.diffusion.personalized_pagerank(m, 0)
+        elif args.case == "dpt":
+            for _ in range(steps):
+                out = scl.diffusion.compute_dpt(m, 0)
+        else:
+            X0 = torch.randn((n, args.features)).numpy()
+            for _ in range(steps):
+                out = torch.from_numpy(X0).pin_memory().numpy()
+                scl.diffusion.diffuse_matrix(m, out, N_STEPS)
+        print(f"case={args.case} cells={n} nnz={nnz} checksum={float(np.sum(out, dtype=np.float64)):.6e}")
+        return
+    if args.case == "backward":
+        gen = torch.Generator(device="cuda").manual_seed(7)
+        X0 = torch.randn((n, args.features), device="cuda", generator=gen)
+        Yt = torch.randn((n, args.features), device="cuda", generator=gen)
+        XT, ck = g.diffuse_checkpointed(X0, steps, args.every)
+        dX, dW = g.diffuse_backward(X0, ck, 2.0 * (XT - Yt), steps, args.every)
+        torch.cuda.synchronize()
+        print(f"case=backward cells={n} nnz={nnz} features={args.features} steps={steps} every={args.every} "
+              f"loss={float(((XT - Yt) ** 2).sum()):.6e} |dX|={float(dX.norm()):.6e} |dW|={float(dW.norm()):.6e}")
+        return
+    if not args.no_reorder:
+        g.reorder(1)
+    dt = {"bf16": torch.bfloat16, "f16": torch.float16}.get(args.storage)
+    if dt is not None:
+        g.set_storage(dt)
+    if args.plan:
+        grp, vec, kind, stage = (int(x) for x in args.plan.split(","))
+        g.set_plan(args.features, grp, vec, kind, stage)
+    X = torch.randn((n, args.features), device="cuda")
+    if dt is not None:
+        X = X.to(dt)
+    Y = g.diffuse(X, steps)
+    torch.cuda.synchronize()
+    print(f"case=spmm cells={n} nnz={nnz} features={args.features} steps={steps} storage={args.storage} "
+          f"reorder={not args.no_reorder} build_ms={info['build_ms']:.2f} checksum={float(Y.float().sum()):.6e}")
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--case", default=None, choices=sorted(CASES),
+                    help="run one named profiling case instead of the benchmark (see run_case)")
+    ap.add_argument("--cells", type=int, default=200_000, help="--case: cells")
+    ap.add_argument("--k", type=int, default=30, help="--case: neighbours")
+    ap.add_argument("--features", type=int, default=64, help="--case: columns")
+    ap.add_argument("--case-steps", type=int, default=3, help="--case: diffusion steps / repetitions")
+    ap.add_argument("--every", type=int, default=4, help="--case backward: checkpoint interval")
+    ap.add_argument("--storage", default="f32", choices=["f32", "bf16", "f16"], help="--case spmm: storage")
+    ap.add_argument("--no-reorder", action="store_true", help="--case spmm: no locality reordering")
+    ap.add_argument("--plan", default="", help="--case spmm: group,vec,kind,stage launch shape")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-forms", action="store_true", help="skip the BF16/FP16 forms")
@@ -462,6 +659,12 @@ def main():
     ap.add_argument("--no-knn", action="store_true", help="skip the kNN configuration")
     args = ap.parse_args()
     warmup = max(3, args.warmup)
+    os.environ.setdefault("OMP_NUM_THREADS", str(os.cpu_count() or 1))
+
+    if args.case:
+        return run_case(args)
+    if args.impl == "reference":
+        return run_reference_arm(args, warmup)
 
     import torch
 
@@ -480,62 +683,25 @@ def main():
 
     import scl
 
-    os.environ.setdefault("OMP_NUM_THREADS", str(os.cpu_count() or 1))
-    ki, kd, t_knn = build_inputs(torch, device)
     stream = torch.cuda.current_stream()
 
-    if args.impl == "reference":
-        # scl-core's CPU path on the host cores; rank 0 only.
-        if rank == 0:
-            g = scl.gpu.GpuGraph.from_knn(ki, kd)
-            ip, ind, W = g.export()
-            del g
-            from oracle import ref
-
-            R = ref.RefLib("f32_i32")
-            n = N_CELLS
-            t0 = time.time()
-            P = R.transition(ip, ind, W, n)
-            t_tr = time.time() - t0
-            per = []
-            for _ in range(args.steps):
-                gbs, st, dt, cores, libname = cpu_reference_diffusion(ip, ind, P, n, N_FEAT, target_s=8.0)
-                per.append((gbs, st, dt))
-            gbs = float(np.median([p[0] for p in per]))
-            line = {"impl": "reference", "metric": METRIC, "value": round(gbs, 3), "unit": "GB/s", "n_gpus": world,
-                    "steps": args.steps, "warmup": 0, "ms_per_step": round(1e3 * np.median([p[2] for p in per]), 3),
-                    "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
-                    "data": "synthetic (seeded 10-component 50-D mixture, kNN on device)",
-                    "config": {"workload": "diffusion 500k cells k=30 64 cols 16 steps (FP32, row-normalised)",
-                               "cells": n, "k": K_NN, "features": N_FEAT, "diffusion_steps": N_STEPS,
-                               "nnz": int(ind.size), "reference_steps_per_sample": per[0][1]},
-                    "cpu_baseline": {"value": round(gbs, 3), "unit": "GB/s", "cores": cores, "kind": "reference",
-                                     "sample": f"scl_diffusion_diffuse_matrix on the full 500k graph, "
-                                               f"{per[0][1]} of 16 steps per sample ({libname}, {cpu_model()})"},
-                    "transition_ms_cpu": round(1e3 * t_tr, 3),
-                    "e2e": {"value": round(gbs, 3), "unit": "GB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
-            print(json.dumps(line), flush=True)
-        if dist is not None:
-            dist.barrier()
-            dist.destroy_process_group()
-        return
-
-    # ---- graph build on the device (timed once, reported beside the metric) ----------
+    # ---- graph from features, natively: scl_knn -> weights / (W+W^T)/2 -> row normalisation ----
+    g, build = native_graph(torch, scl, N_CELLS, K_NN, seed=0, stream=stream, normalize=False)
+    ip, ind, W = g.export()  # pre-normalisation weights, for the FP64 checks
     bt0 = torch.cuda.Event(enable_timing=True)
     bt1 = torch.cuda.Event(enable_timing=True)
     bt0.record(stream)
-    g = scl.gpu.GpuGraph.from_knn(ki, kd, stream=stream)
     g.normalize(symmetric=False, stream=stream)
     bt1.record(stream)
     bt1.synchronize()
-    build_ms = bt0.elapsed_time(bt1)
-    # locality reordering (connected components), a one-off per graph
+    build["normalize_ms"] = round(bt0.elapsed_time(bt1), 3)
+    # locality reordering, a one-off per graph
     bt0.record(stream)
     g.reorder(1, stream=stream)
     bt1.record(stream)
     bt1.synchronize()
-    reorder_ms = bt0.elapsed_time(bt1)
-    _, cc_rounds = g.reorder_info()
+    build["reorder_ms"] = round(bt0.elapsed_time(bt1), 3)
+    _, build["reorder_cc_rounds"] = g.reorder_info()
     n, _, nnz = g.shape
     F, T = N_FEAT, N_STEPS
     tuned = g.autotune(F, reps=3, stream=stream)  # one-off: fastest bit-identical launch shape
@@ -565,22 +731,19 @@ def main():
     per_launch_ms = t_ms / T
     peak, peak_kind = load_peaks()
     achieved = B32 / (per_launch_ms * 1e-3) / 1e9
+    _, _, Pm = g.export()
 
-    # ---- FP64 reference on the device for the precision forms --------------------------
-    ip, ind, Pm = g.export()
+    # ---- FP64 on the device (same weights, FP64 transition) and the precision forms -------
     forms = {}
+    fp64 = {}
     if rank == 0 and not args.no_forms:
-        g64 = scl.gpu.GpuGraph.from_knn(ki, kd, variant="f64_i64")  # same W, FP64 normalisation below
-        ip64, ind64, W32 = g64.export()
-        g64.close()
-        g64 = scl.gpu.GpuGraph.from_csr(ip64, ind64, W32.astype(np.float64), (n, n), variant="f64_i64")
+        g64 = scl.gpu.GpuGraph.from_csr(ip, ind, W.astype(np.float64), (n, n), variant="f64_i64")
         g64.normalize(symmetric=False)
         g64.reorder(1)
         Y64 = g64.diffuse(X0.double(), T)
-        Y32 = Y.clone()
-        err32 = float(torch.linalg.norm(Y32.double() - Y64) / torch.linalg.norm(Y64))
-        forms["f32"] = {"gbs": round(value / world, 2), "ms": round(t_ms, 4), "rel_fro_err_vs_fp64": err32,
-                        "max_rel_err_vs_fp64": float(((Y32.double() - Y64).abs() / Y64.abs().clamp_min(1e-3)).max())}
+        e32 = scl.gpu.residual_fp64(Y, Y64, rel_floor=1e-3)
+        forms["f32"] = {"gbs": round(value / world, 2), "ms": round(t_ms, 4), "rel_fro_err_vs_fp64": e32["rel_fro"],
+                        "max_rel_err_vs_fp64": e32["max_rel"]}
         for name, tdt in (("bf16", torch.bfloat16), ("f16", torch.float16)):
             g.set_storage(tdt, stream=stream)
             tuned_l = g.autotune(F, reps=3, stream=stream)  # fastest bit-identical shape for this storage
@@ -591,21 +754,39 @@ def main():
                 g.diffuse(Xl, T, out=Yl, stream=stream)
 
             tl = float(np.mean(timed_calls(torch, run_l, args.steps, warmup, flush, stream)))
-            err = float(torch.linalg.norm(Yl.double() - Y64) / torch.linalg.norm(Y64))
-            # per-step errors vs FP64 (rounded iterates)
+            el = scl.gpu.residual_fp64(Yl, Y64, rel_floor=1e-3)
+            # per-step errors vs FP64 (16-bit iterates against FP64 iterates), reduced in FP64 on the device
             step_err = []
             Xs, X64s = Xl, X0.double()
-            for s in range(T):
+            for _ in range(T):
                 Xs = g.diffuse(Xs, 1, out_dtype=tdt)
                 X64s = g64.diffuse(X64s, 1)
-                step_err.append(float(torch.linalg.norm(Xs.double() - X64s) / torch.linalg.norm(X64s)))
+                step_err.append(scl.gpu.residual_fp64(Xs, X64s, rel_floor=1e-3)["rel_fro"])
             forms[name] = {"gbs": round(B16 * T / (tl * 1e-3) / 1e9, 2), "ms": round(tl, 4),
                            "plan": {"kind": tuned_l["kind"], "stage": tuned_l["stage"]},
-                           "speedup_vs_f32": round(t_ms / tl, 3), "rel_fro_err_vs_fp64": err,
-                           "max_rel_err_vs_fp64": float(((Yl.double() - Y64).abs() / Y64.abs().clamp_min(1e-3)).max()),
-                           "per_step_rel_fro_err": [round(e, 7) for e in step_err]}
+                           "speedup_vs_f32": round(t_ms / tl, 3), "rel_fro_err_vs_fp64": round(el["rel_fro"], 8),
+                           "max_rel_err_vs_fp64": round(el["max_rel"], 6),
+                           "per_step_rel_fro_err": [round(e, 6) for e in step_err]}
+            del Xs, X64s
         g.set_storage(torch.float32, stream=stream)
         g64.close()
+        # FP64 pinned to scl-core's own f64 build (transition + diffusion on the same weights and block)
+        if world == 1 and not args.no_cpu_baseline:
+            try:
+                from oracle import ref
+
+                R64 = ref.RefLib("f64_i64")
+                P64r = R64.transition(ip, ind, W.astype(np.float64), n)
+                Y64r, t64 = reference_diffusion(R64, ip, ind, P64r, X0.double().cpu().numpy(), T)
+                fp64 = {"gpu_fp64_bit_identical_to_reference_f64": bool(np.array_equal(
+                            Y64.cpu().numpy().view(np.uint64), Y64r.view(np.uint64))),
+                        "reference_f64_s": round(t64[0], 2)}
+                e32r = scl.gpu.residual_fp64(Y, torch.from_numpy(Y64r).to(device), rel_floor=1e-3)
+                fp64["f32_rel_fro_err_vs_reference_f64"] = e32r["rel_fro"]
+                fp64["f32_max_rel_err_vs_reference_f64"] = e32r["max_rel"]
+                del Y64r, P64r
+            except Exception as e:  # informational; never fail the run on it
+                fp64 = {"reference_f64": f"unavailable: {e}"}
         del Y64
 
     # ---- differentiation and batched forms (each rank runs its own replica) ---------------
@@ -614,7 +795,8 @@ def main():
         fwd_bwd = bench_backward(torch, scl, device, stream, args.steps, warmup, flush)
     batched = None
     if not args.no_batched:
-        batched = bench_batched(torch, scl, device, stream, args.steps, warmup, rank, world, dist)
+        batched = bench_batched(torch, scl, device, stream, args.steps, warmup, rank, world, dist,
+                                check_reference=(rank == 0 and not args.no_cpu_baseline))
 
     impute = None
     if rank == 0 and not args.no_impute:
@@ -622,6 +804,7 @@ def main():
     knn = None
     if rank == 0 and not args.no_knn:
         knn = bench_knn(torch, scl, min(args.steps, 3), 1, with_reference=not args.no_cpu_baseline)
+        knn["graph_500k_scl_knn_s"] = build["knn_s"]
 
     # ---- end to end through the drop-in C ABI with pinned host buffers --------------------
     e2e = None
@@ -651,7 +834,8 @@ def main():
             e_s = float(tt.item())
         e2e = {"value": round(world * B32 * T / e_s / 1e9, 3), "unit": "GB/s",
                "h2d_bytes_per_step": int(st["h2d_bytes"]), "d2h_bytes_per_step": int(st["d2h_bytes"]),
-               "ms_per_step": round(1e3 * e_s, 3), "api": "scl_diffusion_diffuse_matrix (libscl_f32_i32.so)",
+               "ms_per_step": round(1e3 * e_s, 3), "device_ms": round(float(st["device_ms"]), 3),
+               "api": "scl_diffusion_diffuse_matrix (libscl_f32_i32.so)",
                "bit_exact_vs_device_path": bool(np.array_equal(Xn.view(np.uint32),
                                                                Y.cpu().numpy().view(np.uint32)))}
         # personalized PageRank on the same graph and host handle (scl_diffusion_personalized_pagerank,
@@ -676,7 +860,7 @@ def main():
                     t0 = time.perf_counter()
                     want = R.walk("ppr", ip, ind, Pm, n, seed=0, alpha=0.85, max_iter=100, tol=1e-6)
                     rdt = time.perf_counter() - t0
-                    walks.update({"reference_cpu_ms": round(1e3 * rdt, 1), "reference_cores": os.cpu_count(),
+                    walks.update({"reference_cpu_ms": round(1e3 * rdt, 1), "reference_cores": host_cores(),
                                   "e2e_speedup_vs_reference": round(rdt / float(np.median(pt)), 2),
                                   "max_rel_diff_vs_reference": float(np.max(np.abs(pr - want) /
                                                                             np.maximum(np.abs(want), 1e-30)))})
@@ -684,40 +868,65 @@ def main():
                     walks["reference_cpu_ms"] = f"unavailable: {e}"
         del m
 
-    # ---- CPU baseline (rank 0, N=1) ------------------------------------------------------------
+    # ---- CPU baseline and full-size parity (rank 0, N=1): scl-core's own diffuse_matrix on the
+    # same P and the same X0 as the device run; the device result must equal it bit for bit ----------
     cpu = None
+    parity = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
-            gbs, st_, dt, cores, libname = cpu_reference_diffusion(ip, ind, Pm, n, F, target_s=12.0)
-            cpu = {"value": round(gbs, 3), "unit": "GB/s", "cores": cores, "kind": "reference",
-                   "sample": f"scl_diffusion_diffuse_matrix (scl-core compiled, {libname}) on the full 500k graph, "
-                             f"{st_} of 16 steps, {dt:.1f} s, {cpu_model()}"}
+            from oracle import ref
+
+            R = ref.RefLib("f32_i32")
+            want, ts = reference_diffusion(R, ip, ind, Pm, X0.cpu().numpy(), T, reps=3)
+            dt = float(np.median(ts))
+            cpu = {"value": round(B32 * T / dt / 1e9, 3), "unit": "GB/s", "cores": host_cores(), "kind": "reference",
+                   "sample": f"scl_diffusion_diffuse_matrix (scl-core compiled, {R.path.name}) on the full 500k "
+                             f"graph and the device run's X0, all 16 steps, median of 3 ({dt:.2f} s), {cpu_model()}"}
+            parity = {"bit_identical_to_reference": bool(np.array_equal(want.view(np.uint32),
+                                                                        Y.cpu().numpy().view(np.uint32))),
+                      "reference": f"{R.path.name} diffuse_matrix, same P and X0, 16 steps"}
+            # transition: this library's FP64-degree normalisation vs scl-core's f32 compute_transition_matrix
+            Pr = R.transition(ip, ind, W, n)
+            du = np.abs(Pm.view(np.int32).astype(np.int64) - Pr.view(np.int32).astype(np.int64))
+            parity["transition_max_ulp_vs_reference_f32"] = int(du.max())
         except Exception as e:  # the baseline is informational; never fail the run on it
-            cpu = {"value": None, "unit": "GB/s", "cores": os.cpu_count(), "kind": "reference",
+            cpu = {"value": None, "unit": "GB/s", "cores": host_cores(), "kind": "reference",
                    "sample": f"unavailable: {e}"}
+    if parity is not None:
+        parity.update(fp64)
 
     if rank == 0:
+        summary = {
+            "f32_ms": round(t_ms, 4), "f32_frac_of_gather_floor": round(floor_ms / per_launch_ms, 4),
+            "bit_identical_to_reference": parity.get("bit_identical_to_reference") if parity else None,
+            "bf16_speedup": forms.get("bf16", {}).get("speedup_vs_f32"),
+            "bf16_rel_fro_err": forms.get("bf16", {}).get("rel_fro_err_vs_fp64"),
+            "f16_speedup": forms.get("f16", {}).get("speedup_vs_f32"),
+            "f16_rel_fro_err": forms.get("f16", {}).get("rel_fro_err_vs_fp64"),
+            "fwd_bwd_over_fwd": fwd_bwd["fwd_bwd_over_fwd"] if fwd_bwd else None,
+            "batched_speedup": batched["speedup"] if batched else None,
+            "batched_bit_identical_to_reference": batched.get("bit_identical_to_reference") if batched else None,
+            "e2e_ms": e2e["ms_per_step"] if e2e else None,
+        }
         line = {
             "metric": METRIC, "value": round(value, 3), "unit": "GB/s", "n_gpus": world, "steps": args.steps,
             "warmup": warmup, "ms_per_step": round(t_ms, 4), "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32",
-            "data": "synthetic (seeded 10-component 50-D mixture; kNN computed on device, untimed)",
-            "config": {"workload": "diffusion 500k cells k=30 64 cols 16 steps (FP32 plain, row-normalised)",
-                       "cells": n, "k": K_NN, "features": F, "diffusion_steps": T, "nnz": nnz,
-                       "bytes_per_spmm_step": B32, "l2": "flushed (256 MiB write) before every timed step",
-                       "parallelism": f"replicas x{world}"},
+            "data": "synthetic (seeded 10-component 50-D mixture; kNN by this library's scl_knn, untimed)",
+            "config": workload_config(world),
+            "graph": {"nnz": nnz, "bytes_per_spmm_step": B32, **build},
             "gpu_launches": args.steps * (T + 1),
             "roofline": {"bound": "hbm", "achieved": round(achieved, 2), "peak": peak, "unit": "GB/s",
                          "frac": round(achieved / peak, 4), "traffic": profiled_traffic("spmm_row_f32_500k"),
                          "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum per launch, "
                                            "profiles/spmm_row_f32_500k.md", "peak_kind": peak_kind,
-                         "kernel": f"SpMM plan kind {tuned['kind']} stage {tuned['stage']} "
-                                   "(kind 4 = k_spmm_row, kind 7 = k_spmm_flow)",
+                         "kernel": f"SpMM plan kind {tuned['kind']} stage {tuned['stage']}",
                          "per_launch_ms": round(per_launch_ms, 5),
                          "gather_floor_ms": round(floor_ms, 5),
                          "frac_of_gather_floor": round(floor_ms / per_launch_ms, 4),
-                         "gather_floor_note": "time of a kernel that only gathers the same 26.1M 256-byte X rows "
+                         "gather_floor_note": "time of a kernel that only gathers the same 256-byte X rows "
                                               "in the same order at full occupancy (scl_gpu_graph_gather_floor)"},
+            "parity": parity,
             "forms": forms,
             "fwd_bwd_ms": fwd_bwd["fwd_bwd_ms"] if fwd_bwd else None,
             "fwd_bwd": fwd_bwd,
@@ -725,13 +934,10 @@ def main():
             "impute": impute,
             "walks": walks,
             "knn": knn,
-            "graph_build_ms": round(build_ms, 3),
-            "reorder_ms": round(reorder_ms, 3),
-            "reorder_cc_rounds": cc_rounds,
-            "knn_harness_s": round(t_knn, 2),
             "e2e": e2e,
             "cpu_baseline": cpu,
             "clocks": clk.summary(),
+            "summary": summary,
         }
         print(json.dumps(line), flush=True)
     if dist is not None:

@@ -498,12 +498,6 @@ SCL_EXPORT scl_error_t scl_diffusion_magic_impute(scl_sparse_t transition, scl_r
   SCL_API_CATCH
 }
 
-#define SCL_NOT_IMPLEMENTED(name)                                                            \
-  do {                                                                                       \
-    sclabi::set_last_error(SCL_ERROR_NOT_IMPLEMENTED, name ": not implemented in the B200 build"); \
-    return SCL_ERROR_NOT_IMPLEMENTED;                                                        \
-  } while (0)
-
 SCL_EXPORT scl_error_t scl_diffusion_compute_dpt(scl_sparse_t transition, scl_index_t root_cell,
                                                  scl_real_t* pseudotime, scl_size_t n_nodes, scl_index_t max_iter,
                                                  scl_real_t tol) {

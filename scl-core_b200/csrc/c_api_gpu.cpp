@@ -250,6 +250,11 @@ SCL_EXPORT scl_error_t scl_gpu_graph_reorder(scl_gpu_graph_t graph, int mode, vo
   cudaStream_t s = as_stream(stream);
   if (mode == 0) {
     graph->reo.reset();
+    // grouped-row plans run on the reordered structure only
+    for (auto it = graph->plans.begin(); it != graph->plans.end();) {
+      if (it->second.kind == 13) it = graph->plans.erase(it);
+      else ++it;
+    }
   } else {
     auto r = std::make_unique<Reordered>();
     build_reorder(graph->g.view(), *r, s);
@@ -292,7 +297,11 @@ SCL_EXPORT scl_error_t scl_gpu_graph_set_plan(scl_gpu_graph_t graph, int64_t n_f
                     ((kind == 5 || kind == 6) && dtype_size(graph->store_type) == 2 && bytes == 16 &&
                      n_features == (int64_t)group * vec &&
                      ((group == 8 && (stage == 2 || stage == 4 || stage == 8)) ||
-                      (group == 16 && (stage == 4 || stage == 8 || stage == 16)))),
+                      (group == 16 && (stage == 4 || stage == 8 || stage == 16)))) ||
+                    (kind == 13 && group == 32 && bytes == 16 && graph->store_type != kF64 &&
+                     grouped_rows_per_warp(n_features, graph->store_type) > 0 &&
+                     (stage == 4 || stage == 8 ||
+                      (stage == 16 && grouped_rows_per_warp(n_features, graph->store_type) < 4))),
                 SCL_ERROR_INVALID_ARGUMENT, "invalid kernel kind / stage for this shape");
     SpmmPlan p;
     p.group = group;
@@ -577,6 +586,22 @@ SCL_EXPORT scl_error_t scl_gpu_spmm_inject_stall(int64_t warp, void* stream) {
   SCL_API_CATCH
 }
 
+SCL_EXPORT scl_error_t scl_gpu_residual_fp64(const void* X, scl_dtype_t x_dtype, const double* X_ref,
+                                             int64_t n_rows, int64_t n_features, double rel_floor, double* out,
+                                             void* stream) {
+  SCL_API_CHECK_NULL(X, "Matrix X is null");
+  SCL_API_CHECK_NULL(X_ref, "Reference matrix is null");
+  SCL_API_CHECK_NULL(out, "Output pointer is null");
+  SCL_API_CHECK(n_rows > 0 && n_features > 0, SCL_ERROR_INVALID_ARGUMENT, "Dimensions must be positive");
+  SCL_API_CHECK(rel_floor >= 0.0, SCL_ERROR_INVALID_ARGUMENT, "rel_floor must be non-negative");
+  SCL_API_TRY
+  const DType t = checked_dtype(x_dtype);
+  SCL_REQUIRE(is_float_dtype(t), SCL_ERROR_TYPE_MISMATCH, "X must be a float dtype");
+  residual_fp64(X, t, X_ref, n_rows * n_features, rel_floor, out, as_stream(stream));
+  SCL_API_RETURN_OK;
+  SCL_API_CATCH
+}
+
 SCL_EXPORT scl_error_t scl_gpu_graph_gather_floor(scl_gpu_graph_t graph, int64_t n_features, scl_dtype_t dtype,
                                                   int reps, double* ms, void* stream) {
   SCL_API_CHECK_NULL(graph, "Graph is null");
@@ -624,7 +649,19 @@ SCL_EXPORT scl_error_t scl_gpu_graph_autotune(scl_gpu_graph_t graph, int64_t n_f
   SCL_CUDA(cudaMemsetAsync(X.p, 0, blk, s));
   a.X = X.p;
   a.Y = Y.p;
-  const std::vector<SpmmPlan> cands = candidate_plans(n_features, t, X.p, Y.p, t);
+  std::vector<SpmmPlan> cands = candidate_plans(n_features, t, X.p, Y.p, t);
+  if (graph->reo && t == kF32 && grouped_fits(n_features, t, X.p, Y.p, t)) {
+    // grouped-row kernel on the permuted structure: the same sequential chains as kind 4
+    for (int u : {4, 8, 16}) {
+      if (u == 16 && grouped_rows_per_warp(n_features, t) == 4) continue;
+      SpmmPlan p;
+      p.group = 32;
+      p.vec = 16 / (int)dtype_size(t);
+      p.kind = 13;
+      p.stage = u;
+      cands.push_back(p);
+    }
+  }
   cudaEvent_t e0, e1;
   SCL_CUDA(cudaEventCreate(&e0));
   SCL_CUDA(cudaEventCreate(&e1));
@@ -632,12 +669,16 @@ SCL_EXPORT scl_error_t scl_gpu_graph_autotune(scl_gpu_graph_t graph, int64_t n_f
   SpmmPlan best_plan = cands.front();
   const int r = std::max(reps, 1);
   try {
+    auto step = [&](const SpmmPlan& p) {
+      if (graph->reo) spmm_reordered(*graph->reo, a, p, s);
+      else spmm_with_plan(a, p, s);
+    };
     for (const SpmmPlan& p : cands) {
-      spmm_with_plan(a, p, s);  // warm-up (also validates the shape)
+      step(p);  // warm-up (also validates the shape and builds any layout it needs)
       std::vector<float> ts(r);
       for (int k = 0; k < r; ++k) {
         SCL_CUDA(cudaEventRecord(e0, s));
-        spmm_with_plan(a, p, s);
+        step(p);
         SCL_CUDA(cudaEventRecord(e1, s));
         SCL_CUDA(cudaEventSynchronize(e1));
         SCL_CUDA(cudaEventElapsedTime(&ts[k], e0, e1));

@@ -8,6 +8,7 @@
 
 #include <cstddef>
 #include <cstdint>
+#include <memory>
 #include <stdexcept>
 #include <string>
 #include <vector>
@@ -184,9 +185,34 @@ void spmm_bulk_inject_stall(int64_t warp, cudaStream_t s);
 void diffuse(const CsrView& g, const void* X0, DType xtype, void* Y, DType ytype, DType mtype, int64_t F,
              int64_t steps, cudaStream_t s, const SpmmPlan* plan = nullptr);
 
+// ---- grouped-row layout (plan kind 13, spmm_grouped.cu) ------------------------------
+// The rows of a structure taken C at a time (C = 32 lanes / (row bytes / 16)),
+// each group's entries stored as blocks of 32 slots: slot s of block b holds
+// entry b*(32/C) + s%(32/C) of row gC + s/(32/C), padding past a row's end.
+struct Grouped {
+  int C = 0;
+  int64_t n_groups = 0, n_blocks = 0;
+  DevBuf lens;   // int32[n]          row lengths
+  DevBuf boff;   // int64[n_groups+1] first block of each group
+  DevBuf gidx;   // int32[n_blocks*32] column ids (0 in padding)
+  DevBuf gmap;   // int32[n_blocks*32] entry position in the source structure, -1 = padding
+  DevBuf gval;   // vtype[n_blocks*32] values (0 in padding)
+  DType vtype = kF32;
+  uint64_t values_version = 0;  // source values version the slots were filled from
+};
+// Rows per group for this row pitch (0 when the pitch is not 128/256/512 bytes).
+int grouped_rows_per_warp(int64_t F, DType xtype);
+bool grouped_fits(int64_t F, DType xtype, const void* X, const void* Y, DType ytype);
+void build_grouped(const CsrView& r, int C, Grouped& gr, cudaStream_t s);
+void grouped_values(const void* vals, DType t, uint64_t version, Grouped& gr, cudaStream_t s);
+// One Y = P X (a.X, a.Y, a.row_map, a.n_rows, a.F, dtypes) on the grouped layout with
+// U gathers in flight per lane (4, 8 or 16); same bits as the sequential-chain kernels.
+void spmm_grouped(const Grouped& gr, const SpmmArgs& a, int U, cudaStream_t s);
+
 // ---- locality reordering ------------------------------------------------------
-// Rows grouped by connected component (stable within a component); entries of
-// each row keep their original order, so diffusion results are bit-identical.
+// Rows grouped by connected component, longest rows first inside a component
+// (stable among equal lengths); entries of each row keep their original order,
+// so diffusion results are bit-identical.
 struct Reordered {
   int64_t n = 0, nnz = 0;
   int cc_rounds = 0;
@@ -198,7 +224,14 @@ struct Reordered {
   DevBuf values;   // vtype[nnz] values gathered through emap
   DType vtype = kF32;
   bool values_ok = false;
+  uint64_t values_version = 0;  // bumped whenever `values` is rewritten
+  // grouped layouts of the permuted structure for C = 1, 2, 4 rows per warp (built on first use)
+  mutable std::unique_ptr<Grouped> grouped[3];
 };
+// The grouped layout for C rows per warp with current values (built or refreshed on demand).
+const Grouped& reordered_grouped(const Reordered& r, int C, cudaStream_t s);
+// One SpMM step on the permuted structure with `plan` (kind 13 runs on the grouped layout).
+void spmm_reordered(const Reordered& r, SpmmArgs a, const SpmmPlan& plan, cudaStream_t s);
 void build_reorder(const CsrView& g, Reordered& r, cudaStream_t s);
 void reorder_values(const void* vals, DType t, Reordered& r, cudaStream_t s);
 // Y = P^steps X0 through the permuted structure: X0 is gathered into permuted
@@ -306,6 +339,13 @@ void diffusion_map(const CsrView& P, void* out, int K, int64_t n_iter, cudaStrea
 // Diffusion distance: D (n x n) = pairwise L2 distances between the rows of
 // P^steps (n <= 1000) or its columns (n > 1000), as the reference's two branches.
 void diffusion_distance(const CsrView& P, void* D, int64_t steps, cudaStream_t s);
+
+// FP64 error of a block X (f32/f64/bf16/f16, `total` elements) against an FP64
+// reference R, reduced on the device in a fixed order (residual.cu). Writes to
+// host memory: relative Frobenius error, max |x-r|/max(|r|, rel_floor), max
+// |x-r|, ||r||. Synchronises s.
+void residual_fp64(const void* X, DType xt, const double* R, int64_t total, double rel_floor, double* out_host,
+                   cudaStream_t s);
 
 // dL/dP in CSR order from its CSC-order accumulator.
 void scatter_adjoint_entries(const Adjoint& adj, const void* gPt, DType t, void* gP, cudaStream_t s);

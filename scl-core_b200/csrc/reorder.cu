@@ -67,10 +67,15 @@ __global__ void k_cc_jump(int32_t* __restrict__ L, int64_t n) {
   }
 }
 
-__global__ void k_label_keys(const int32_t* __restrict__ L, int64_t n, uint64_t* __restrict__ keys,
-                             uint32_t* __restrict__ vals) {
+// Sort key of row i: its component label, then its length, longest first
+// (lengths saturate at 2^20 - 1; ties keep the original order).
+constexpr int kLenBits = 20;
+__global__ void k_label_keys(const int32_t* __restrict__ L, const int64_t* __restrict__ indptr, int64_t n,
+                             uint64_t* __restrict__ keys, uint32_t* __restrict__ vals) {
+  constexpr uint64_t kLenMax = (1ull << kLenBits) - 1;
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
-    keys[i] = (uint64_t)(uint32_t)L[i];
+    const uint64_t len = (uint64_t)(indptr[i + 1] - indptr[i]);
+    keys[i] = ((uint64_t)(uint32_t)L[i] << kLenBits) | (kLenMax - (len < kLenMax ? len : kLenMax));
     vals[i] = (uint32_t)i;
   }
 }
@@ -167,9 +172,10 @@ void build_reorder(const CsrView& g, Reordered& r, cudaStream_t s) {
   }
   r.cc_rounds = rounds;
   DevBuf keys(n * 8, s), vals(n * 4, s), keys2(n * 8, s), vals2(n * 4, s);
-  k_label_keys<<<nblocks(n, 256), 256, 0, s>>>(L.as<int32_t>(), n, keys.as<uint64_t>(), vals.as<uint32_t>());
+  k_label_keys<<<nblocks(n, 256), 256, 0, s>>>(L.as<int32_t>(), g.indptr, n, keys.as<uint64_t>(),
+                                               vals.as<uint32_t>());
   radix_sort_pairs(keys.as<uint64_t>(), vals.as<uint32_t>(), keys2.as<uint64_t>(), vals2.as<uint32_t>(), n,
-                   bits_for(std::max<int64_t>(n, 2)), s);
+                   bits_for(std::max<int64_t>(n, 2)) + kLenBits, s);
   r.perm = DevBuf(n * 4, s);
   r.iperm = DevBuf(n * 4, s);
   DevBuf lens((n + 1) * 8, s);
@@ -200,6 +206,37 @@ void reorder_values(const void* vals, DType t, Reordered& r, cudaStream_t s) {
     SCL_CUDA(cudaGetLastError());
   }
   r.values_ok = true;
+  ++r.values_version;
+}
+
+const Grouped& reordered_grouped(const Reordered& r, int C, cudaStream_t s) {
+  SCL_REQUIRE(C == 1 || C == 2 || C == 4, kErrInvalidArgument, "rows per group must be 1, 2 or 4");
+  SCL_REQUIRE(r.values_ok, kErrInternal, "reordered values are stale");
+  const int slot = C == 1 ? 0 : (C == 2 ? 1 : 2);
+  std::unique_ptr<Grouped>& gp = r.grouped[slot];
+  if (!gp) {
+    CsrView v;
+    v.n_rows = r.n;
+    v.n_cols = r.n;
+    v.nnz = r.nnz;
+    v.indptr = r.indptr.as<int64_t>();
+    v.indices = r.indices.as<int32_t>();
+    auto g = std::make_unique<Grouped>();
+    build_grouped(v, C, *g, s);
+    gp = std::move(g);
+  }
+  if (gp->values_version != r.values_version || gp->vtype != r.vtype)
+    grouped_values(r.values.p, r.vtype, r.values_version, *gp, s);
+  return *gp;
+}
+
+void spmm_reordered(const Reordered& r, SpmmArgs a, const SpmmPlan& plan, cudaStream_t s) {
+  if (plan.kind == 13) {
+    const Grouped& gr = reordered_grouped(r, grouped_rows_per_warp(a.F, a.xtype), s);
+    a.values = gr.gval.p;
+    return spmm_grouped(gr, a, plan.stage, s);
+  }
+  spmm_with_plan(a, plan, s);
 }
 
 void diffuse_reordered(const Reordered& r, const void* X0, DType xtype, void* Y, DType ytype, int64_t F,
@@ -248,7 +285,7 @@ void diffuse_reordered(const Reordered& r, const void* X0, DType xtype, void* Y,
     a.Y = dst;
     a.ytype = ot;
     const SpmmPlan plan = plan_in ? *plan_in : default_spmm_plan(F, mtype, src, dst, ot);
-    spmm_with_plan(a, plan, s);
+    spmm_reordered(r, a, plan, s);
     src = dst;
   }
 }

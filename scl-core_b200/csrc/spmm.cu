@@ -1916,6 +1916,8 @@ std::vector<SpmmPlan> candidate_plans(int64_t F, DType xtype, const void* X, con
 
 void spmm_with_plan(const SpmmArgs& a, const SpmmPlan& plan, cudaStream_t s) {
   if (a.n_rows <= 0 || a.F <= 0) return;
+  SCL_REQUIRE(plan.kind != 13, kErrInvalidArgument,
+              "plan kind 13 (grouped rows) runs on a reordered graph only (scl_gpu_graph_reorder)");
   SCL_REQUIRE(plan.group >= 1 && plan.group <= 32 && (plan.group & (plan.group - 1)) == 0, kErrInvalidArgument,
               "lane-group size must be a power of two in [1, 32]");
   SCL_REQUIRE(plan.kind == 0 || plan.kind == 2 || plan.kind == 3 || plan.kind == 4 || plan.kind == 5 ||

@@ -8,6 +8,6 @@ torch callers live in :mod:`scl.gpu`.
 from . import _bindings  # noqa: F401  (binds every registered C function)
 from .core import (BlockStrategy, CsrMatrix, IndexType, RealType, SCLError, check_error, get_library,  # noqa: F401
                    get_precision, set_precision)
-from . import algebra, diffusion, gpu, impute, neighbors, synthetic, workloads  # noqa: F401
+from . import algebra, diffusion, gpu, impute, neighbors, synthetic  # noqa: F401
 
 __version__ = "1.0.0"

@@ -273,6 +273,26 @@ class GpuGraph:
             pass
 
 
+def residual_fp64(X, X_ref, rel_floor: float = 1e-3, variant: str = "f32_i32", stream=None) -> dict:
+    """FP64 error of a device block X (f32/f64/bf16/f16) against an FP64 device
+    block X_ref of the same shape, reduced on the device (scl_gpu_residual_fp64).
+
+    Returns rel_fro = ||X - X_ref|| / ||X_ref||, max_rel = max |x - r| /
+    max(|r|, rel_floor), max_abs and ref_fro. Synchronises the stream."""
+    torch = _torch()
+    if X.shape != X_ref.shape or X_ref.dtype != torch.float64:
+        raise ValueError("X_ref must be float64 with X's shape")
+    X = X.contiguous()
+    X_ref = X_ref.contiguous()
+    n = X.shape[0]
+    F = X.numel() // max(n, 1)
+    lib = get_library(variant)
+    out = (ctypes.c_double * 4)()
+    check_error(lib.scl_gpu_residual_fp64(_ptr(X), dtype_code(X.dtype), _ptr(X_ref), int(n), int(F),
+                                          float(rel_floor), out, _stream_ptr(stream)), "residual_fp64", lib)
+    return {"rel_fro": out[0], "max_rel": out[1], "max_abs": out[2], "ref_fro": out[3]}
+
+
 class GpuBatch:
     """Many independent graphs diffused together in one persistent, CUDA-graph
     replayed launch (scl_gpu_batch_*). Blocks are the graphs' n_b x F blocks

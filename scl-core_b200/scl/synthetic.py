@@ -9,8 +9,10 @@ Euclidean distances) in the same list format as scl-core's kNN
 Two kNN builders:
   * ``knn_exact``  — FP64 NumPy, ties broken by (distance, index); used for the
                      parity cases, where both sides must read identical lists.
-  * ``knn_device`` — FP32 torch on a CUDA device, for the 200k/500k-cell
-                     benchmark graphs (an input generator, not a measured step).
+  * ``knn_device`` — FP32 torch on a CUDA device: the kNN lists of the
+                     benchmark's reference arm, which runs scl-core's own CPU
+                     code and loads none of this library (an input generator,
+                     not a measured step).
 """
 from __future__ import annotations
 

@@ -2,8 +2,10 @@
 scl-core's own scl_diffusion_diffusion_map_embedding (compiled from the
 reference sources and shipped with the tests). The GPU reduces the
 Gram-Schmidt dot products in FP64 blocks where the reference sums
-sequentially, and its starting cosines come from CUDA's cos/sin, so the two
-agree to a tolerance, not bit for bit; both outputs are orthonormal."""
+sequentially in the value type, and its starting cosines come from CUDA's
+cos/sin, so the two agree to a tolerance, not bit for bit; both outputs are
+orthonormal. Against scl-core's FP64 build the FP32 GPU result is within 1e-5
+of the largest entry, and no further from it than scl-core's own FP32 build."""
 import numpy as np
 import pytest
 import scipy.sparse as sp
@@ -26,7 +28,7 @@ def _graph(n, dt, idt, seed):
     return m, P
 
 
-@pytest.mark.parametrize("dt,idt,tol", [(np.float32, np.int32, 2e-3), (np.float64, np.int64, 1e-8)])
+@pytest.mark.parametrize("dt,idt,tol", [(np.float32, np.int32, 1e-6), (np.float64, np.int64, 1e-8)])
 @pytest.mark.parametrize("n,K,n_iter", [(200, 3, 10), (400, 6, 50), (300, 1, 0)])
 def test_diffusion_map_matches_reference(dt, idt, tol, n, K, n_iter):
     variant = "f32_i32" if dt == np.float32 else "f64_i64"
@@ -38,6 +40,14 @@ def test_diffusion_map_matches_reference(dt, idt, tol, n, K, n_iter):
         pytest.skip("reference library not shipped with the tests")
     want = ref.RefLib(variant).diffusion_map(P.indptr, P.indices, P.data, n, K, n_iter)
     np.testing.assert_allclose(got, want, atol=tol, rtol=0)
+    if dt == np.float32 and ref.available("f64_i64"):
+        # whose error: both FP32 results against scl-core's FP64 build of the same P
+        want64 = ref.RefLib("f64_i64").diffusion_map(P.indptr.astype(np.int64), P.indices.astype(np.int64),
+                                                     P.data.astype(np.float64), n, K, n_iter)
+        err_gpu = np.abs(got - want64).max()
+        err_ref32 = np.abs(want - want64).max()
+        assert err_gpu <= 1e-5 * np.abs(want64).max()
+        assert err_gpu <= 2.0 * err_ref32 + 1e-7
 
 
 def test_diffusion_map_errors():

@@ -254,6 +254,18 @@ SCL_EXPORT scl_error_t scl_gpu_residual_fp64(const void* X, scl_dtype_t x_dtype,
                                              int64_t n_rows, int64_t n_features, double rel_floor, double* out,
                                              void* stream);
 
+/* Which kernel scl_knn / scl_knn_simple run. No counterpart in scl-core
+ * (scl/kernel/neighbors.hpp:319-478 has one CPU loop); both kernels replay
+ * that loop's skip test, distance arithmetic and heap rules and return the
+ * same bits.
+ *   kernel 0 (default): tensor-core filter. BF16 inner products on tcgen05
+ *     bound every distance; only candidates that can reach the heap are
+ *     recomputed exactly. Any feature count, any k.
+ *   kernel 1: every distance computed exactly on CUDA cores; up to 128
+ *     features and k up to 64.
+ * The choice is process-wide. previous (may be null) receives the old one. */
+SCL_EXPORT scl_error_t scl_gpu_knn_set_kernel(int kernel, int* previous);
+
 /* Diffusion that allocates no device memory. No counterpart in scl-core.
  *
  * For callers that cannot allocate GPU memory while they run: a framework

@@ -353,8 +353,7 @@ DenseSamples dense_samples(scl_sparse_matrix& m, Stats& st) {
   ds.s = library_stream(current_device());
   ds.n = m.primary_dim();
   const int64_t d = m.secondary_dim();
-  SCL_REQUIRE(d >= 1 && d <= knn_max_features(), SCL_ERROR_INVALID_ARGUMENT,
-              "kNN on the device takes 1 to 128 features");
+  SCL_REQUIRE(d >= 1 && d <= 0x7fffffff, SCL_ERROR_INVALID_ARGUMENT, "Dimensions must be positive");
   ds.d = (int)d;
   auto mir = device_graph(m, ds.s, st.h2d);
   ds.X = DevBuf(std::max<int64_t>(ds.n * d, 1) * sizeof(Real), ds.s);
@@ -366,7 +365,7 @@ void knn_host(scl_sparse_matrix& m, const Real* norms, size_t n_samples, size_t 
   Stats st;
   SCL_REQUIRE(n_samples == (size_t)m.primary_dim(), SCL_ERROR_DIMENSION_MISMATCH,
               "kNN: n_samples must equal the matrix's primary dimension");
-  SCL_REQUIRE(k >= 1 && k <= 64, SCL_ERROR_INVALID_ARGUMENT, "kNN on the device takes k from 1 to 64");
+  SCL_REQUIRE(k >= 1, SCL_ERROR_INVALID_ARGUMENT, "Dimensions must be positive");
   DenseSamples ds = dense_samples(m, st);
   DevBuf nd(std::max<int64_t>(ds.n, 1) * sizeof(Real), ds.s);
   if (norms) {

@@ -602,6 +602,16 @@ SCL_EXPORT scl_error_t scl_gpu_residual_fp64(const void* X, scl_dtype_t x_dtype,
   SCL_API_CATCH
 }
 
+SCL_EXPORT scl_error_t scl_gpu_knn_set_kernel(int kernel, int* previous) {
+  SCL_API_CHECK(kernel == 0 || kernel == 1, SCL_ERROR_INVALID_ARGUMENT,
+                "kNN kernel must be 0 (tensor cores) or 1 (CUDA cores)");
+  SCL_API_TRY
+  const int prev = knn_set_kernel(kernel);
+  if (previous) *previous = prev;
+  SCL_API_RETURN_OK;
+  SCL_API_CATCH
+}
+
 SCL_EXPORT scl_error_t scl_gpu_graph_gather_floor(scl_gpu_graph_t graph, int64_t n_features, scl_dtype_t dtype,
                                                   int reps, double* ms, void* stream) {
   SCL_API_CHECK_NULL(graph, "Graph is null");

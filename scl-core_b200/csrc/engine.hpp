@@ -314,12 +314,17 @@ void knn_impute(const CsrView& m, bool csr, int64_t n_cells, int64_t n_genes, co
 // Y (A.n_rows x K) <- alpha A X + beta Y, X: A.n_cols x K (scl_algebra_spmm's arithmetic).
 void algebra_spmm(const CsrView& A, const void* X, int64_t K, void* Y, double alpha, double beta, cudaStream_t s);
 
-// Brute-force kNN (knn.cu) over the rows of a dense n x d block (d <= 128,
-// k <= 64): indices (kI32/kI64) and sqrt distances [n, k], ascending, missing
-// slots (inf, -1); and the squared row norms as sequential fma chains.
+// Brute-force kNN over the rows of a dense n x d block: indices (kI32/kI64)
+// and sqrt distances [n, k], ascending, missing slots (inf, -1); and the
+// squared row norms as sequential fma chains. knn_dense runs the tensor-core
+// filter (knn_tc.cu, any d and k) unless knn_set_kernel(1) selected the
+// CUDA-core kernel (knn.cu, d <= 128, k <= 64); both give the same bits.
 int knn_max_features();
+int knn_set_kernel(int kernel);  // returns the previous choice
 void knn_dense(const void* X, const void* norms, DType t, int64_t n, int d, int k, void* idx, DType it, void* dist,
                cudaStream_t s);
+void knn_tensor(const void* X, const void* norms, DType t, int64_t n, int d, int k, void* idx, DType it, void* dist,
+                cudaStream_t s);
 void row_norms_dense(const void* X, DType t, int64_t n, int d, void* out, cudaStream_t s);
 
 // Vector walks (walks.cu). walk_linear: x <- c_x x + c_p P x, `steps` times

@@ -1,5 +1,7 @@
-// Brute-force k-nearest neighbours (scl/kernel/neighbors.hpp:302-478): the
-// graph-building step before the transition matrix.
+// Brute-force k-nearest neighbours on CUDA cores (scl/kernel/neighbors.hpp:302-478):
+// the graph-building step before the transition matrix. The default search is
+// the tensor-core filter of knn_tc.cu; this kernel computes every distance
+// exactly and stays selectable (knn_set_kernel) for comparison.
 //
 // The samples (the handle's primary rows) are made dense on the device, n x d
 // with d <= 128 features. Every query walks every candidate j in increasing
@@ -391,12 +393,25 @@ void knn_typed(const T* X, const T* norms, int64_t n, int d, int k, IT* idx, T* 
 
 int knn_max_features() { return kKnnMaxD; }
 
+namespace {
+int g_knn_kernel = 0;  // 0: tensor-core filter (knn_tc.cu), 1: the warp-specialised CUDA-core kernel above
+}
+
+int knn_set_kernel(int kernel) {
+  SCL_REQUIRE(kernel == 0 || kernel == 1, kErrInvalidArgument, "kNN kernel must be 0 (tensor cores) or 1 (CUDA cores)");
+  const int prev = g_knn_kernel;
+  g_knn_kernel = kernel;
+  return prev;
+}
+
 void knn_dense(const void* X, const void* norms, DType t, int64_t n, int d, int k, void* idx, DType it, void* dist,
                cudaStream_t s) {
-  SCL_REQUIRE(d >= 1 && d <= kKnnMaxD, kErrInvalidArgument, "kNN on the device takes 1 to 128 features");
-  SCL_REQUIRE(k >= 1 && k <= 64, kErrInvalidArgument, "kNN on the device takes k from 1 to 64");
+  SCL_REQUIRE(d >= 1 && k >= 1, kErrInvalidArgument, "Dimensions must be positive");
   SCL_REQUIRE(n < (int64_t)0x7fffffff, kErrInvalidArgument, "kNN sample count exceeds the int32 range");
   if (n == 0) return;
+  if (g_knn_kernel == 0) return knn_tensor(X, norms, t, n, d, k, idx, it, dist, s);
+  SCL_REQUIRE(d <= kKnnMaxD, kErrInvalidArgument, "the CUDA-core kNN kernel takes 1 to 128 features");
+  SCL_REQUIRE(k <= 64, kErrInvalidArgument, "the CUDA-core kNN kernel takes k from 1 to 64");
   if (t == kF32) {
     if (it == kI32)
       return knn_typed<float, int32_t>(static_cast<const float*>(X), static_cast<const float*>(norms), n, d, k,

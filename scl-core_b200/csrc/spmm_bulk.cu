@@ -298,6 +298,9 @@ k_spmm_gather4(const __grid_constant__ CUtensorMap xmap, const int64_t* __restri
   }
 }
 
+}  // namespace
+
+// The driver's tensor-map encoder, looked up once (shared with the kNN operand maps).
 PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
   static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
   static std::once_flag once;
@@ -311,6 +314,8 @@ PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
   SCL_REQUIRE(fn != nullptr, kErrFeatureUnavailable, "cuTensorMapEncodeTiled is not available from the driver");
   return fn;
 }
+
+namespace {
 
 // X as a row-major [rows, F] tensor whose box is one row of F elements.
 CUtensorMap row_gather_map(const void* X, DType t, int64_t rows, int64_t F) {

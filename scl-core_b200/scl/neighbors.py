@@ -34,3 +34,16 @@ def knn(mat: CsrMatrix, k: int, norms: np.ndarray = None):
         check_error(lib.scl_knn(mat.handle, nr.ctypes.data_as(ctypes.POINTER(lib.real_type)), n, int(k), PI, PD),
                     "knn", lib)
     return idx, dist
+
+
+def set_kernel(kernel: int, mat_or_variant="f32_i32") -> int:
+    """Choose the kernel scl_knn runs in one library variant (scl_gpu_knn_set_kernel):
+    0 = tensor-core filter (default; any feature count and k), 1 = every distance
+    on CUDA cores (up to 128 features, k up to 64). Both return the same bits.
+    Returns the previous choice."""
+    from ._bindings._loader import get_library
+
+    lib = mat_or_variant.lib if isinstance(mat_or_variant, CsrMatrix) else get_library(mat_or_variant)
+    prev = ctypes.c_int(0)
+    check_error(lib.scl_gpu_knn_set_kernel(int(kernel), ctypes.byref(prev)), "knn_set_kernel", lib)
+    return prev.value

@@ -73,7 +73,88 @@ def test_knn_errors():
     assert lib.scl_knn(m.handle, None, 10, 3, PI, PD) == 4
     assert lib.scl_knn(m.handle, PN, 0, 3, PI, PD) == 10
     assert lib.scl_knn(m.handle, PN, 9, 3, PI, PD) == 11  # n_samples must be the row count
-    assert lib.scl_knn(m.handle, PN, 10, 65, PI, PD) == 10  # this build: k <= 64
+    # the CUDA-core kernel is limited to k <= 64 and 128 features; the default is not
     wide, _ = _matrix(10, 129, np.float32, np.int32)
-    assert lib.scl_knn_simple(wide.handle, 10, 3, PI, PD) == 10  # this build: <= 128 features
+    prev = scl.neighbors.set_kernel(1, m)
+    try:
+        assert lib.scl_knn(m.handle, PN, 10, 65, PI, PD) == 10
+        assert lib.scl_knn_simple(wide.handle, 10, 3, PI, PD) == 10
+    finally:
+        scl.neighbors.set_kernel(prev, m)
+    big = np.zeros(10 * 65, np.int32), np.zeros(10 * 65, np.float32)
+    assert lib.scl_knn(m.handle, PN, 10, 65, big[0].ctypes.data_as(ctypes.POINTER(lib.index_type)),
+                       big[1].ctypes.data_as(ctypes.POINTER(lib.real_type))) == 0
+    assert lib.scl_knn_simple(wide.handle, 10, 3, PI, PD) == 0
+    assert lib.scl_gpu_knn_set_kernel(2, None) == 10
     assert lib.scl_neighbors_compute_norms(None, PN) == 4
+
+
+def _dense_case(n, d, dt, seed, dens=1.0, scale=1.0, dup=0):
+    rng = np.random.default_rng(seed)
+    Xd = rng.standard_normal((n, d)) * scale
+    if dens < 1.0:
+        Xd *= rng.random((n, d)) < dens
+    if dup:  # repeated rows: exact distance ties and zero distances
+        Xd[n - dup:] = Xd[:dup]
+    Xd = Xd.astype(dt)
+    X = sp.csr_matrix(Xd)
+    X.sort_indices()
+    idt = np.int32 if dt == np.float32 else np.int64
+    m = scl.CsrMatrix.wrap(X.indptr.astype(idt), X.indices.astype(idt), X.data.astype(dt), X.shape)
+    norms = np.einsum("ij,ij->i", Xd.astype(np.float64), Xd.astype(np.float64)).astype(dt)
+    return m, Xd, norms
+
+
+@pytest.mark.parametrize("dt", [np.float32, np.float64])
+@pytest.mark.parametrize("n,d,k,dens,scale,dup", [
+    (1000, 300, 20, 1.0, 1.0, 0),       # more than 128 features
+    (700, 1500, 15, 0.05, 3.0, 0),      # raw-expression-like width and sparsity
+    (600, 40, 100, 1.0, 1.0, 0),        # k above 64
+    (300, 17, 250, 1.0, 1.0, 0),        # k close to n
+    (40, 9, 64, 1.0, 1.0, 0),           # k >= n: unfilled slots (-1, inf)
+    (777, 64, 30, 1.0, 1.0, 200),       # duplicated rows: ties and zero distances
+    (513, 62, 30, 1.0, 1e12, 0),        # large magnitudes (norms near 1e26)
+    (900, 50, 30, 1.0, 1e-9, 0),        # tiny magnitudes
+    (257, 1, 5, 1.0, 1.0, 100),         # one feature, many ties
+])
+def test_knn_any_width_and_k(dt, n, d, k, dens, scale, dup):
+    """The tensor-core filter (default kernel) at sizes the CUDA-core kernel
+    does not take, against the restatement, bit for bit."""
+    m, Xd, norms = _dense_case(n, d, dt, seed=n + d + k, dens=dens, scale=scale, dup=dup)
+    gi, gd = scl.neighbors.knn(m, k, norms)
+    oi, od = port.knn_dense(Xd, norms, k)
+    np.testing.assert_array_equal(gd.view(np.uint8), od.view(np.uint8))
+    np.testing.assert_array_equal(gi.astype(np.int64), oi)
+
+
+@pytest.mark.parametrize("dt", [np.float32, np.float64])
+def test_knn_kernels_agree(dt):
+    """Tensor-core filter and CUDA-core kernel: the same bits, including with
+    norms that are not the rows' own (the filter's bound does not assume them)."""
+    m, Xd, norms = _dense_case(3000, 50, dt, seed=5, dup=300)
+    rng = np.random.default_rng(9)
+    odd = (norms * rng.uniform(0.5, 2.0, norms.shape)).astype(dt)
+    for nr in (norms, odd):
+        a = scl.neighbors.knn(m, 30, nr)
+        prev = scl.neighbors.set_kernel(1, m)
+        try:
+            b = scl.neighbors.knn(m, 30, nr)
+        finally:
+            scl.neighbors.set_kernel(prev, m)
+        np.testing.assert_array_equal(a[0], b[0])
+        np.testing.assert_array_equal(a[1].view(np.uint8), b[1].view(np.uint8))
+
+
+def test_knn_non_finite_values_replay_every_candidate():
+    """A non-finite sample switches the filter off; the result is still the
+    restatement's."""
+    m0, Xd, norms = _dense_case(400, 12, np.float32, seed=2)
+    Xd[7, 3] = np.inf
+    norms[7] = np.inf
+    X = sp.csr_matrix(Xd)
+    X.sort_indices()
+    m = scl.CsrMatrix.wrap(X.indptr.astype(np.int32), X.indices.astype(np.int32), X.data, X.shape)
+    gi, gd = scl.neighbors.knn(m, 10, norms)
+    oi, od = port.knn_dense(Xd, norms, 10)
+    np.testing.assert_array_equal(gd.view(np.uint8), od.view(np.uint8))
+    np.testing.assert_array_equal(gi.astype(np.int64), oi)

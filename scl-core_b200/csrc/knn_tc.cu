@@ -111,9 +111,12 @@ __device__ __forceinline__ bool mbar_wait(unsigned bar, unsigned parity, const v
                                           unsigned long long limit_ns) {
   if (mbar_try(bar, parity)) return true;
   const unsigned long long t0 = tc_ns();
+  unsigned sleep_ns = 32;
   while (!mbar_try(bar, parity)) {
     if (*abort_flag) return false;
     if (tc_ns() - t0 > limit_ns) return false;
+    __nanosleep(sleep_ns);  // a waiting role must not take issue slots from the epilogue warps
+    if (sleep_ns < 512) sleep_ns <<= 1;
   }
   return true;
 }
@@ -355,15 +358,63 @@ __device__ __forceinline__ void tmem_ld64(uint32_t taddr, float (&v)[64]) {
 
 // The four epilogue warps: thread tid owns query q0 + tid and tensor-memory
 // lane tid. Per tile it reads its 256 accumulator columns 64 at a time and
-// sets a bit for every candidate whose s_ij is above the query's threshold
-// for the tile (one compare per candidate). Then the warp lists its set bits
-// as (query, candidate) pairs in shared memory, chunk by chunk, computes their
-// exact distances with every lane busy (one pair per lane per round, the
-// candidate's norm and root norm fetched alongside), and each thread replays
-// its own pairs in increasing j: the reference's skip test against the
-// current heap top, the exact distance, the heap rules. A list that would
-// exceed the warp's capacity is computed and replayed first.
-template <class T, class IT>
+// keeps, in registers, a bit for every candidate whose s_ij is above the
+// query's threshold (one subtraction and one funnel shift per candidate).
+// The warp then lists its pairs in shared memory, lane after lane and each
+// lane's in increasing j, computes their exact distances with every lane
+// busy (one pair per lane per round, the candidate's root norm fetched
+// alongside), and each thread replays its own pairs in order: the
+// reference's skip test against the current heap top, the exact distance,
+// the heap rules. More pairs than the list holds are taken in windows.
+// P exact distances at once: the P dot products are independent fma chains
+// (each in feature order), so their row loads are in flight together.
+template <class T, int P>
+__device__ __forceinline__ void exact_dist_sq_multi(const T* const (&a)[P], const T* const (&b)[P], int dp,
+                                                    const T (&na)[P], const T (&nb)[P], T (&out)[P]) {
+  T dot[P];
+#pragma unroll
+  for (int q = 0; q < P; ++q) dot[q] = T(0);
+  if constexpr (sizeof(T) == 4) {
+#pragma unroll 2
+    for (int v = 0; v < dp / 4; ++v) {
+      float4 x[P], y[P];
+#pragma unroll
+      for (int q = 0; q < P; ++q) {
+        x[q] = __ldg(reinterpret_cast<const float4*>(a[q]) + v);
+        y[q] = __ldg(reinterpret_cast<const float4*>(b[q]) + v);
+      }
+#pragma unroll
+      for (int q = 0; q < P; ++q) {
+        dot[q] = tfma(x[q].x, y[q].x, dot[q]);
+        dot[q] = tfma(x[q].y, y[q].y, dot[q]);
+        dot[q] = tfma(x[q].z, y[q].z, dot[q]);
+        dot[q] = tfma(x[q].w, y[q].w, dot[q]);
+      }
+    }
+  } else {
+#pragma unroll 2
+    for (int v = 0; v < dp / 2; ++v) {
+      double2 x[P], y[P];
+#pragma unroll
+      for (int q = 0; q < P; ++q) {
+        x[q] = __ldg(reinterpret_cast<const double2*>(a[q]) + v);
+        y[q] = __ldg(reinterpret_cast<const double2*>(b[q]) + v);
+      }
+#pragma unroll
+      for (int q = 0; q < P; ++q) {
+        dot[q] = tfma(x[q].x, y[q].x, dot[q]);
+        dot[q] = tfma(x[q].y, y[q].y, dot[q]);
+      }
+    }
+  }
+#pragma unroll
+  for (int q = 0; q < P; ++q) {
+    const T ds = tfma(T(-2), dot[q], na[q] + nb[q]);
+    out[q] = ds < T(0) ? T(0) : ds;
+  }
+}
+
+template <class T, class IT, bool PER_CAND>
 __device__ __forceinline__ void tc_epilogue(const TcParams& p, const T* __restrict__ Xp, const T* __restrict__ norms,
                                             const T* __restrict__ snorms, const float* __restrict__ Rn,
                                             const float* __restrict__ Rmax, const float* __restrict__ Nmax,
@@ -382,14 +433,12 @@ __device__ __forceinline__ void tc_epilogue(const TcParams& p, const T* __restri
   const T si = live ? snorms[i] : T(0);
   const float Ri = live ? Rn[i] : 0.0f;
   // this warp's scratch: exact distances and root norms of listed pairs, the
-  // warp's query norms, per-chunk keep masks and list offsets, the pair list
+  // warp's query norms, the pair list, the tile's (R_j, |n_j|)
   unsigned char* ws = base + p.off_warp + (size_t)warp * p.warp_bytes;
   T* Dq = reinterpret_cast<T*>(ws);
   T* Sq = Dq + cap;
   T* QN = Sq + cap;
-  uint32_t* Msk = reinterpret_cast<uint32_t*>(QN + 32);  // [chunk][lane]
-  uint16_t* Off = reinterpret_cast<uint16_t*>(Msk + kChunks * 32);  // [chunk][lane]
-  uint16_t* Pq = Off + kChunks * 32;  // (lane << 8) | candidate within the tile
+  uint16_t* Pq = reinterpret_cast<uint16_t*>(QN + 32);  // listed pairs: (lane << 8) | candidate within the tile
   float2* RN = reinterpret_cast<float2*>(Pq + cap);  // the tile's (R_j, |n_j|) when thresholds are per candidate
   QN[lane] = ni;
   T* Hd;
@@ -448,33 +497,6 @@ __device__ __forceinline__ void tc_epilogue(const TcParams& p, const T* __restri
     maxd = Hd[0];
   };
 
-  // exact distances of the listed pairs (one per lane per round), then each
-  // thread replays its own pairs of chunks [c0, c1) in increasing j
-  auto flush = [&](int64_t tb, int c0, int c1, int listed) {
-    __syncwarp();
-    for (int r0 = 0; r0 < listed; r0 += 32) {
-      const int r = r0 + lane;
-      if (r < listed) {
-        const int e = Pq[r];
-        const int o = e >> 8;
-        const int64_t io = q0 + warp * 32 + o, j = tb + (e & 255);
-        Dq[r] = exact_dist_sq<T>(Xp + io * dp, Xp + j * dp, dp, QN[o], norms[j]);
-        Sq[r] = snorms[j];
-      }
-    }
-    __syncwarp();
-    for (int ch = c0; ch < c1; ++ch) {
-      uint32_t m = Msk[ch * 32 + lane];
-      int r = Off[ch * 32 + lane];
-      for (; m; m &= m - 1, ++r) {
-        const T nd = si - Sq[r];
-        if (nd * nd >= maxd) continue;  // the reference's lower-bound skip
-        offer(Dq[r], tb + ch * 32 + (__ffs(m) - 1));
-      }
-    }
-    __syncwarp();  // the list is rebuilt next
-  };
-
   for (int64_t t = 0; t < ntiles; ++t) {
     const int b = (int)(t & 1);
     // lane 0 waits for the warp, so the tensor-memory loads below stay warp-uniform
@@ -494,7 +516,7 @@ __device__ __forceinline__ void tc_epilogue(const TcParams& p, const T* __restri
     const bool all = !(theta > -INFINITY);  // heap still filling, or the filter is off
     // per-candidate threshold base_i - b_i R_j - g |n_j|, every rounding downwards
     float base_i = -INFINITY, b_i = 0.0f, g = 0.0f;
-    if (p.per_cand) {
+    if constexpr (PER_CAND) {
       __syncwarp();
 #pragma unroll
       for (int m = 0; m < kChunks; ++m) {
@@ -510,6 +532,8 @@ __device__ __forceinline__ void tc_epilogue(const TcParams& p, const T* __restri
         g = __double2float_ru(0.5 * (p.gamma_n + 0x1p-20));
       }
     }
+    uint32_t mk[kChunks];  // this query's keep bits, chunk by chunk
+#pragma unroll
     for (int h = 0; h < kTcN / 64; ++h) {
       float v[64];
       __syncwarp();  // the tensor-memory load is warp-collective
@@ -518,53 +542,109 @@ __device__ __forceinline__ void tc_epilogue(const TcParams& p, const T* __restri
         tc_fence_before();
         mbar_arrive(saddr(&acce[b]));
       }
+      // bit c set when s_ic > threshold: the sign of threshold - s_ic (nonzero unless equal), shifted in
+      // from the top (one funnel shift per candidate) and bit-reversed at the end
       uint32_t m0 = 0, m1 = 0;
-      if (p.per_cand) {
+      if constexpr (PER_CAND) {
 #pragma unroll
         for (int c = 0; c < 32; ++c) {
           const float2 r0 = RN[h * 64 + c], r1 = RN[h * 64 + 32 + c];
           const float t0 = __fmaf_rd(-b_i, r0.x, __fmaf_rd(-g, r0.y, base_i));
           const float t1 = __fmaf_rd(-b_i, r1.x, __fmaf_rd(-g, r1.y, base_i));
-          m0 |= (!(v[c] <= t0) ? 1u : 0u) << c;
-          m1 |= (!(v[32 + c] <= t1) ? 1u : 0u) << c;
+          m0 = __funnelshift_l(__float_as_uint(t0 - v[c]), m0, 1);
+          m1 = __funnelshift_l(__float_as_uint(t1 - v[32 + c]), m1, 1);
         }
       } else {
 #pragma unroll
         for (int c = 0; c < 32; ++c) {
-          m0 |= (!(v[c] <= theta) ? 1u : 0u) << c;
-          m1 |= (!(v[32 + c] <= theta) ? 1u : 0u) << c;
+          m0 = __funnelshift_l(__float_as_uint(theta - v[c]), m0, 1);
+          m1 = __funnelshift_l(__float_as_uint(theta - v[32 + c]), m1, 1);
         }
       }
+      m0 = __brev(m0);
+      m1 = __brev(m1);
       if (all) m0 = m1 = 0xffffffffu;
-      Msk[(2 * h) * 32 + lane] = m0;
-      Msk[(2 * h + 1) * 32 + lane] = m1;
+      mk[2 * h] = m0;
+      mk[2 * h + 1] = m1;
     }
-    int listed = 0, c0 = 0;
+    // drop candidates past n and the query itself; count this lane's pairs
+    int mine = 0;
+#pragma unroll
     for (int ch = 0; ch < kChunks; ++ch) {
       const int64_t j0 = tb + ch * 32;
-      uint32_t m = live ? Msk[ch * 32 + lane] : 0u;
+      uint32_t m = live ? mk[ch] : 0u;
       if (n - j0 < 32) m &= n - j0 <= 0 ? 0u : ((1u << (unsigned)(n - j0)) - 1u);
       if (i >= j0 && i < j0 + 32) m &= ~(1u << (unsigned)(i - j0));
-      Msk[ch * 32 + lane] = m;
-      const int mine = __popc(m);
-      int incl = mine;
-#pragma unroll
-      for (int o = 1; o < 32; o <<= 1) {
-        const int y = __shfl_up_sync(0xffffffffu, incl, o);
-        if (lane >= o) incl += y;
-      }
-      const int tot = __shfl_sync(0xffffffffu, incl, 31);
-      if (listed + tot > cap) {
-        flush(tb, c0, ch, listed);
-        listed = 0;
-        c0 = ch;
-      }
-      int pos = listed + incl - mine;
-      Off[ch * 32 + lane] = (uint16_t)pos;
-      for (uint32_t mm = m; mm; mm &= mm - 1) Pq[pos++] = (uint16_t)((lane << 8) | (ch * 32 + __ffs(mm) - 1));
-      listed += tot;
+      mk[ch] = m;
+      mine += __popc(m);
     }
-    if (listed > 0) flush(tb, c0, kChunks, listed);
+    // the warp's pairs, lane after lane, each lane's in increasing j; processed in windows of cap
+    int incl = mine;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int y = __shfl_up_sync(0xffffffffu, incl, o);
+      if (lane >= o) incl += y;
+    }
+    const int total = __shfl_sync(0xffffffffu, incl, 31);
+    const int off = incl - mine;
+    for (int wb = 0; wb < total; wb += cap) {
+      const int we = total - wb < cap ? total : wb + cap;
+      if (off < we && off + mine > wb) {  // list this lane's pairs that fall in the window
+        int q = off;
+#pragma unroll
+        for (int ch = 0; ch < kChunks; ++ch)
+          for (uint32_t m = mk[ch]; m; m &= m - 1, ++q)
+            if (q >= wb && q < we) Pq[q - wb] = (uint16_t)((lane << 8) | (ch * 32 + __ffs(m) - 1));
+      }
+      __syncwarp();
+      // exact distances, with the candidate's root norm beside: one pair per lane per round, four
+      // interleaved per lane when the window holds more than a round
+      const int nw_ = we - wb;
+      int r = lane;
+      if (nw_ > 32) {
+        for (; r < nw_; r += 128) {
+          const T* qa[4];
+          const T* cb[4];
+          T na[4], nb[4], dd[4];
+#pragma unroll
+          for (int q = 0; q < 4; ++q) {
+            const int rq = r + 32 * q < nw_ ? r + 32 * q : r;  // a missing pair repeats the first
+            const int e = Pq[rq];
+            const int o = e >> 8;
+            const int64_t j = tb + (e & 255);
+            qa[q] = Xp + (q0 + warp * 32 + o) * dp;
+            cb[q] = Xp + j * dp;
+            na[q] = QN[o];
+            nb[q] = norms[j];
+          }
+          exact_dist_sq_multi<T, 4>(qa, cb, dp, na, nb, dd);
+#pragma unroll
+          for (int q = 0; q < 4; ++q)
+            if (r + 32 * q < nw_) {
+              Dq[r + 32 * q] = dd[q];
+              Sq[r + 32 * q] = snorms[tb + (Pq[r + 32 * q] & 255)];
+            }
+        }
+      } else if (r < nw_) {
+        const int e = Pq[r];
+        const int o = e >> 8;
+        const int64_t io = q0 + warp * 32 + o, j = tb + (e & 255);
+        const T nj = norms[j];
+        Sq[r] = snorms[j];
+        Dq[r] = exact_dist_sq<T>(Xp + io * dp, Xp + j * dp, dp, QN[o], nj);
+      }
+      __syncwarp();
+      // replay this lane's pairs of the window in increasing j
+      const int r0 = off > wb ? off : wb, r1 = off + mine < we ? off + mine : we;
+      for (int r = r0; r < r1; ++r) {
+        const T ds = Dq[r - wb];
+        if (cnt >= k && !(ds < maxd)) continue;  // a full heap takes only distances below its top
+        const T nd = si - Sq[r - wb];
+        if (nd * nd >= maxd) continue;  // the reference's lower-bound skip
+        offer(ds, tb + (Pq[r - wb] & 255));
+      }
+      __syncwarp();  // the window's slots are reused next
+    }
   }
   if (!live || *abort_flag) return;
   // heap sort as the reference does: min-heap build, extract to the back, reverse
@@ -601,7 +681,7 @@ __device__ __forceinline__ void tc_epilogue(const TcParams& p, const T* __restri
   }
 }
 
-template <class T, class IT>
+template <class T, class IT, bool PER_CAND>
 __global__ void __launch_bounds__(kTcThreads, 1)
 k_knn_tc(const __grid_constant__ CUtensorMap qmap, const __grid_constant__ CUtensorMap cmap,
          const T* __restrict__ Xp, const T* __restrict__ norms, const T* __restrict__ snorms,
@@ -739,7 +819,7 @@ k_knn_tc(const __grid_constant__ CUtensorMap qmap, const __grid_constant__ CUten
       }
     }
   } else {
-    tc_epilogue<T, IT>(p, Xp, norms, snorms, Rn, Rmax, Nmax, base, tmem, warp, lane, q0, ntiles, &s_accf[0], &s_acce[0],
+    tc_epilogue<T, IT, PER_CAND>(p, Xp, norms, snorms, Rn, Rmax, Nmax, base, tmem, warp, lane, q0, ntiles, &s_accf[0], &s_acce[0],
                        &s_abort, out_idx, out_dist);
   }
   tc_fence_before();
@@ -791,12 +871,11 @@ void knn_tc_typed(const T* X, const T* norms, int64_t n, int d, int k, IT* idx, 
   p.resident = nK <= kTcResidentChunks ? 1 : 0;
   const size_t a_bytes = p.resident ? (size_t)nK * kChunkA : 0;
   const size_t stage = p.resident ? kChunkB : (size_t)(kChunkA + kChunkB);
-  // per epilogue warp: cap exact distances and root norms, 32 query norms, 8 x 32 masks and
-  // offsets, cap pair entries
+  // per epilogue warp: cap exact distances and root norms, 32 query norms, cap pair entries and
+  // the tile's (R_j, |n_j|)
   p.cap = 1024;
   const size_t warp_bytes =
-      (((size_t)p.cap * 2 * sizeof(T) + 32 * sizeof(T) + (kTcN / 32) * 32 * 6 + (size_t)p.cap * 2 + kTcN * 8) + 15) &
-      ~(size_t)15;
+      (((size_t)p.cap * 2 * sizeof(T) + 32 * sizeof(T) + (size_t)p.cap * 2 + kTcN * 8) + 15) & ~(size_t)15;
   p.per_cand = d > 128 ? 1 : 0;
   p.prefetch = (size_t)dp * sizeof(T) <= 512 ? 1 : 0;
   const size_t heap_bytes = (size_t)kTcQ * (size_t)k * (sizeof(T) + sizeof(IT));
@@ -841,7 +920,7 @@ void knn_tc_typed(const T* X, const T* norms, int64_t n, int d, int k, IT* idx, 
 
   const CUtensorMap qmap = operand_map(Qb.p, n, Kp, kTcQ);
   const CUtensorMap cmap = operand_map(Cb.p, n, Kp, kTcN);
-  auto kern = k_knn_tc<T, IT>;
+  auto kern = p.per_cand ? k_knn_tc<T, IT, true> : k_knn_tc<T, IT, false>;
   SCL_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   kern<<<(unsigned)((n + kTcQ - 1) / kTcQ), kTcThreads, smem, s>>>(qmap, cmap, Xp.as<T>(), norms, sn.as<T>(),
                                                                    Rn.as<float>(), Rmax, Nmax, p, idx, dist);

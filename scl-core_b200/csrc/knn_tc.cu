@@ -8,12 +8,14 @@
 // Only the candidates the heap can act on matter to the result: every
 // candidate while the heap is short, afterwards those strictly below its top.
 //
-// Here the tensor cores find those candidates. A CTA owns 128 queries (the
-// rows of one tcgen05.mma, M = 128) and streams every candidate tile of 256
-// rows (N = 256) through a TMA ring, so one MMA sequence gives the 128 x 256
-// approximate inner products of the tile, accumulated in FP32 in tensor
-// memory (two accumulators of 256 columns, 512 in all, so the MMAs of tile
-// t + 1 run while tile t is read). The operands are the samples rounded to
+// Here the tensor cores find those candidates. A CTA owns 256 queries, two
+// halves of 128 (the rows of one tcgen05.mma, M = 128), and streams every
+// candidate tile of 256 rows (N = 256) through a TMA ring; both halves'
+// MMAs read the same candidate tile, so each tile gives the 256 x 256
+// approximate inner products, accumulated in FP32 in tensor memory (one
+// accumulator of 256 columns per half, 512 in all; the epilogue releases it
+// as soon as it has read it, so the MMAs of tile t + 1 overlap the rest of
+// tile t's work). The operands are the samples rounded to
 // BF16, K-major rows of 64 values (128 bytes) in the 128-byte swizzled layout
 // both TMA and the MMA descriptors use. Two more K columns carry -n_j / 2 as a
 // BF16 pair (hi + lo) against ones on the query side, so the accumulator
@@ -61,22 +63,26 @@ PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder();  // spmm_bulk.cu
 
 namespace {
 
-constexpr int kTcQ = 128;                   // queries per CTA: MMA M, tensor-memory lanes
+constexpr int kTcQ = 256;                   // queries per CTA: two MMAs of M = 128 share every candidate tile
+constexpr int kTcM = 128;                   // MMA M: tensor-memory lanes
+constexpr int kTcEpiWarps = kTcQ / 32;      // one epilogue thread per query
 constexpr int kTcN = 256;                   // candidates per tile: MMA N
 constexpr int kTcK = 64;                    // BF16 values per 128-byte swizzled row chunk
 constexpr int kTcMaxStages = 4;             // candidate ring depth (at most)
-constexpr int kTcThreads = 192;             // 4 epilogue warps, a TMA warp, an MMA warp
-constexpr int kTcResidentChunks = 4;        // queries kept resident up to 256 K columns
-constexpr unsigned kChunkA = kTcQ * 128u;   // 16 KB: 128 query rows x 128 bytes
+constexpr int kTcThreads = 32 * (kTcEpiWarps + 2);  // epilogue warps, a TMA warp, an MMA warp
+constexpr int kTcProducerWarp = kTcEpiWarps, kTcMmaWarp = kTcEpiWarps + 1;
+constexpr int kTcResidentChunks = 2;        // queries kept resident up to 128 K columns
+constexpr unsigned kChunkA = kTcQ * 128u;   // 32 KB: 256 query rows x 128 bytes
+constexpr unsigned kHalfA = kTcM * 128u;    // the rows of one MMA
 constexpr unsigned kChunkB = kTcN * 128u;   // 32 KB: 256 candidate rows x 128 bytes
-constexpr unsigned kTmemCols = 2 * kTcN;    // two FP32 accumulators of 256 columns
+constexpr unsigned kTmemCols = 2 * kTcN;    // one FP32 accumulator of 256 columns per query half
 constexpr unsigned long long kTcWaitNs = 2000ull * 1000ull * 1000ull;   // 2 s
 constexpr unsigned long long kTcDrainNs = 200ull * 1000ull * 1000ull;   // 0.2 s
 
 // instruction descriptor of tcgen05.mma kind::f16: BF16 A and B, FP32 D,
 // both K-major, M = 128, N = 256
 constexpr uint32_t kIdesc = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(kTcN >> 3) << 17) |
-                            ((uint32_t)(kTcQ >> 4) << 24);
+                            ((uint32_t)(kTcM >> 4) << 24);
 
 __device__ __forceinline__ unsigned long long tc_ns() {
   unsigned long long t;
@@ -264,7 +270,7 @@ struct TcParams {
   int resident;   // queries loaded once (n_chunks <= kTcResidentChunks)
   int stages;     // candidate ring depth
   int heap_smem;  // heaps in shared memory ([k][128]); else in the output arrays
-  int cap;        // pairs one epilogue warp lists before it computes their exact distances
+  int cap;        // kept candidates an epilogue lane queues before it computes their exact distances
   int per_cand;   // per-candidate thresholds (R_j, |n_j|) instead of the tile maxima
   int prefetch;   // bulk-prefetch each tile's padded rows into L2 ahead of the exact dot products
   unsigned off_warp, warp_bytes, off_heap;  // byte offsets in the aligned dynamic shared memory
@@ -285,37 +291,6 @@ __device__ __forceinline__ float tc_theta(bool full, T ni, T maxd, float Ri, flo
   const double th = 0.5 * (n_i - M - B);
   if (th != th) return -INFINITY;
   return __double2float_rd(th);
-}
-
-// The reference's dist_sq of rows a and b: the sequential fma chain of the dot
-// product over the features in order (zeros past d change nothing), then
-// max(0, fma(-2, dot, n_a + n_b)).
-template <class T>
-__device__ __forceinline__ T exact_dist_sq(const T* __restrict__ a, const T* __restrict__ b, int dp, T na, T nb) {
-  T dot = T(0);
-  if constexpr (sizeof(T) == 4) {
-    const float4* A = reinterpret_cast<const float4*>(a);
-    const float4* B = reinterpret_cast<const float4*>(b);
-#pragma unroll 8
-    for (int v = 0; v < dp / 4; ++v) {
-      const float4 x = __ldg(A + v), y = __ldg(B + v);
-      dot = tfma(x.x, y.x, dot);
-      dot = tfma(x.y, y.y, dot);
-      dot = tfma(x.z, y.z, dot);
-      dot = tfma(x.w, y.w, dot);
-    }
-  } else {
-    const double2* A = reinterpret_cast<const double2*>(a);
-    const double2* B = reinterpret_cast<const double2*>(b);
-#pragma unroll 8
-    for (int v = 0; v < dp / 2; ++v) {
-      const double2 x = __ldg(A + v), y = __ldg(B + v);
-      dot = tfma(x.x, y.x, dot);
-      dot = tfma(x.y, y.y, dot);
-    }
-  }
-  T ds = tfma(T(-2), dot, na + nb);
-  return ds < T(0) ? T(0) : ds;
 }
 
 // 64 consecutive FP32 accumulator columns of this thread's tensor-memory lane:
@@ -356,18 +331,10 @@ __device__ __forceinline__ void tmem_ld64(uint32_t taddr, float (&v)[64]) {
   }
 }
 
-// The four epilogue warps: thread tid owns query q0 + tid and tensor-memory
-// lane tid. Per tile it reads its 256 accumulator columns 64 at a time and
-// keeps, in registers, a bit for every candidate whose s_ij is above the
-// query's threshold (one subtraction and one funnel shift per candidate).
-// The warp then lists its pairs in shared memory, lane after lane and each
-// lane's in increasing j, computes their exact distances with every lane
-// busy (one pair per lane per round, the candidate's root norm fetched
-// alongside), and each thread replays its own pairs in order: the
-// reference's skip test against the current heap top, the exact distance,
-// the heap rules. More pairs than the list holds are taken in windows.
-// P exact distances at once: the P dot products are independent fma chains
-// (each in feature order), so their row loads are in flight together.
+// The reference's dist_sq for P candidate rows at once: each dot product is
+// the sequential fma chain over the features in order (zeros past d change
+// nothing), then max(0, fma(-2, dot, n_a + n_b)); the P chains are
+// independent, so their row loads are in flight together.
 template <class T, int P>
 __device__ __forceinline__ void exact_dist_sq_multi(const T* const (&a)[P], const T* const (&b)[P], int dp,
                                                     const T (&na)[P], const T (&nb)[P], T (&out)[P]) {
@@ -414,6 +381,17 @@ __device__ __forceinline__ void exact_dist_sq_multi(const T* const (&a)[P], cons
   }
 }
 
+// The eight epilogue warps: thread tid owns query q0 + tid, which is lane
+// tid % 128 of the accumulator of query half tid / 128. Per tile it reads its
+// 256 accumulator columns 64 at a time and keeps, in registers, a bit for
+// every candidate whose s_ij is above the query's threshold (one subtraction
+// and one funnel shift per candidate), then appends the kept candidates to
+// its own queue in shared memory. When the queue would overflow, and after
+// the last tile, the thread works through it in increasing j, four at a
+// time: the four exact distances as independent chains, then for each in
+// order the reference's skip test against the current heap top and the heap
+// rules. Thresholds come from the heap top at the start of each tile, which
+// only falls, so the filter never drops a candidate the replay would act on.
 template <class T, class IT, bool PER_CAND>
 __device__ __forceinline__ void tc_epilogue(const TcParams& p, const T* __restrict__ Xp, const T* __restrict__ norms,
                                             const T* __restrict__ snorms, const float* __restrict__ Rn,
@@ -428,19 +406,17 @@ __device__ __forceinline__ void tc_epilogue(const TcParams& p, const T* __restri
   const int64_t i = q0 + tid;
   const bool live = i < n;
   const bool keep_all = *p.flag != 0;
-  const int k = p.k, dp = p.dp, cap = p.cap;
+  const int k = p.k, dp = p.dp, qcap = p.cap;
   const T ni = live ? norms[i] : T(0);
   const T si = live ? snorms[i] : T(0);
   const float Ri = live ? Rn[i] : 0.0f;
-  // this warp's scratch: exact distances and root norms of listed pairs, the
-  // warp's query norms, the pair list, the tile's (R_j, |n_j|)
+  // this warp's scratch: each lane's queue of kept candidates (slot s of lane l
+  // at s * 32 + l) and the tile's (R_j, |n_j|) for per-candidate thresholds
   unsigned char* ws = base + p.off_warp + (size_t)warp * p.warp_bytes;
-  T* Dq = reinterpret_cast<T*>(ws);
-  T* Sq = Dq + cap;
-  T* QN = Sq + cap;
-  uint16_t* Pq = reinterpret_cast<uint16_t*>(QN + 32);  // listed pairs: (lane << 8) | candidate within the tile
-  float2* RN = reinterpret_cast<float2*>(Pq + cap);  // the tile's (R_j, |n_j|) when thresholds are per candidate
-  QN[lane] = ni;
+  int32_t* Qj = reinterpret_cast<int32_t*>(ws);
+  float2* RN = reinterpret_cast<float2*>(Qj + (size_t)qcap * 32);
+  const T* xi = Xp + (live ? i : 0) * (int64_t)dp;
+  int qn = 0;  // candidates in this lane's queue
   T* Hd;
   IT* Hj;
   int hs;  // heap element m at Hd[m * hs], Hj[m * hs]
@@ -455,7 +431,8 @@ __device__ __forceinline__ void tc_epilogue(const TcParams& p, const T* __restri
   }
   T maxd = std::numeric_limits<T>::max();
   int cnt = 0;
-  const uint32_t lane_base = tmem + ((uint32_t)(warp * 32) << 16);
+  // warp w reads lane quarter w % 4 of the accumulator of query half w / 4
+  const uint32_t lane_base = tmem + ((uint32_t)((warp & 3) * 32) << 16) + (uint32_t)((warp >> 2) * kTcN);
 
   auto swap_at = [&](int a, int b) {
     const T td = Hd[a * hs];
@@ -497,11 +474,47 @@ __device__ __forceinline__ void tc_epilogue(const TcParams& p, const T* __restri
     maxd = Hd[0];
   };
 
+  // exact distances of up to four candidates of this query at once (independent fma chains), then
+  // the reference's steps for each in order: the lower-bound skip against the current heap top, the
+  // heap rules
+  auto run4 = [&](const int64_t (&js)[4], int c) {
+    const T* qa[4];
+    const T* cb[4];
+    T na[4], nb[4], dd[4];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const int64_t j = js[q < c ? q : 0];
+      qa[q] = xi;
+      cb[q] = Xp + j * dp;
+      na[q] = ni;
+      nb[q] = norms[j];
+    }
+    exact_dist_sq_multi<T, 4>(qa, cb, dp, na, nb, dd);
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      if (q >= c) break;
+      const T ds = dd[q];
+      if (cnt >= k && !(ds < maxd)) continue;  // a full heap takes only distances below its top
+      const T nd = si - snorms[js[q]];
+      if (nd * nd >= maxd) continue;  // the reference's lower-bound skip
+      offer(ds, js[q]);
+    }
+  };
+  auto flush_queue = [&]() {
+    for (int s0 = 0; s0 < qn; s0 += 4) {
+      int64_t js[4];
+      const int c = qn - s0 < 4 ? qn - s0 : 4;
+#pragma unroll
+      for (int q = 0; q < 4; ++q) js[q] = q < c ? (int64_t)Qj[(s0 + q) * 32 + lane] : 0;
+      run4(js, c);
+    }
+    qn = 0;
+  };
+
   for (int64_t t = 0; t < ntiles; ++t) {
-    const int b = (int)(t & 1);
     // lane 0 waits for the warp, so the tensor-memory loads below stay warp-uniform
     int ok = 1;
-    if (lane == 0) ok = mbar_wait(saddr(&accf[b]), (unsigned)((t >> 1) & 1), abort_flag, kTcWaitNs) ? 1 : 0;
+    if (lane == 0) ok = mbar_wait(saddr(accf), (unsigned)(t & 1), abort_flag, kTcWaitNs) ? 1 : 0;
     ok = __shfl_sync(0xffffffffu, ok, 0);
     if (!ok) {
       if (lane == 0 && !*abort_flag) {
@@ -537,10 +550,10 @@ __device__ __forceinline__ void tc_epilogue(const TcParams& p, const T* __restri
     for (int h = 0; h < kTcN / 64; ++h) {
       float v[64];
       __syncwarp();  // the tensor-memory load is warp-collective
-      tmem_ld64(lane_base + (uint32_t)(b * kTcN + h * 64), v);
-      if (h == kTcN / 64 - 1) {  // accumulator b is read: the MMAs of tile t + 2 may overwrite it
+      tmem_ld64(lane_base + (uint32_t)(h * 64), v);
+      if (h == kTcN / 64 - 1) {  // the accumulator is read: the MMAs of tile t + 1 may overwrite it
         tc_fence_before();
-        mbar_arrive(saddr(&acce[b]));
+        mbar_arrive(saddr(acce));
       }
       // bit c set when s_ic > threshold: the sign of threshold - s_ic (nonzero unless equal), shifted in
       // from the top (one funnel shift per candidate) and bit-reversed at the end
@@ -548,11 +561,13 @@ __device__ __forceinline__ void tc_epilogue(const TcParams& p, const T* __restri
       if constexpr (PER_CAND) {
 #pragma unroll
         for (int c = 0; c < 32; ++c) {
-          const float2 r0 = RN[h * 64 + c], r1 = RN[h * 64 + 32 + c];
-          const float t0 = __fmaf_rd(-b_i, r0.x, __fmaf_rd(-g, r0.y, base_i));
-          const float t1 = __fmaf_rd(-b_i, r1.x, __fmaf_rd(-g, r1.y, base_i));
-          m0 = __funnelshift_l(__float_as_uint(t0 - v[c]), m0, 1);
-          m1 = __funnelshift_l(__float_as_uint(t1 - v[32 + c]), m1, 1);
+          const float2 r0 = RN[h * 64 + c];
+          m0 = __funnelshift_l(__float_as_uint(__fmaf_rd(-b_i, r0.x, __fmaf_rd(-g, r0.y, base_i)) - v[c]), m0, 1);
+        }
+#pragma unroll
+        for (int c = 0; c < 32; ++c) {
+          const float2 r1 = RN[h * 64 + 32 + c];
+          m1 = __funnelshift_l(__float_as_uint(__fmaf_rd(-b_i, r1.x, __fmaf_rd(-g, r1.y, base_i)) - v[32 + c]), m1, 1);
         }
       } else {
 #pragma unroll
@@ -567,7 +582,7 @@ __device__ __forceinline__ void tc_epilogue(const TcParams& p, const T* __restri
       mk[2 * h] = m0;
       mk[2 * h + 1] = m1;
     }
-    // drop candidates past n and the query itself; count this lane's pairs
+    // drop candidates past n and the query itself
     int mine = 0;
 #pragma unroll
     for (int ch = 0; ch < kChunks; ++ch) {
@@ -578,74 +593,29 @@ __device__ __forceinline__ void tc_epilogue(const TcParams& p, const T* __restri
       mk[ch] = m;
       mine += __popc(m);
     }
-    // the warp's pairs, lane after lane, each lane's in increasing j; processed in windows of cap
-    int incl = mine;
+    // the warp's queues together (so their latencies overlap) when any lane's would overflow; then
+    // each lane's candidates of this tile into its queue, or straight through when they alone exceed it
+    if (__any_sync(0xffffffffu, qn + mine > qcap)) flush_queue();
+    if (mine > qcap) {
+      int64_t js[4];
+      int c = 0;
 #pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-      const int y = __shfl_up_sync(0xffffffffu, incl, o);
-      if (lane >= o) incl += y;
-    }
-    const int total = __shfl_sync(0xffffffffu, incl, 31);
-    const int off = incl - mine;
-    for (int wb = 0; wb < total; wb += cap) {
-      const int we = total - wb < cap ? total : wb + cap;
-      if (off < we && off + mine > wb) {  // list this lane's pairs that fall in the window
-        int q = off;
-#pragma unroll
-        for (int ch = 0; ch < kChunks; ++ch)
-          for (uint32_t m = mk[ch]; m; m &= m - 1, ++q)
-            if (q >= wb && q < we) Pq[q - wb] = (uint16_t)((lane << 8) | (ch * 32 + __ffs(m) - 1));
-      }
-      __syncwarp();
-      // exact distances, with the candidate's root norm beside: one pair per lane per round, four
-      // interleaved per lane when the window holds more than a round
-      const int nw_ = we - wb;
-      int r = lane;
-      if (nw_ > 32) {
-        for (; r < nw_; r += 128) {
-          const T* qa[4];
-          const T* cb[4];
-          T na[4], nb[4], dd[4];
-#pragma unroll
-          for (int q = 0; q < 4; ++q) {
-            const int rq = r + 32 * q < nw_ ? r + 32 * q : r;  // a missing pair repeats the first
-            const int e = Pq[rq];
-            const int o = e >> 8;
-            const int64_t j = tb + (e & 255);
-            qa[q] = Xp + (q0 + warp * 32 + o) * dp;
-            cb[q] = Xp + j * dp;
-            na[q] = QN[o];
-            nb[q] = norms[j];
+      for (int ch = 0; ch < kChunks; ++ch)
+        for (uint32_t m = mk[ch]; m; m &= m - 1) {
+          js[c++] = tb + ch * 32 + (__ffs(m) - 1);
+          if (c == 4) {
+            run4(js, 4);
+            c = 0;
           }
-          exact_dist_sq_multi<T, 4>(qa, cb, dp, na, nb, dd);
-#pragma unroll
-          for (int q = 0; q < 4; ++q)
-            if (r + 32 * q < nw_) {
-              Dq[r + 32 * q] = dd[q];
-              Sq[r + 32 * q] = snorms[tb + (Pq[r + 32 * q] & 255)];
-            }
         }
-      } else if (r < nw_) {
-        const int e = Pq[r];
-        const int o = e >> 8;
-        const int64_t io = q0 + warp * 32 + o, j = tb + (e & 255);
-        const T nj = norms[j];
-        Sq[r] = snorms[j];
-        Dq[r] = exact_dist_sq<T>(Xp + io * dp, Xp + j * dp, dp, QN[o], nj);
-      }
-      __syncwarp();
-      // replay this lane's pairs of the window in increasing j
-      const int r0 = off > wb ? off : wb, r1 = off + mine < we ? off + mine : we;
-      for (int r = r0; r < r1; ++r) {
-        const T ds = Dq[r - wb];
-        if (cnt >= k && !(ds < maxd)) continue;  // a full heap takes only distances below its top
-        const T nd = si - Sq[r - wb];
-        if (nd * nd >= maxd) continue;  // the reference's lower-bound skip
-        offer(ds, tb + (Pq[r - wb] & 255));
-      }
-      __syncwarp();  // the window's slots are reused next
+      if (c) run4(js, c);
+    } else if (mine) {
+#pragma unroll
+      for (int ch = 0; ch < kChunks; ++ch)
+        for (uint32_t m = mk[ch]; m; m &= m - 1) Qj[(qn++) * 32 + lane] = (int32_t)(tb + ch * 32 + (__ffs(m) - 1));
     }
   }
+  flush_queue();
   if (!live || *abort_flag) return;
   // heap sort as the reference does: min-heap build, extract to the back, reverse
   auto sort_sift = [&](int pos, int size) {
@@ -688,8 +658,8 @@ k_knn_tc(const __grid_constant__ CUtensorMap qmap, const __grid_constant__ CUten
          const float* __restrict__ Rn, const float* __restrict__ Rmax, const float* __restrict__ Nmax, TcParams p,
          IT* __restrict__ out_idx, T* __restrict__ out_dist) {
   extern __shared__ __align__(1024) unsigned char tc_smem_raw[];
-  __shared__ __align__(8) unsigned long long s_full[kTcMaxStages], s_empty[kTcMaxStages], s_aload, s_accf[2],
-      s_acce[2], s_drain;
+  __shared__ __align__(8) unsigned long long s_full[kTcMaxStages], s_empty[kTcMaxStages], s_aload, s_accf, s_acce,
+      s_drain;
   __shared__ uint32_t s_tmem;
   __shared__ volatile int s_abort;
 
@@ -709,22 +679,20 @@ k_knn_tc(const __grid_constant__ CUtensorMap qmap, const __grid_constant__ CUten
   const int64_t q0 = (int64_t)blockIdx.x * kTcQ;
   const int64_t ntiles = (n + kTcN - 1) / kTcN;
 
-  if (tid == 128) {
+  if (tid == 32 * kTcProducerWarp) {
     for (int s = 0; s < S; ++s) {
       mbar_init(saddr(&s_full[s]), 1);
       mbar_init(saddr(&s_empty[s]), 1);
     }
     mbar_init(saddr(&s_aload), 1);
-    for (int b = 0; b < 2; ++b) {
-      mbar_init(saddr(&s_accf[b]), 1);
-      mbar_init(saddr(&s_acce[b]), kTcQ);
-    }
+    mbar_init(saddr(&s_accf), 1);
+    mbar_init(saddr(&s_acce), kTcQ);
     mbar_init(saddr(&s_drain), 1);
     s_abort = 0;
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
   }
-  if (warp == 5) {
+  if (warp == kTcMmaWarp) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(saddr(&s_tmem)),
                  "r"(kTmemCols)
                  : "memory");
@@ -740,7 +708,7 @@ k_knn_tc(const __grid_constant__ CUtensorMap qmap, const __grid_constant__ CUten
     s_abort = 1;
   };
 
-  if (warp == 4) {
+  if (warp == kTcProducerWarp) {
     // ---------------- TMA producer ----------------
     if (lane == 0) {
       int64_t issued = 0;
@@ -777,7 +745,7 @@ k_knn_tc(const __grid_constant__ CUtensorMap qmap, const __grid_constant__ CUten
       }
       if (resident) mbar_wait(saddr(&s_aload), 0, &s_abort, kTcDrainNs);
     }
-  } else if (warp == 5) {
+  } else if (warp == kTcMmaWarp) {
     // ---------------- MMA issuer ----------------
     if (lane == 0) {
       bool ok = !resident || mbar_wait(saddr(&s_aload), 0, &s_abort, kTcWaitNs);
@@ -785,13 +753,11 @@ k_knn_tc(const __grid_constant__ CUtensorMap qmap, const __grid_constant__ CUten
       int64_t it = 0;
       bool issued_any = false;
       for (int64_t t = 0; ok && t < ntiles; ++t) {
-        const int b = (int)(t & 1);
-        if (t >= 2 && !mbar_wait(saddr(&s_acce[b]), (unsigned)(((t >> 1) - 1) & 1), &s_abort, kTcWaitNs)) {
+        if (t >= 1 && !mbar_wait(saddr(&s_acce), (unsigned)((t - 1) & 1), &s_abort, kTcWaitNs)) {
           if (!s_abort) give_up(3);
           break;
         }
         tc_fence_after();
-        const uint32_t dt = tmem + (uint32_t)(b * kTcN);
         for (int c = 0; c < nK; ++c, ++it) {
           const int s = (int)(it % S);
           const unsigned use = (unsigned)(it / S);
@@ -805,13 +771,16 @@ k_knn_tc(const __grid_constant__ CUtensorMap qmap, const __grid_constant__ CUten
           const unsigned a0 = saddr(resident ? a_res + (size_t)c * kChunkA : st + kChunkB);
           const unsigned b0 = saddr(st);
 #pragma unroll
-          for (int kk = 0; kk < kTcK / 16; ++kk)
-            umma_bf16(dt, sw128_desc(a0 + 32u * kk), sw128_desc(b0 + 32u * kk), (c | kk) != 0 ? 1u : 0u);
+          for (int hq = 0; hq < 2; ++hq)  // the two query halves, each into its own accumulator
+#pragma unroll
+            for (int kk = 0; kk < kTcK / 16; ++kk)
+              umma_bf16(tmem + (uint32_t)(hq * kTcN), sw128_desc(a0 + hq * kHalfA + 32u * kk),
+                        sw128_desc(b0 + 32u * kk), (c | kk) != 0 ? 1u : 0u);
           umma_commit(saddr(&s_empty[s]));  // the stage is free once these MMAs have read it
           issued_any = true;
         }
         if (!ok) break;
-        umma_commit(saddr(&s_accf[b]));  // accumulator b holds tile t
+        umma_commit(saddr(&s_accf));  // the accumulators hold tile t
       }
       if (issued_any) {  // no MMA in flight when the tensor memory is freed
         umma_commit(saddr(&s_drain));
@@ -819,12 +788,12 @@ k_knn_tc(const __grid_constant__ CUtensorMap qmap, const __grid_constant__ CUten
       }
     }
   } else {
-    tc_epilogue<T, IT, PER_CAND>(p, Xp, norms, snorms, Rn, Rmax, Nmax, base, tmem, warp, lane, q0, ntiles, &s_accf[0], &s_acce[0],
+    tc_epilogue<T, IT, PER_CAND>(p, Xp, norms, snorms, Rn, Rmax, Nmax, base, tmem, warp, lane, q0, ntiles, &s_accf, &s_acce,
                        &s_abort, out_idx, out_dist);
   }
   tc_fence_before();
   __syncthreads();
-  if (warp == 5) {
+  if (warp == kTcMmaWarp) {
     tc_fence_after();
     asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTmemCols) : "memory");
   }
@@ -871,18 +840,16 @@ void knn_tc_typed(const T* X, const T* norms, int64_t n, int d, int k, IT* idx, 
   p.resident = nK <= kTcResidentChunks ? 1 : 0;
   const size_t a_bytes = p.resident ? (size_t)nK * kChunkA : 0;
   const size_t stage = p.resident ? kChunkB : (size_t)(kChunkA + kChunkB);
-  // per epilogue warp: cap exact distances and root norms, 32 query norms, cap pair entries and
-  // the tile's (R_j, |n_j|)
-  p.cap = 1024;
-  const size_t warp_bytes =
-      (((size_t)p.cap * 2 * sizeof(T) + 32 * sizeof(T) + (size_t)p.cap * 2 + kTcN * 8) + 15) & ~(size_t)15;
+  // per epilogue warp: a queue of cap candidates per lane and the tile's (R_j, |n_j|)
+  p.cap = 16;
+  const size_t warp_bytes = (size_t)p.cap * 32 * 4 + kTcN * 8;
   p.per_cand = d > 128 ? 1 : 0;
   p.prefetch = (size_t)dp * sizeof(T) <= 512 ? 1 : 0;
   const size_t heap_bytes = (size_t)kTcQ * (size_t)k * (sizeof(T) + sizeof(IT));
   p.stages = 0;
   for (int hs = 1; hs >= 0 && p.stages == 0; --hs)
     for (int S = kTcMaxStages; S >= 2; --S)
-      if (a_bytes + S * stage + 4 * warp_bytes + (hs ? heap_bytes : 0) <= budget) {
+      if (a_bytes + S * stage + kTcEpiWarps * warp_bytes + (hs ? heap_bytes : 0) <= budget) {
         p.stages = S;
         p.heap_smem = hs;
         break;
@@ -890,7 +857,7 @@ void knn_tc_typed(const T* X, const T* norms, int64_t n, int d, int k, IT* idx, 
   SCL_REQUIRE(p.stages >= 2, kErrInternal, "kNN tile ring exceeds the device's shared memory");
   p.off_warp = (unsigned)(a_bytes + p.stages * stage);
   p.warp_bytes = (unsigned)warp_bytes;
-  p.off_heap = p.off_warp + 4 * (unsigned)warp_bytes;
+  p.off_heap = p.off_warp + kTcEpiWarps * (unsigned)warp_bytes;
   const size_t smem = 1024 + p.off_heap + (p.heap_smem ? heap_bytes : 0);
   // |exact - approximate dist_sq| <= beta R_i R_j + gamma_n |n_j| + 2^-20 (...): BF16 rounding of both
   // operands (2^-6), the tensor core's FP32 accumulation and the exact chain's own rounding

@@ -135,61 +135,101 @@ struct DptCtl {
   int done;              // set by the step whose largest unvisited probability fell below tol
 };
 
-constexpr int kDptWarps = 4;  // warps per block
-template <class T>
-constexpr int kDptStage = 4096 / (int)sizeof(T);  // entries a warp stages per round
+constexpr int kDptWarps = 8;      // warps per block
+constexpr int kDptHubLen = 256;   // rows longer than this get a warp of their own
+constexpr int kDptChunk = 8;      // entries a lane gathers before it consumes them
 
-// A warp owns 32 consecutive rows and stages their entries (the values and
-// the gathered p values), read coalesced, in shared memory; then each lane
-// runs its own row's sequential fma chain in stored order from there, so the
-// sums are the ones a thread walking its row in global memory would form.
-// Rows whose entries exceed one staging round continue in the next round
-// with the partial sum kept. The largest unvisited probability is
-// max-reduced per block into one word (one atomic per block); the last block
-// of the step compares it with tol, raises the done flag (the later steps'
-// launches then return at once) and clears the word for the next step.
+// The row update after p_new[i] = s: hitting time and visit probability of
+// rows still below 0.99 visited; returns 1 - visited.
+template <class T>
+__device__ __forceinline__ T dpt_update(int64_t i, T s, T* __restrict__ p_new, T* __restrict__ hit,
+                                        T* __restrict__ vis, T step) {
+  p_new[i] = s;
+  T v = vis[i];
+  if (v < T(0.99) && s > T(1e-15)) {
+    const T np = wmul(s, T(1) - v);
+    hit[i] = wfma(step, np, hit[i]);
+    v = v + np;
+    v = v < T(1) ? v : T(1);
+    vis[i] = v;
+  }
+  return T(1) - v;
+}
+
+// Rows are taken longest first (`order`, a permutation by decreasing length,
+// computed once per walk). Every row's sum is the sequential fma chain over
+// its entries in stored order, as a thread walking the row would form it.
+// * The n_hub longest rows (> kDptHubLen entries) get a warp each: the lanes
+//   gather the row's values and p values into shared memory 256 entries at a
+//   time, with all loads in flight together, and lane 0 runs the chain.
+// * The other rows go 32 to a warp, neighbours in length order, so the lanes
+//   finish together; a lane gathers kDptChunk entries of its row (values,
+//   indices, then the p values) before it consumes them.
+// The largest unvisited probability is max-reduced per block into one word
+// (one atomic per block); the last block of the step compares it with tol,
+// raises the done flag (the later steps' launches then return at once) and
+// clears the word for the next step.
 template <class T>
 __global__ void __launch_bounds__(kDptWarps * 32)
 k_dpt_step(const int64_t* __restrict__ ptr, const int32_t* __restrict__ idx, const T* __restrict__ val, int64_t n,
-           const T* __restrict__ p, T* __restrict__ p_new, T* __restrict__ hit, T* __restrict__ vis, T step,
-           unsigned long long* __restrict__ max_unvisited, DptCtl* ctl, T tol) {
+           const int32_t* __restrict__ order, int64_t n_hub, const T* __restrict__ p, T* __restrict__ p_new,
+           T* __restrict__ hit, T* __restrict__ vis, T step, unsigned long long* __restrict__ max_unvisited,
+           DptCtl* ctl, T tol) {
   if (*reinterpret_cast<volatile int*>(&ctl->done)) return;
-  __shared__ T sv[kDptWarps][kDptStage<T>];
-  __shared__ T sp[kDptWarps][kDptStage<T>];
+  __shared__ T sv[kDptWarps][kDptHubLen];
+  __shared__ T sp[kDptWarps][kDptHubLen];
   __shared__ T part[kDptWarps];
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const int64_t gw = (int64_t)blockIdx.x * kDptWarps + w, nw = (int64_t)gridDim.x * kDptWarps;
   T m = T(0);
-  const int64_t groups = (n + 31) / 32;
-  for (int64_t g = (int64_t)blockIdx.x * kDptWarps + w; g < groups; g += (int64_t)gridDim.x * kDptWarps) {
-    const int64_t r0 = g * 32;
-    const int64_t i = r0 + lane;
-    const bool live = i < n;
-    const int64_t rb = live ? ptr[i] : 0, re = live ? ptr[i + 1] : 0;
-    const int64_t b = ptr[r0], e = ptr[(r0 + 32) < n ? r0 + 32 : n];
+  for (int64_t hr = gw; hr < n_hub; hr += nw) {
+    const int64_t i = order[hr];
+    const int64_t rb = ptr[i], re = ptr[i + 1];
     T s = T(0);
-    for (int64_t c0 = b; c0 < e; c0 += kDptStage<T>) {
-      const int cn = (e - c0) < (int64_t)kDptStage<T> ? (int)(e - c0) : kDptStage<T>;
-#pragma unroll 4
-      for (int j = lane; j < cn; j += 32) {
-        sv[w][j] = val[c0 + j];
-        sp[w][j] = p[idx[c0 + j]];
+    for (int64_t c0 = rb; c0 < re; c0 += kDptHubLen) {
+      const int cn = (re - c0) < (int64_t)kDptHubLen ? (int)(re - c0) : kDptHubLen;
+#pragma unroll
+      for (int q = 0; q < kDptHubLen / 32; ++q) {
+        const int j = q * 32 + lane;
+        if (j < cn) {
+          sv[w][j] = val[c0 + j];
+          sp[w][j] = p[idx[c0 + j]];
+        }
       }
       __syncwarp();
-      const int64_t lo = rb > c0 ? rb : c0, hi = re < c0 + cn ? re : c0 + cn;
-      for (int64_t k = lo; k < hi; ++k) s = wfma(sv[w][k - c0], sp[w][k - c0], s);
+      if (lane == 0)
+        for (int k = 0; k < cn; ++k) s = wfma(sv[w][k], sp[w][k], s);
       __syncwarp();
     }
-    if (live) {
-      p_new[i] = s;
-      T v = vis[i];
-      if (v < T(0.99) && s > T(1e-15)) {
-        const T np = wmul(s, T(1) - v);
-        hit[i] = wfma(step, np, hit[i]);
-        v = v + np;
-        v = v < T(1) ? v : T(1);
-        vis[i] = v;
+    if (lane == 0) {
+      const T u = dpt_update<T>(i, s, p_new, hit, vis, step);
+      m = u > m ? u : m;
+    }
+  }
+  const int64_t groups = (n - n_hub + 31) / 32;
+  for (int64_t g = gw; g < groups; g += nw) {
+    const int64_t r = n_hub + g * 32 + lane;
+    if (r < n) {
+      const int64_t i = order[r];
+      const int64_t rb = ptr[i], re = ptr[i + 1];
+      T s = T(0);
+      for (int64_t k = rb; k < re; k += kDptChunk) {
+        T vv[kDptChunk], pp[kDptChunk];
+        int32_t jj[kDptChunk];
+#pragma unroll
+        for (int q = 0; q < kDptChunk; ++q)
+          if (k + q < re) {
+            vv[q] = val[k + q];
+            jj[q] = idx[k + q];
+          }
+#pragma unroll
+        for (int q = 0; q < kDptChunk; ++q)
+          if (k + q < re) pp[q] = p[jj[q]];
+#pragma unroll
+        for (int q = 0; q < kDptChunk; ++q)
+          if (k + q < re) s = wfma(vv[q], pp[q], s);
       }
-      const T u = T(1) - v;
+      const T u = dpt_update<T>(i, s, p_new, hit, vis, step);
       m = u > m ? u : m;
     }
   }
@@ -212,6 +252,20 @@ k_dpt_step(const int64_t* __restrict__ ptr, const int32_t* __restrict__ idx, con
       ctl->arrived = 0;
     }
   }
+}
+
+// Sort keys of the DPT row order: decreasing length, ties by row index.
+__global__ void k_dpt_keys(const int64_t* __restrict__ ptr, int64_t n, uint64_t* __restrict__ keys,
+                           uint32_t* __restrict__ vals, unsigned long long* __restrict__ n_hub) {
+  unsigned long long hubs = 0;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t len = ptr[i + 1] - ptr[i];
+    const uint64_t l = len < (int64_t)0xffffffff ? (uint64_t)len : 0xffffffffull;
+    keys[i] = 0xffffffffull - l;
+    vals[i] = (uint32_t)i;
+    hubs += len > kDptHubLen ? 1ull : 0ull;
+  }
+  if (hubs) atomicAdd(n_hub, hubs);
 }
 
 // hitting time / visit probability on the visited rows (> 0.5), max-reduced
@@ -327,15 +381,27 @@ void dpt_typed(const CsrView& P, int64_t root, T* out, int64_t max_iter, T tol, 
   T* bufs[2] = {pa.as<T>(), pb.as<T>()};  // step it reads bufs[(it + 1) & 1] and writes the other one
   int dev = 0;
   SCL_CUDA(cudaGetDevice(&dev));
-  const int64_t groups = (n + 31) / 32;
+  // rows longest first; the hub rows (one warp each) lead the order
+  DevBuf keys(std::max<int64_t>(n, 1) * 8, s), keys2(std::max<int64_t>(n, 1) * 8, s);
+  DevBuf rows(std::max<int64_t>(n, 1) * 4, s), order(std::max<int64_t>(n, 1) * 4, s), hubs(8, s);
+  SCL_CUDA(cudaMemsetAsync(hubs.p, 0, 8, s));
+  k_dpt_keys<<<walk_grid(n), 256, 0, s>>>(P.indptr, n, keys.as<uint64_t>(), rows.as<uint32_t>(),
+                                          hubs.as<unsigned long long>());
+  SCL_CUDA(cudaGetLastError());
+  radix_sort_pairs(keys.as<uint64_t>(), rows.as<uint32_t>(), keys2.as<uint64_t>(), order.as<uint32_t>(), n, 32, s);
+  unsigned long long n_hub = 0;
+  SCL_CUDA(cudaMemcpyAsync(&n_hub, hubs.p, 8, cudaMemcpyDeviceToHost, s));
+  SCL_CUDA(cudaStreamSynchronize(s));
+  const int64_t groups = (int64_t)n_hub + (n - (int64_t)n_hub + 31) / 32;
   const unsigned grid = (unsigned)std::max<int64_t>(
-      1, std::min<int64_t>((groups + kDptWarps - 1) / kDptWarps, (int64_t)sm_count(dev) * 12));
+      1, std::min<int64_t>((groups + kDptWarps - 1) / kDptWarps, (int64_t)sm_count(dev) * 8));
   constexpr int64_t kChunk = 8;  // steps queued between reads of the flag
   DptCtl host{};
   for (int64_t c0 = 1; c0 <= max_iter; c0 += kChunk) {
     const int64_t c1 = std::min<int64_t>(max_iter, c0 + kChunk - 1);
     for (int64_t it = c0; it <= c1; ++it) {
       k_dpt_step<T><<<grid, kDptWarps * 32, 0, s>>>(P.indptr, P.indices, static_cast<const T*>(P.values), n,
+                                                    reinterpret_cast<const int32_t*>(order.p), (int64_t)n_hub,
                                                     bufs[(it + 1) & 1], bufs[it & 1], hit.as<T>(), vis.as<T>(),
                                                     static_cast<T>(it), word.as<unsigned long long>(),
                                                     ctl.as<DptCtl>(), tol);

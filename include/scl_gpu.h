@@ -258,11 +258,13 @@ SCL_EXPORT scl_error_t scl_gpu_residual_fp64(const void* X, scl_dtype_t x_dtype,
  * (scl/kernel/neighbors.hpp:319-478 has one CPU loop); both kernels replay
  * that loop's skip test, distance arithmetic and heap rules and return the
  * same bits.
- *   kernel 0 (default): tensor-core filter. BF16 inner products on tcgen05
- *     bound every distance; only candidates that can reach the heap are
- *     recomputed exactly. Any feature count, any k.
+ *   kernel 0 (default): automatic; kernel 1 below 24,576 samples when it
+ *     applies, kernel 2 otherwise.
  *   kernel 1: every distance computed exactly on CUDA cores; up to 128
  *     features and k up to 64.
+ *   kernel 2: tensor-core filter. BF16 inner products on tcgen05 bound
+ *     every distance; only candidates that can reach the heap are recomputed
+ *     exactly. Any feature count, any k.
  * The choice is process-wide. previous (may be null) receives the old one. */
 SCL_EXPORT scl_error_t scl_gpu_knn_set_kernel(int kernel, int* previous);
 

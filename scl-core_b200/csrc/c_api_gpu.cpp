@@ -603,8 +603,8 @@ SCL_EXPORT scl_error_t scl_gpu_residual_fp64(const void* X, scl_dtype_t x_dtype,
 }
 
 SCL_EXPORT scl_error_t scl_gpu_knn_set_kernel(int kernel, int* previous) {
-  SCL_API_CHECK(kernel == 0 || kernel == 1, SCL_ERROR_INVALID_ARGUMENT,
-                "kNN kernel must be 0 (tensor cores) or 1 (CUDA cores)");
+  SCL_API_CHECK(kernel >= 0 && kernel <= 2, SCL_ERROR_INVALID_ARGUMENT,
+                "kNN kernel must be 0 (automatic), 1 (CUDA cores) or 2 (tensor cores)");
   SCL_API_TRY
   const int prev = knn_set_kernel(kernel);
   if (previous) *previous = prev;

@@ -316,9 +316,10 @@ void algebra_spmm(const CsrView& A, const void* X, int64_t K, void* Y, double al
 
 // Brute-force kNN over the rows of a dense n x d block: indices (kI32/kI64)
 // and sqrt distances [n, k], ascending, missing slots (inf, -1); and the
-// squared row norms as sequential fma chains. knn_dense runs the tensor-core
-// filter (knn_tc.cu, any d and k) unless knn_set_kernel(1) selected the
-// CUDA-core kernel (knn.cu, d <= 128, k <= 64); both give the same bits.
+// squared row norms as sequential fma chains. knn_dense picks the CUDA-core
+// kernel (knn.cu, d <= 128, k <= 64) for small sample counts and the
+// tensor-core filter (knn_tc.cu, any d and k) otherwise, unless
+// knn_set_kernel(1 or 2) fixed one; both give the same bits.
 int knn_max_features();
 int knn_set_kernel(int kernel);  // returns the previous choice
 void knn_dense(const void* X, const void* norms, DType t, int64_t n, int d, int k, void* idx, DType it, void* dist,

@@ -1,7 +1,7 @@
 // Brute-force k-nearest neighbours on CUDA cores (scl/kernel/neighbors.hpp:302-478):
-// the graph-building step before the transition matrix. The default search is
-// the tensor-core filter of knn_tc.cu; this kernel computes every distance
-// exactly and stays selectable (knn_set_kernel) for comparison.
+// the graph-building step before the transition matrix. This kernel computes
+// every distance exactly; it runs for small sample counts (up to 128 features,
+// k up to 64), the tensor-core filter of knn_tc.cu for the rest.
 //
 // The samples (the handle's primary rows) are made dense on the device, n x d
 // with d <= 128 features. Every query walks every candidate j in increasing
@@ -394,11 +394,15 @@ void knn_typed(const T* X, const T* norms, int64_t n, int d, int k, IT* idx, T* 
 int knn_max_features() { return kKnnMaxD; }
 
 namespace {
-int g_knn_kernel = 0;  // 0: tensor-core filter (knn_tc.cu), 1: the warp-specialised CUDA-core kernel above
+// 0: automatic, 1: the warp-specialised CUDA-core kernel above, 2: the tensor-core filter (knn_tc.cu)
+int g_knn_kernel = 0;
+// below this many samples the CUDA-core kernel fills the GPU better (a tensor-core CTA takes 256 queries)
+constexpr int64_t kKnnTensorMinSamples = 24576;
 }
 
 int knn_set_kernel(int kernel) {
-  SCL_REQUIRE(kernel == 0 || kernel == 1, kErrInvalidArgument, "kNN kernel must be 0 (tensor cores) or 1 (CUDA cores)");
+  SCL_REQUIRE(kernel >= 0 && kernel <= 2, kErrInvalidArgument,
+              "kNN kernel must be 0 (automatic), 1 (CUDA cores) or 2 (tensor cores)");
   const int prev = g_knn_kernel;
   g_knn_kernel = kernel;
   return prev;
@@ -409,7 +413,9 @@ void knn_dense(const void* X, const void* norms, DType t, int64_t n, int d, int 
   SCL_REQUIRE(d >= 1 && k >= 1, kErrInvalidArgument, "Dimensions must be positive");
   SCL_REQUIRE(n < (int64_t)0x7fffffff, kErrInvalidArgument, "kNN sample count exceeds the int32 range");
   if (n == 0) return;
-  if (g_knn_kernel == 0) return knn_tensor(X, norms, t, n, d, k, idx, it, dist, s);
+  const bool cuda_cores_fit = d <= kKnnMaxD && k <= 64;
+  const bool tensor = g_knn_kernel == 2 || (g_knn_kernel == 0 && (!cuda_cores_fit || n >= kKnnTensorMinSamples));
+  if (tensor) return knn_tensor(X, norms, t, n, d, k, idx, it, dist, s);
   SCL_REQUIRE(d <= kKnnMaxD, kErrInvalidArgument, "the CUDA-core kNN kernel takes 1 to 128 features");
   SCL_REQUIRE(k <= 64, kErrInvalidArgument, "the CUDA-core kNN kernel takes k from 1 to 64");
   if (t == kF32) {

@@ -38,9 +38,9 @@ def knn(mat: CsrMatrix, k: int, norms: np.ndarray = None):
 
 def set_kernel(kernel: int, mat_or_variant="f32_i32") -> int:
     """Choose the kernel scl_knn runs in one library variant (scl_gpu_knn_set_kernel):
-    0 = tensor-core filter (default; any feature count and k), 1 = every distance
-    on CUDA cores (up to 128 features, k up to 64). Both return the same bits.
-    Returns the previous choice."""
+    0 = automatic (default), 1 = every distance on CUDA cores (up to 128 features,
+    k up to 64), 2 = tensor-core filter (any feature count and k). All return the
+    same bits. Returns the previous choice."""
     from ._bindings._loader import get_library
 
     lib = mat_or_variant.lib if isinstance(mat_or_variant, CsrMatrix) else get_library(mat_or_variant)

@@ -26,13 +26,22 @@ def _matrix(n, d, dt, idt, dens=1.0, seed=0, quantised=False):
     return m, X
 
 
+@pytest.fixture(params=[1, 2], ids=["cuda_cores", "tensor_cores"])
+def knn_kernel(request):
+    """Runs a test once per kNN kernel (scl_gpu_knn_set_kernel) in every library variant."""
+    prev = {v: scl.neighbors.set_kernel(request.param, v) for v in ("f32_i32", "f64_i64")}
+    yield request.param
+    for v, k in prev.items():
+        scl.neighbors.set_kernel(k, v)
+
+
 @pytest.mark.parametrize("dt,idt", [(np.float32, np.int32), (np.float64, np.int64)])
 @pytest.mark.parametrize("n,d,k,dens,quant", [(1, 3, 4, 1.0, False), (12, 5, 15, 1.0, False),
                                               (300, 20, 10, 1.0, False), (700, 50, 30, 1.0, False),
                                               (400, 60, 12, 0.3, False), (500, 8, 6, 1.0, True),
                                               (2000, 128, 64, 1.0, False), (129, 1, 3, 1.0, True),
                                               (3000, 33, 40, 1.0, True)])
-def test_knn_bit_exact(dt, idt, n, d, k, dens, quant):
+def test_knn_bit_exact(knn_kernel, dt, idt, n, d, k, dens, quant):
     m, X = _matrix(n, d, dt, idt, dens, seed=n + d, quantised=quant)
     Xd = X.toarray()
     norms = np.einsum("ij,ij->i", Xd.astype(np.float64), Xd.astype(np.float64)).astype(dt)
@@ -49,7 +58,7 @@ def test_knn_bit_exact(dt, idt, n, d, k, dens, quant):
     np.testing.assert_allclose(gn, norms, rtol=1e-5 if dt == np.float32 else 1e-13)
 
 
-def test_knn_equals_the_reference_with_its_norms():
+def test_knn_equals_the_reference_with_its_norms(knn_kernel):
     if not ref.available("f32_i32"):
         pytest.skip("reference library not shipped with the tests")
     R = ref.RefLib("f32_i32")
@@ -73,7 +82,7 @@ def test_knn_errors():
     assert lib.scl_knn(m.handle, None, 10, 3, PI, PD) == 4
     assert lib.scl_knn(m.handle, PN, 0, 3, PI, PD) == 10
     assert lib.scl_knn(m.handle, PN, 9, 3, PI, PD) == 11  # n_samples must be the row count
-    # the CUDA-core kernel is limited to k <= 64 and 128 features; the default is not
+    # the CUDA-core kernel is limited to k <= 64 and 128 features; the automatic choice is not
     wide, _ = _matrix(10, 129, np.float32, np.int32)
     prev = scl.neighbors.set_kernel(1, m)
     try:
@@ -85,7 +94,7 @@ def test_knn_errors():
     assert lib.scl_knn(m.handle, PN, 10, 65, big[0].ctypes.data_as(ctypes.POINTER(lib.index_type)),
                        big[1].ctypes.data_as(ctypes.POINTER(lib.real_type))) == 0
     assert lib.scl_knn_simple(wide.handle, 10, 3, PI, PD) == 0
-    assert lib.scl_gpu_knn_set_kernel(2, None) == 10
+    assert lib.scl_gpu_knn_set_kernel(3, None) == 10
     assert lib.scl_neighbors_compute_norms(None, PN) == 4
 
 
@@ -118,8 +127,17 @@ def _dense_case(n, d, dt, seed, dens=1.0, scale=1.0, dup=0):
     (257, 1, 5, 1.0, 1.0, 100),         # one feature, many ties
 ])
 def test_knn_any_width_and_k(dt, n, d, k, dens, scale, dup):
-    """The tensor-core filter (default kernel) at sizes the CUDA-core kernel
-    does not take, against the restatement, bit for bit."""
+    """The tensor-core filter at sizes the CUDA-core kernel does not take (and
+    at sizes it does), against the restatement, bit for bit."""
+    variant = "f32_i32" if dt == np.float32 else "f64_i64"
+    prev = scl.neighbors.set_kernel(2, variant)
+    try:
+        _any_width_case(dt, n, d, k, dens, scale, dup)
+    finally:
+        scl.neighbors.set_kernel(prev, variant)
+
+
+def _any_width_case(dt, n, d, k, dens, scale, dup):
     m, Xd, norms = _dense_case(n, d, dt, seed=n + d + k, dens=dens, scale=scale, dup=dup)
     gi, gd = scl.neighbors.knn(m, k, norms)
     oi, od = port.knn_dense(Xd, norms, k)
@@ -135,9 +153,10 @@ def test_knn_kernels_agree(dt):
     rng = np.random.default_rng(9)
     odd = (norms * rng.uniform(0.5, 2.0, norms.shape)).astype(dt)
     for nr in (norms, odd):
-        a = scl.neighbors.knn(m, 30, nr)
-        prev = scl.neighbors.set_kernel(1, m)
+        prev = scl.neighbors.set_kernel(2, m)
         try:
+            a = scl.neighbors.knn(m, 30, nr)
+            scl.neighbors.set_kernel(1, m)
             b = scl.neighbors.knn(m, 30, nr)
         finally:
             scl.neighbors.set_kernel(prev, m)
@@ -154,7 +173,11 @@ def test_knn_non_finite_values_replay_every_candidate():
     X = sp.csr_matrix(Xd)
     X.sort_indices()
     m = scl.CsrMatrix.wrap(X.indptr.astype(np.int32), X.indices.astype(np.int32), X.data, X.shape)
-    gi, gd = scl.neighbors.knn(m, 10, norms)
+    prev = scl.neighbors.set_kernel(2, m)
+    try:
+        gi, gd = scl.neighbors.knn(m, 10, norms)
+    finally:
+        scl.neighbors.set_kernel(prev, m)
     oi, od = port.knn_dense(Xd, norms, 10)
     np.testing.assert_array_equal(gd.view(np.uint8), od.view(np.uint8))
     np.testing.assert_array_equal(gi.astype(np.int64), oi)

@@ -137,7 +137,6 @@ struct DptCtl {
 
 constexpr int kDptWarps = 8;      // warps per block
 constexpr int kDptHubLen = 256;   // rows longer than this get a warp of their own
-constexpr int kDptChunk = 8;      // entries a lane gathers before it consumes them
 
 // The row update after p_new[i] = s: hitting time and visit probability of
 // rows still below 0.99 visited; returns 1 - visited.
@@ -163,8 +162,8 @@ __device__ __forceinline__ T dpt_update(int64_t i, T s, T* __restrict__ p_new, T
 //   gather the row's values and p values into shared memory 256 entries at a
 //   time, with all loads in flight together, and lane 0 runs the chain.
 // * The other rows go 32 to a warp, neighbours in length order, so the lanes
-//   finish together; a lane gathers kDptChunk entries of its row (values,
-//   indices, then the p values) before it consumes them.
+//   finish together; a lane reads its row's values and indices in 16-byte
+//   blocks, two at a time, gathers their p values, then consumes them.
 // The largest unvisited probability is max-reduced per block into one word
 // (one atomic per block); the last block of the step compares it with tol,
 // raises the done flag (the later steps' launches then return at once) and
@@ -206,6 +205,10 @@ k_dpt_step(const int64_t* __restrict__ ptr, const int32_t* __restrict__ idx, con
       m = u > m ? u : m;
     }
   }
+  // values and indices in 16-byte blocks (aligned to the block, entries outside the row skipped),
+  // two blocks per round, then the round's p gathers, then its fmas in order
+  constexpr int V = 16 / (int)sizeof(T);
+  const int64_t nnz = ptr[n];
   const int64_t groups = (n - n_hub + 31) / 32;
   for (int64_t g = gw; g < groups; g += nw) {
     const int64_t r = n_hub + g * 32 + lane;
@@ -213,21 +216,40 @@ k_dpt_step(const int64_t* __restrict__ ptr, const int32_t* __restrict__ idx, con
       const int64_t i = order[r];
       const int64_t rb = ptr[i], re = ptr[i + 1];
       T s = T(0);
-      for (int64_t k = rb; k < re; k += kDptChunk) {
-        T vv[kDptChunk], pp[kDptChunk];
-        int32_t jj[kDptChunk];
+      for (int64_t k0 = rb & ~(int64_t)(V - 1); k0 < re; k0 += 2 * V) {
+        T vv[2 * V];
+        int32_t jj[2 * V];
 #pragma unroll
-        for (int q = 0; q < kDptChunk; ++q)
-          if (k + q < re) {
-            vv[q] = val[k + q];
-            jj[q] = idx[k + q];
+        for (int h = 0; h < 2; ++h) {
+          const int64_t kb = k0 + h * V;
+          if (kb + V <= nnz) {
+            if constexpr (sizeof(T) == 4) {
+              const float4 a = __ldg(reinterpret_cast<const float4*>(val + kb));
+              const int4 b = __ldg(reinterpret_cast<const int4*>(idx + kb));
+              vv[h * V] = a.x, vv[h * V + 1] = a.y, vv[h * V + 2] = a.z, vv[h * V + 3] = a.w;
+              jj[h * V] = b.x, jj[h * V + 1] = b.y, jj[h * V + 2] = b.z, jj[h * V + 3] = b.w;
+            } else {
+              const double2 a = __ldg(reinterpret_cast<const double2*>(val + kb));
+              const int2 b = __ldg(reinterpret_cast<const int2*>(idx + kb));
+              vv[h * V] = a.x, vv[h * V + 1] = a.y;
+              jj[h * V] = b.x, jj[h * V + 1] = b.y;
+            }
+          } else {
+#pragma unroll
+            for (int q = 0; q < V; ++q) {
+              const bool in = kb + q < nnz;
+              vv[h * V + q] = in ? val[kb + q] : T(0);
+              jj[h * V + q] = in ? idx[kb + q] : 0;
+            }
           }
+        }
+        T pp[2 * V];
 #pragma unroll
-        for (int q = 0; q < kDptChunk; ++q)
-          if (k + q < re) pp[q] = p[jj[q]];
+        for (int q = 0; q < 2 * V; ++q)
+          if (k0 + q >= rb && k0 + q < re) pp[q] = p[jj[q]];
 #pragma unroll
-        for (int q = 0; q < kDptChunk; ++q)
-          if (k + q < re) s = wfma(vv[q], pp[q], s);
+        for (int q = 0; q < 2 * V; ++q)
+          if (k0 + q >= rb && k0 + q < re) s = wfma(vv[q], pp[q], s);
       }
       const T u = dpt_update<T>(i, s, p_new, hit, vis, step);
       m = u > m ? u : m;
@@ -381,6 +403,8 @@ void dpt_typed(const CsrView& P, int64_t root, T* out, int64_t max_iter, T tol, 
   T* bufs[2] = {pa.as<T>(), pb.as<T>()};  // step it reads bufs[(it + 1) & 1] and writes the other one
   int dev = 0;
   SCL_CUDA(cudaGetDevice(&dev));
+  SCL_REQUIRE((reinterpret_cast<uintptr_t>(P.values) & 15u) == 0 && (reinterpret_cast<uintptr_t>(P.indices) & 15u) == 0,
+              kErrInternal, "DPT: the step reads values and indices in 16-byte blocks");
   // rows longest first; the hub rows (one warp each) lead the order
   DevBuf keys(std::max<int64_t>(n, 1) * 8, s), keys2(std::max<int64_t>(n, 1) * 8, s);
   DevBuf rows(std::max<int64_t>(n, 1) * 4, s), order(std::max<int64_t>(n, 1) * 4, s), hubs(8, s);

@@ -288,6 +288,9 @@ SCL_EXPORT scl_error_t scl_gpu_graph_set_plan(scl_gpu_graph_t graph, int64_t n_f
                     (kind == 12 && (group == 8 || group == 16 || group == 32) && bytes == 16 &&
                      n_features == (int64_t)group * vec && dtype_size(graph->store_type) >= 4 &&
                      (stage == 4 || stage == 8 || stage == 16)) ||
+                    (kind == 14 && (group == 8 || group == 16) && bytes == 16 &&
+                     n_features == (int64_t)group * vec && dtype_size(graph->store_type) == 2 &&
+                     (stage == 4 || stage == 8 || stage == 16)) ||
                     (kind == 11 && group == 32 && n_features == 32 * vec && dtype_size(graph->store_type) >= 4 &&
                      (bytes == 4 || bytes == 8 || bytes == 16) && bytes >= (int)dtype_size(graph->store_type) &&
                      (stage == 2 || stage == 3 || stage == 4 || stage == 6)) ||

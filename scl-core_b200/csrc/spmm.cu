@@ -846,6 +846,198 @@ k_spmm_rows16(const int64_t* __restrict__ indptr, const int32_t* __restrict__ in
   }
 }
 
+// ---- multi-row kernel for 16-bit storage (BF16/FP16, 128/256-byte rows) -----------
+// k_spmm_rows16's layout with 16-bit values and X: L = ROWB/16 lanes cover a
+// gathered row (8 values per lane), one warp advances Q = 32/L rows in
+// lockstep, and every row keeps Q interleaved FP32 fma chains over its
+// entries: entry p of the row feeds chain p mod Q, and the chains are summed
+// pairwise at the end ((c0 + c1) + (c2 + c3) for Q = 4). That is the
+// summation order of the other 16-bit kernels (kinds 5, 6, 9, 10), which the
+// restatement oracle_diffuse_lowp_chains states, so all give the same bits.
+// On rows ordered by length the lockstep costs little, and one load
+// instruction gathers Q entries.
+template <class VT, class YT, int ROWB, int U, int MINB>
+__global__ void __launch_bounds__(kSpmmThreads, MINB)
+k_spmm_rows16_lp(const int64_t* __restrict__ indptr, const int32_t* __restrict__ indices,
+                 const VT* __restrict__ values, const VT* __restrict__ X, YT* __restrict__ Y,
+                 const int32_t* __restrict__ row_map, int64_t n_rows) {
+  constexpr int L = ROWB / 16;
+  constexpr int Q = 32 / L;  // rows per warp = chains per row
+  constexpr int VEC = 8;     // 16-bit values per lane
+  constexpr int WARPS = kSpmmThreads / 32;
+  constexpr int F = ROWB / 2;
+  static_assert(L == 8 || L == 16, "16-bit rows of 128 or 256 bytes");
+  static_assert(U == 4 || U == 8 || U == 16, "batch must be 4, 8 or 16");
+  __shared__ __align__(16) int32_t s_j[WARPS][2][32 * Q];
+  __shared__ __align__(16) float s_v[WARPS][2][32 * Q];
+  const int lane = threadIdx.x & 31;
+  const int w = threadIdx.x >> 5;
+  const int q = lane / L;
+  const int lq = lane % L;
+  const int64_t n_grp = (n_rows + Q - 1) / Q;
+  const int64_t nw = ((int64_t)gridDim.x * kSpmmThreads) >> 5;
+  int64_t grp = ((int64_t)blockIdx.x * kSpmmThreads + threadIdx.x) >> 5;
+  if (grp >= n_grp) return;
+  const char* __restrict__ Xl = reinterpret_cast<const char*>(X) + lq * 16;
+  auto gather = [&](int32_t j) -> uint4 {
+    return __ldg(reinterpret_cast<const uint4*>(Xl + (size_t)(uint32_t)j * ROWB));
+  };
+  auto bounds = [&](int64_t g, int64_t& b0, int64_t& b1) {
+    const int64_t r = g * Q + q;
+    b0 = b1 = 0;
+    if (g < n_grp && r < n_rows) {
+      b0 = indptr[r];
+      b1 = indptr[r + 1];
+    }
+  };
+  auto fetch = [&](int64_t b0, int64_t b1, int base, int32_t (&j)[Q], float (&v)[Q]) {
+#pragma unroll
+    for (int k = 0; k < Q; ++k) {
+      const int64_t p = b0 + base + lq + L * k;
+      j[k] = 0;
+      v[k] = 0.0f;
+      if (p < b1) {
+        j[k] = __ldcs(indices + p);
+        v[k] = to_acc<float, VT>(__ldcs(values + p));
+      }
+    }
+  };
+  auto publish = [&](int b, const int32_t (&j)[Q], const float (&v)[Q]) {
+#pragma unroll
+    for (int k = 0; k < Q; ++k) {
+      s_j[w][b][q * 32 + lq + L * k] = j[k];
+      s_v[w][b][q * 32 + lq + L * k] = v[k];
+    }
+  };
+  int64_t s_cur, e_cur, s_nx, e_nx;
+  bounds(grp, s_cur, e_cur);
+  bounds(grp + nw, s_nx, e_nx);
+  int buf = 0;
+  {
+    int32_t j[Q];
+    float v[Q];
+    fetch(s_cur, e_cur, 0, j, v);
+    publish(0, j, v);
+    __syncwarp();
+  }
+  for (; grp < n_grp; grp += nw) {
+    int64_t s_nn, e_nn;
+    bounds(grp + 2 * nw, s_nn, e_nn);
+    const int len = (int)(e_cur - s_cur);
+    int maxlen = len, minlen = len;
+#pragma unroll
+    for (int o = L; o < 32; o <<= 1) {
+      maxlen = max(maxlen, __shfl_xor_sync(0xffffffffu, maxlen, o));
+      minlen = min(minlen, __shfl_xor_sync(0xffffffffu, minlen, o));
+    }
+    float acc[Q][VEC];
+#pragma unroll
+    for (int c = 0; c < Q; ++c)
+#pragma unroll
+      for (int i = 0; i < VEC; ++i) acc[c][i] = 0.0f;
+    for (int base = 0; base < maxlen; base += 32) {
+      int32_t jn[Q];
+      float vn[Q];
+      if (base + 32 < maxlen) fetch(s_cur, e_cur, base + 32, jn, vn);
+      else fetch(s_nx, e_nx, 0, jn, vn);
+      const int cnt = len - base;  // this lane's row: entries left (may be <= 0)
+      const int cmax = min(maxlen - base, 32);
+      const int cmin = min(minlen - base, 32);
+      const int32_t* __restrict__ jb = &s_j[w][buf][q * 32];
+      const float* __restrict__ vb = &s_v[w][buf][q * 32];
+#pragma unroll 1
+      for (int t = 0; t < cmax; t += U) {
+        uint4 xr[U];
+        const bool full = (t + U <= cmin);
+#pragma unroll
+        for (int u = 0; u < U; u += 4) {
+          const int4 j4 = *reinterpret_cast<const int4*>(jb + t + u);
+          if (full) {
+            xr[u] = gather(j4.x);
+            xr[u + 1] = gather(j4.y);
+            xr[u + 2] = gather(j4.z);
+            xr[u + 3] = gather(j4.w);
+          } else {
+            if (t + u < cnt) xr[u] = gather(j4.x);
+            if (t + u + 1 < cnt) xr[u + 1] = gather(j4.y);
+            if (t + u + 2 < cnt) xr[u + 2] = gather(j4.z);
+            if (t + u + 3 < cnt) xr[u + 3] = gather(j4.w);
+          }
+        }
+#pragma unroll
+        for (int u = 0; u < U; u += 4) {
+          const float4 v4 = *reinterpret_cast<const float4*>(vb + t + u);
+          const float vq[4] = {v4.x, v4.y, v4.z, v4.w};
+#pragma unroll
+          for (int r = 0; r < 4; ++r) {
+            if (full || t + u + r < cnt) {
+              // entry base + t + u + r of the row; base and t are multiples of 4, so its chain is (u + r) mod Q
+              const uint32_t wv[4] = {xr[u + r].x, xr[u + r].y, xr[u + r].z, xr[u + r].w};
+              float x[VEC];
+#pragma unroll
+              for (int h = 0; h < 4; ++h) {
+                if constexpr (std::is_same_v<VT, __nv_bfloat16>) {
+                  x[2 * h] = __uint_as_float(wv[h] << 16);
+                  x[2 * h + 1] = __uint_as_float(wv[h] & 0xffff0000u);
+                } else {
+                  const float2 f = __half22float2(*reinterpret_cast<const __half2*>(&wv[h]));
+                  x[2 * h] = f.x;
+                  x[2 * h + 1] = f.y;
+                }
+              }
+#pragma unroll
+              for (int i = 0; i < VEC; ++i) acc[(u + r) % Q][i] = __fmaf_rn(vq[r], x[i], acc[(u + r) % Q][i]);
+            }
+          }
+        }
+      }
+      // the other buffer was last read one chunk ago, before the last __syncwarp
+      publish(buf ^ 1, jn, vn);
+      __syncwarp();
+      buf ^= 1;
+    }
+    if (maxlen == 0) {  // empty rows only: nothing was prefetched, stage the next group's first chunk
+      int32_t j[Q];
+      float v[Q];
+      fetch(s_nx, e_nx, 0, j, v);
+      publish(buf, j, v);
+      __syncwarp();
+    }
+    const int64_t r = grp * Q + q;
+    if (r < n_rows) {
+      float y[VEC];
+#pragma unroll
+      for (int i = 0; i < VEC; ++i) {
+        if constexpr (Q == 4) y[i] = (acc[0][i] + acc[1][i]) + (acc[2][i] + acc[3][i]);
+        else y[i] = acc[0][i] + acc[1][i];
+      }
+      const int64_t orow = row_map ? (int64_t)row_map[r] : r;
+      YT* dst = Y + orow * F + lq * VEC;
+      if constexpr (std::is_same_v<YT, float>) {
+        *reinterpret_cast<float4*>(dst) = make_float4(y[0], y[1], y[2], y[3]);
+        *reinterpret_cast<float4*>(dst + 4) = make_float4(y[4], y[5], y[6], y[7]);
+      } else {
+        uint32_t o[4];
+#pragma unroll
+        for (int h = 0; h < 4; ++h) {
+          if constexpr (std::is_same_v<YT, __nv_bfloat16>) {
+            const __nv_bfloat162 b = __floats2bfloat162_rn(y[2 * h], y[2 * h + 1]);
+            o[h] = *reinterpret_cast<const uint32_t*>(&b);
+          } else {
+            const __half2 b = __floats2half2_rn(y[2 * h], y[2 * h + 1]);
+            o[h] = *reinterpret_cast<const uint32_t*>(&b);
+          }
+        }
+        *reinterpret_cast<uint4*>(dst) = make_uint4(o[0], o[1], o[2], o[3]);
+      }
+    }
+    s_cur = s_nx;
+    e_cur = e_nx;
+    s_nx = s_nn;
+    e_nx = e_nn;
+  }
+}
+
 // ---- flat-stream kernel: a warp walks the entries of a block of rows ---------------
 // A task is R consecutive rows; their entries [indptr[r0], indptr[r0+R]) are
 // one contiguous stream that the warp consumes in batches of U gathers, with
@@ -1691,6 +1883,36 @@ void launch_split_lean(const SpmmArgs& a, int mode, cudaStream_t s) {
   throw Error(kErrInvalidArgument, "the lean split-chain SpMM needs 128- or 256-byte rows");
 }
 
+// kind 14: multi-row kernel for 16-bit storage; stage = gathers per batch (4/8/16)
+template <class VT, class YT, int ROWB, int U, int MINB>
+void launch_rows16_lp_u(const SpmmArgs& a, cudaStream_t s) {
+  constexpr int R = 32 / (ROWB / 16);
+  auto kern = k_spmm_rows16_lp<VT, YT, ROWB, U, MINB>;
+  const int64_t groups = (a.n_rows + R - 1) / R;
+  const dim3 grid(persistent_blocks(kern, 0, groups, 32));
+  kern<<<grid, kSpmmThreads, 0, s>>>(a.indptr, a.indices, static_cast<const VT*>(a.values),
+                                     static_cast<const VT*>(a.X), static_cast<YT*>(a.Y), a.row_map, a.n_rows);
+  SCL_CUDA(cudaGetLastError());
+}
+
+template <class VT, class YT>
+void launch_rows16_lp(const SpmmArgs& a, int U, cudaStream_t s) {
+  const int64_t rowb = a.F * 2;
+  SCL_REQUIRE(reinterpret_cast<uintptr_t>(a.X) % 16 == 0 && reinterpret_cast<uintptr_t>(a.Y) % 16 == 0,
+              kErrInvalidArgument, "the 16-bit multi-row SpMM needs 16-byte aligned X and Y");
+#define SCL_LP_CASE(RB)                                                               \
+  if (rowb == RB) {                                                                   \
+    if (U == 4) return launch_rows16_lp_u<VT, YT, RB, 4, 3>(a, s);                   \
+    if (U == 8) return launch_rows16_lp_u<VT, YT, RB, 8, 2>(a, s);                   \
+    if (U == 16) return launch_rows16_lp_u<VT, YT, RB, 16, 2>(a, s);                 \
+    throw Error(kErrInvalidArgument, "16-bit multi-row SpMM batch must be 4, 8 or 16"); \
+  }
+  SCL_LP_CASE(128)
+  SCL_LP_CASE(256)
+#undef SCL_LP_CASE
+  throw Error(kErrInvalidArgument, "the 16-bit multi-row SpMM needs 128- or 256-byte rows");
+}
+
 // kinds 5/6: split-chain kernel for 16-bit storage (6 = mixed-precision fma);
 // stage = gathers per lane per batch (U * chains must divide 32)
 template <class VT, class XT, class YT, int ROWB, int U, bool MIXED>
@@ -1780,6 +2002,15 @@ void launch_typed(const SpmmArgs& a, const SpmmPlan& plan, cudaStream_t s) {
       return launch_split_lean<VT, XT, YT>(a, plan.stage, s);
     }
     throw Error(kErrInvalidArgument, "the lean split-chain SpMM is for bf16 or f16 storage");
+  }
+  if (plan.kind == 14) {
+    SCL_REQUIRE(plan.vec == kVec && (int64_t)plan.group * kVec == a.F && (plan.group == 8 || plan.group == 16),
+                kErrInvalidArgument, "the 16-bit multi-row SpMM covers a row with 16-byte chunks, 8 or 16 lanes per row");
+    if constexpr (sizeof(XT) == 2 && std::is_same<VT, XT>::value && sizeof(AT) == 4 &&
+                  (std::is_same<YT, XT>::value || std::is_same<YT, float>::value)) {
+      return launch_rows16_lp<VT, YT>(a, plan.stage, s);
+    }
+    throw Error(kErrInvalidArgument, "the 16-bit multi-row SpMM is for bf16 or f16 values and X");
   }
   if (plan.kind == 9) {
     SCL_REQUIRE(plan.vec == kVec && (int64_t)plan.group * kVec == a.F && (plan.stage == 0 || plan.stage == 1),
@@ -1900,6 +2131,8 @@ std::vector<SpmmPlan> candidate_plans(int64_t F, DType xtype, const void* X, con
     add(group, 8, 9, 1);
     add(group, 8, 10, 0);
     if (xtype == kBF16) add(group, 8, 10, 1);
+    if ((reinterpret_cast<uintptr_t>(X) & 15u) == 0 && (reinterpret_cast<uintptr_t>(Y) & 15u) == 0)
+      for (int st : {4, 8, 16}) add(group, 8, 14, st);
   } else if (d.kind == 4) {
     // sequential-chain family, fixed row pitch
     for (int st : {8, 16, 32}) add(32, d.vec, 4, st);
@@ -1922,7 +2155,7 @@ void spmm_with_plan(const SpmmArgs& a, const SpmmPlan& plan, cudaStream_t s) {
               "lane-group size must be a power of two in [1, 32]");
   SCL_REQUIRE(plan.kind == 0 || plan.kind == 2 || plan.kind == 3 || plan.kind == 4 || plan.kind == 5 ||
                   plan.kind == 6 || plan.kind == 7 || plan.kind == 9 || plan.kind == 10 || plan.kind == 11 ||
-                  plan.kind == 12 ||
+                  plan.kind == 12 || plan.kind == 14 ||
                   (plan.kind == 1 && plan.vec > 1 && plan.group >= 4),
               kErrInvalidArgument, "the pipelined SpMM needs 16-byte lane chunks and a lane group of at least 4");
   if (plan.kind == 11) {

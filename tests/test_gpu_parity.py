@@ -431,12 +431,17 @@ def test_split_chain_shapes_are_exact(graph_3k, storage, F):
         ref1 = port.diffuse_lowp_chains(ip, ind, P, Xd.float().cpu().numpy(), 1, kind_code, chains, True)
         stages = (2, 4, 8) if group == 8 else (4, 8, 16)
         shapes = [(k, st) for k in (5, 6) for st in stages] + [(9, 0), (9, 1), (10, 0)]
+        shapes += [(14, st) for st in (4, 8, 16)]  # rows in lockstep, 32/group rows per warp
         if storage == "bf16":
             shapes.append((10, 1))  # packed f32x2 fma
+        ref1_lowp = port.diffuse_lowp_chains(ip, ind, P, Xd.float().cpu().numpy(), 1, kind_code, chains, False)
         for kind, stage in shapes:
             Y = torch.empty((n, F), dtype=torch.float32, device="cuda")
             g.spmm(Xd, Y, group=group, vec=8, kind=kind, stage=stage)
             np.testing.assert_array_equal(bits(Y.cpu().numpy()), bits(ref1))
+            Yl = torch.empty((n, F), dtype=tdt, device="cuda")  # 16-bit output, rounded once
+            g.spmm(Xd, Yl, group=group, vec=8, kind=kind, stage=stage)
+            np.testing.assert_array_equal(bits(Yl.float().cpu().numpy()), bits(ref1_lowp))
         Yd = g.diffuse(Xd, 3, out_dtype=torch.float32).cpu().numpy()
         np.testing.assert_array_equal(bits(Yd), bits(port.diffuse_lowp_chains(ip, ind, P, X0, 3, kind_code, chains)))
     finally:

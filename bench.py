@@ -908,6 +908,8 @@ def main():
             "batched_bit_identical_to_reference": batched.get("bit_identical_to_reference") if batched else None,
             "e2e_ms": e2e["ms_per_step"] if e2e else None,
         }
+        # the ncu capture of the plan the autotuner picked (kind 12: multi-row, kind 4: warp per row)
+        traffic_profile = "spmm_rows16_f32_500k" if tuned["kind"] == 12 else "spmm_row_f32_500k"
         line = {
             "metric": METRIC, "value": round(value, 3), "unit": "GB/s", "n_gpus": world, "steps": args.steps,
             "warmup": warmup, "ms_per_step": round(t_ms, 4), "higher_is_better": True, "scaling": "weak",
@@ -917,9 +919,9 @@ def main():
             "graph": {"nnz": nnz, "bytes_per_spmm_step": B32, **build},
             "gpu_launches": args.steps * (T + 1),
             "roofline": {"bound": "hbm", "achieved": round(achieved, 2), "peak": peak, "unit": "GB/s",
-                         "frac": round(achieved / peak, 4), "traffic": profiled_traffic("spmm_row_f32_500k"),
+                         "frac": round(achieved / peak, 4), "traffic": profiled_traffic(traffic_profile),
                          "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum per launch, "
-                                           "profiles/spmm_row_f32_500k.md", "peak_kind": peak_kind,
+                                           f"profiles/{traffic_profile}.md", "peak_kind": peak_kind,
                          "kernel": f"SpMM plan kind {tuned['kind']} stage {tuned['stage']}",
                          "per_launch_ms": round(per_launch_ms, 5),
                          "gather_floor_ms": round(floor_ms, 5),

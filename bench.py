@@ -391,6 +391,16 @@ def bench_knn(torch, scl, reps, warmup, with_reference=True):
            "cells": n, "features": int(pts.shape[1]), "k": k, "e2e_ms": round(1e3 * float(np.median(ts)), 3),
            "device_ms": round(float(st["device_ms"]), 3),
            "distance_evaluations_per_s": round(n * (n - 1) / (st["device_ms"] * 1e-3), 1)}
+    # the same search with every distance on CUDA cores: the tensor-core filter must give the same bits
+    prev = scl.neighbors.set_kernel(1, m)
+    try:
+        ci, cd = scl.neighbors.knn(m, k, norms)
+        sc = scl.diffusion.last_stats(m.lib)
+    finally:
+        scl.neighbors.set_kernel(prev, m)
+    res.update({"kernel": "tensor cores (k_knn_tc)", "cuda_core_kernel_device_ms": round(float(sc["device_ms"]), 3),
+                "bit_identical_to_cuda_core_kernel": bool(np.array_equal(ci, gi) and
+                                                          np.array_equal(cd.view(np.uint32), gd.view(np.uint32)))})
     if with_reference:
         try:
             from oracle import ref

@@ -181,3 +181,23 @@ def test_knn_non_finite_values_replay_every_candidate():
     oi, od = port.knn_dense(Xd, norms, 10)
     np.testing.assert_array_equal(gd.view(np.uint8), od.view(np.uint8))
     np.testing.assert_array_equal(gi.astype(np.int64), oi)
+
+
+def test_knn_kernels_agree_on_a_large_mixture():
+    """100,000 cells of the benchmark's 50-D mixture, k = 30: the tensor-core
+    filter and the exact CUDA-core kernel return the same neighbours and
+    distances, bit for bit (the restatement is too slow at this size)."""
+    pts = scl.synthetic.mixture(100_000, seed=5).astype(np.float32)
+    n, d = pts.shape
+    ip = np.arange(0, (n + 1) * d, d, dtype=np.int64).astype(np.int32)
+    m = scl.CsrMatrix.wrap(ip, np.tile(np.arange(d, dtype=np.int32), n), pts.reshape(-1), (n, d))
+    norms = scl.neighbors.compute_norms(m)
+    prev = scl.neighbors.set_kernel(2, m)
+    try:
+        a = scl.neighbors.knn(m, 30, norms)
+        scl.neighbors.set_kernel(1, m)
+        b = scl.neighbors.knn(m, 30, norms)
+    finally:
+        scl.neighbors.set_kernel(prev, m)
+    np.testing.assert_array_equal(a[0], b[0])
+    np.testing.assert_array_equal(a[1].view(np.uint32), b[1].view(np.uint32))

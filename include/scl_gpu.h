@@ -76,10 +76,12 @@ SCL_EXPORT scl_error_t scl_gpu_graph_set_storage(scl_gpu_graph_t graph, scl_dtyp
 SCL_EXPORT scl_error_t scl_gpu_diffuse(scl_gpu_graph_t graph, const void* X, scl_dtype_t x_dtype, void* Y,
                                        scl_dtype_t y_dtype, int64_t n_features, int64_t n_steps, void* stream);
 
-/* Locality reordering used by scl_gpu_diffuse: mode 1 groups the rows of each
- * connected component together (P' = Pi P Pi^T, X gathered once and the result
- * scattered back on the last step); mode 0 drops it. Each row keeps its stored
- * entry order, so results are bit-identical with and without it. The
+/* Row reordering used by scl_gpu_diffuse (P' = Pi P Pi^T, X gathered once and
+ * the result scattered back on the last step): mode 1 groups the rows of each
+ * connected component together, longest rows first inside a component; mode 2
+ * puts the longest rows first across the whole graph; mode 0 drops it. Each
+ * row keeps its stored entry order, so results are bit-identical with and
+ * without it. The
  * permutation is rebuilt only by this call; value changes (normalize,
  * set_storage) are picked up automatically. Synchronises `stream`. */
 SCL_EXPORT scl_error_t scl_gpu_graph_reorder(scl_gpu_graph_t graph, int mode, void* stream);

@@ -244,7 +244,8 @@ SCL_EXPORT scl_error_t scl_gpu_diffuse(scl_gpu_graph_t graph, const void* X, scl
 
 SCL_EXPORT scl_error_t scl_gpu_graph_reorder(scl_gpu_graph_t graph, int mode, void* stream) {
   SCL_API_CHECK_NULL(graph, "Graph is null");
-  SCL_API_CHECK(mode == 0 || mode == 1, SCL_ERROR_INVALID_ARGUMENT, "reorder mode must be 0 (off) or 1 (components)");
+  SCL_API_CHECK(mode >= 0 && mode <= 2, SCL_ERROR_INVALID_ARGUMENT,
+                "reorder mode must be 0 (off), 1 (components) or 2 (longest rows first)");
   SCL_API_TRY
   ensure_device(graph);
   cudaStream_t s = as_stream(stream);
@@ -257,7 +258,7 @@ SCL_EXPORT scl_error_t scl_gpu_graph_reorder(scl_gpu_graph_t graph, int mode, vo
     }
   } else {
     auto r = std::make_unique<Reordered>();
-    build_reorder(graph->g.view(), *r, s);
+    build_reorder(graph->g.view(), *r, s, mode);
     graph->reo = std::move(r);
   }
   SCL_API_RETURN_OK;

@@ -232,7 +232,9 @@ struct Reordered {
 const Grouped& reordered_grouped(const Reordered& r, int C, cudaStream_t s);
 // One SpMM step on the permuted structure with `plan` (kind 13 runs on the grouped layout).
 void spmm_reordered(const Reordered& r, SpmmArgs a, const SpmmPlan& plan, cudaStream_t s);
-void build_reorder(const CsrView& g, Reordered& r, cudaStream_t s);
+// mode 1: connected components together, longest rows first inside each; mode 2: longest rows
+// first across the whole graph (no component labelling).
+void build_reorder(const CsrView& g, Reordered& r, cudaStream_t s, int mode = 1);
 void reorder_values(const void* vals, DType t, Reordered& r, cudaStream_t s);
 // Y = P^steps X0 through the permuted structure: X0 is gathered into permuted
 // order once, the last step scatters rows back (Y may equal X0).

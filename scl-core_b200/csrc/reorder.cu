@@ -150,7 +150,8 @@ int bits_for(int64_t n) {
 
 }  // namespace
 
-void build_reorder(const CsrView& g, Reordered& r, cudaStream_t s) {
+void build_reorder(const CsrView& g, Reordered& r, cudaStream_t s, int mode) {
+  SCL_REQUIRE(mode == 1 || mode == 2, kErrInvalidArgument, "reorder mode must be 1 (components) or 2 (lengths)");
   SCL_REQUIRE(g.n_rows == g.n_cols, kErrDimensionMismatch, "reordering needs a square matrix");
   SCL_REQUIRE(g.nnz < (1ll << 31) && g.n_rows < (1ll << 31), kErrInvalidArgument, "graph too large to reorder");
   const int64_t n = g.n_rows, nnz = g.nnz;
@@ -158,10 +159,11 @@ void build_reorder(const CsrView& g, Reordered& r, cudaStream_t s) {
   r.nnz = nnz;
   r.values_ok = false;
   DevBuf L(std::max<int64_t>(n, 1) * 4, s), changed(4, s);
-  k_cc_init<<<nblocks(n, 256), 256, 0, s>>>(L.as<int32_t>(), n);
   const int max_rounds = 4 * bits_for(std::max<int64_t>(n, 2)) + 16;
   int rounds = 0;
-  for (; rounds < max_rounds; ++rounds) {
+  if (mode == 2) SCL_CUDA(cudaMemsetAsync(L.p, 0, std::max<int64_t>(n, 1) * 4, s));  // one group: lengths only
+  else k_cc_init<<<nblocks(n, 256), 256, 0, s>>>(L.as<int32_t>(), n);
+  for (; mode == 1 && rounds < max_rounds; ++rounds) {
     SCL_CUDA(cudaMemsetAsync(changed.p, 0, 4, s));
     k_cc_hook<<<nblocks(n * 32, 256), 256, 0, s>>>(g.indptr, g.indices, n, L.as<int32_t>(), changed.as<int32_t>());
     k_cc_jump<<<nblocks(n, 256), 256, 0, s>>>(L.as<int32_t>(), n);

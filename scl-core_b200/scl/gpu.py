@@ -120,7 +120,8 @@ class GpuGraph:
         return self
 
     def reorder(self, mode: int = 1, stream=None) -> "GpuGraph":
-        """Group rows by connected component for the diffusion (results unchanged)."""
+        """Reorder rows for the diffusion (results unchanged): 1 = connected components together, longest
+        rows first inside each; 2 = longest rows first across the graph; 0 = off."""
         check_error(self._lib.scl_gpu_graph_reorder(self._h, int(mode), _stream_ptr(stream)), "reorder", self._lib)
         return self
 

@@ -270,6 +270,14 @@ SCL_EXPORT scl_error_t scl_gpu_residual_fp64(const void* X, scl_dtype_t x_dtype,
  * The choice is process-wide. previous (may be null) receives the old one. */
 SCL_EXPORT scl_error_t scl_gpu_knn_set_kernel(int kernel, int* previous);
 
+/* Test hook of the tensor-core kNN's bounded waits. No counterpart in
+ * scl-core. CTA `cta` of the following tensor-core searches never receives
+ * its first accumulator, so its epilogue's wait runs out after 2 s: the
+ * kernel then stops every role of that CTA, drains its copies and MMAs,
+ * frees its tensor memory and returns, and scl_knn reports
+ * SCL_ERROR_CONVERGENCE. Nothing faults. -1 switches the hook off. */
+SCL_EXPORT scl_error_t scl_gpu_knn_inject_stall(int64_t cta, void* stream);
+
 /* Diffusion that allocates no device memory. No counterpart in scl-core.
  *
  * For callers that cannot allocate GPU memory while they run: a framework

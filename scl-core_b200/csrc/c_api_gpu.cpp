@@ -590,6 +590,13 @@ SCL_EXPORT scl_error_t scl_gpu_spmm_inject_stall(int64_t warp, void* stream) {
   SCL_API_CATCH
 }
 
+SCL_EXPORT scl_error_t scl_gpu_knn_inject_stall(int64_t cta, void* stream) {
+  SCL_API_TRY
+  knn_tensor_inject_stall(cta, as_stream(stream));
+  SCL_API_RETURN_OK;
+  SCL_API_CATCH
+}
+
 SCL_EXPORT scl_error_t scl_gpu_residual_fp64(const void* X, scl_dtype_t x_dtype, const double* X_ref,
                                              int64_t n_rows, int64_t n_features, double rel_floor, double* out,
                                              void* stream) {

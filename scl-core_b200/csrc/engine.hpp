@@ -328,6 +328,8 @@ void knn_dense(const void* X, const void* norms, DType t, int64_t n, int d, int 
                cudaStream_t s);
 void knn_tensor(const void* X, const void* norms, DType t, int64_t n, int d, int k, void* idx, DType it, void* dist,
                 cudaStream_t s);
+// test hook: CTA `cta` of the next tensor-core kNN launches never sees its first accumulator (-1 = off)
+void knn_tensor_inject_stall(int64_t cta, cudaStream_t s);
 void row_norms_dense(const void* X, DType t, int64_t n, int d, void* out, cudaStream_t s);
 
 // Vector walks (walks.cu). walk_linear: x <- c_x x + c_p P x, `steps` times

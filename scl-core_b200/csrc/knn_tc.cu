@@ -63,6 +63,11 @@ PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder();  // spmm_bulk.cu
 
 namespace {
 
+// Test hook: the MMA thread of this CTA never signals its first accumulator,
+// so that CTA's epilogue wait runs out (the error path of the bounded waits,
+// exercised without any fault). -1 = off.
+__device__ long long g_knn_tc_stall_cta = -1;
+
 constexpr int kTcQ = 256;                   // queries per CTA: two MMAs of M = 128 share every candidate tile
 constexpr int kTcM = 128;                   // MMA M: tensor-memory lanes
 constexpr int kTcEpiWarps = kTcQ / 32;      // one epilogue thread per query
@@ -662,6 +667,7 @@ k_knn_tc(const __grid_constant__ CUtensorMap qmap, const __grid_constant__ CUten
       s_drain;
   __shared__ uint32_t s_tmem;
   __shared__ volatile int s_abort;
+  __shared__ volatile int s_never;  // drains wait for their copies and MMAs even after an abort
 
   // 1024-byte aligned operand area (the 128-byte swizzle repeats every 8 rows of 128 bytes)
   unsigned char* base = reinterpret_cast<unsigned char*>(
@@ -689,6 +695,7 @@ k_knn_tc(const __grid_constant__ CUtensorMap qmap, const __grid_constant__ CUten
     mbar_init(saddr(&s_acce), kTcQ);
     mbar_init(saddr(&s_drain), 1);
     s_abort = 0;
+    s_never = 0;
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
   }
@@ -741,9 +748,9 @@ k_knn_tc(const __grid_constant__ CUtensorMap qmap, const __grid_constant__ CUten
       // drain: every copy issued into the ring has landed before the CTA ends
       for (int s = 0; s < S; ++s) {
         const int64_t uses = issued / S + ((issued % S) > s ? 1 : 0);
-        if (uses > 0) mbar_wait(saddr(&s_full[s]), (unsigned)((uses - 1) & 1), &s_abort, kTcDrainNs);
+        if (uses > 0) mbar_wait(saddr(&s_full[s]), (unsigned)((uses - 1) & 1), &s_never, kTcDrainNs);
       }
-      if (resident) mbar_wait(saddr(&s_aload), 0, &s_abort, kTcDrainNs);
+      if (resident) mbar_wait(saddr(&s_aload), 0, &s_never, kTcDrainNs);
     }
   } else if (warp == kTcMmaWarp) {
     // ---------------- MMA issuer ----------------
@@ -758,6 +765,7 @@ k_knn_tc(const __grid_constant__ CUtensorMap qmap, const __grid_constant__ CUten
           break;
         }
         tc_fence_after();
+        const bool stall = t == 0 && g_knn_tc_stall_cta == (long long)blockIdx.x;
         for (int c = 0; c < nK; ++c, ++it) {
           const int s = (int)(it % S);
           const unsigned use = (unsigned)(it / S);
@@ -780,11 +788,11 @@ k_knn_tc(const __grid_constant__ CUtensorMap qmap, const __grid_constant__ CUten
           issued_any = true;
         }
         if (!ok) break;
-        umma_commit(saddr(&s_accf));  // the accumulators hold tile t
+        if (!stall) umma_commit(saddr(&s_accf));  // the accumulators hold tile t
       }
       if (issued_any) {  // no MMA in flight when the tensor memory is freed
         umma_commit(saddr(&s_drain));
-        mbar_wait(saddr(&s_drain), 0, &s_abort, kTcDrainNs);
+        mbar_wait(saddr(&s_drain), 0, &s_never, kTcDrainNs);
       }
     }
   } else {
@@ -899,6 +907,12 @@ void knn_tc_typed(const T* X, const T* norms, int64_t n, int d, int k, IT* idx, 
 }
 
 }  // namespace
+
+void knn_tensor_inject_stall(int64_t cta, cudaStream_t s) {
+  const long long v = cta;
+  SCL_CUDA(cudaMemcpyToSymbolAsync(g_knn_tc_stall_cta, &v, sizeof(v), 0, cudaMemcpyHostToDevice, s));
+  SCL_CUDA(cudaStreamSynchronize(s));
+}
 
 void knn_tensor(const void* X, const void* norms, DType t, int64_t n, int d, int k, void* idx, DType it, void* dist,
                 cudaStream_t s) {

@@ -201,3 +201,31 @@ def test_knn_kernels_agree_on_a_large_mixture():
         scl.neighbors.set_kernel(prev, m)
     np.testing.assert_array_equal(a[0], b[0])
     np.testing.assert_array_equal(a[1].view(np.uint32), b[1].view(np.uint32))
+
+
+def test_knn_tensor_wait_runs_out_without_fault():
+    """The tensor-core kernel's bounded waits: a host-set hook keeps one CTA's
+    first accumulator from ever being signalled. Its epilogue gives up after
+    2 s, the CTA drains and frees its tensor memory, scl_knn returns
+    SCL_ERROR_CONVERGENCE, and the library keeps working afterwards."""
+    m, Xd, norms = _dense_case(3000, 20, np.float32, seed=1)
+    lib = m.lib
+    k = 10
+    idx = np.zeros(3000 * k, np.int32)
+    dist = np.zeros(3000 * k, np.float32)
+    nr = np.ascontiguousarray(norms, np.float32)
+    prev = scl.neighbors.set_kernel(2, m)
+    try:
+        assert lib.scl_gpu_knn_inject_stall(3, None) == 0
+        rc = lib.scl_knn(m.handle, nr.ctypes.data_as(ctypes.POINTER(lib.real_type)), 3000, k,
+                         idx.ctypes.data_as(ctypes.POINTER(lib.index_type)),
+                         dist.ctypes.data_as(ctypes.POINTER(lib.real_type)))
+        assert rc == 54  # SCL_ERROR_CONVERGENCE
+        assert lib.scl_gpu_knn_inject_stall(-1, None) == 0
+        gi, gd = scl.neighbors.knn(m, k, norms)
+    finally:
+        lib.scl_gpu_knn_inject_stall(-1, None)
+        scl.neighbors.set_kernel(prev, m)
+    oi, od = port.knn_dense(Xd, norms, k)
+    np.testing.assert_array_equal(gd.view(np.uint8), od.view(np.uint8))
+    np.testing.assert_array_equal(gi.astype(np.int64), oi)

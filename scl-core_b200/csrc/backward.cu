@@ -212,7 +212,7 @@ __global__ void __launch_bounds__(256, (NCB == 1 && sizeof(T) == 4 && !FUSE) ? 3
 k_adj_quarter(const int64_t* __restrict__ tptr, const int32_t* __restrict__ tidx, const T* __restrict__ tval,
               const T* __restrict__ G1, const T* __restrict__ Xs, T* __restrict__ G0, T* __restrict__ gPt,
               int64_t n, const T* __restrict__ pval, const T* __restrict__ Xprev, T* __restrict__ Xnew,
-              int gp_accum) {
+              int gp_accum, const uint32_t* __restrict__ order, unsigned int* __restrict__ ticket) {
   constexpr int VEC = 16 / (int)sizeof(T);
   constexpr int CB = 8 * VEC;      // columns per block
   constexpr int F = NCB * CB;
@@ -222,16 +222,38 @@ k_adj_quarter(const int64_t* __restrict__ tptr, const int32_t* __restrict__ tidx
   const int q = lane >> 3, lq = lane & 7;
   const int e_own = lq * 4 + q;    // chunk entry whose dot this lane finishes
   const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
-  int64_t row = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  if (row >= n) return;
-  // Prefetch pipeline (as in the forward row kernel): bounds two rows ahead,
-  // the next chunk's (index, value) pairs one chunk ahead, the next row's
-  // X_s chunk one row ahead, each chunk's accumulator values at its start.
+  const int64_t w = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  if (w >= n) return;
+  // Rows are handed out dynamically: warp w starts with order[w], then takes
+  // ticket numbers (order[nw + ticket]) from a counter the host zeroed. With
+  // the long rows first in `order`, the warps finish within about one row of
+  // each other; a static grid stride over these heavy-tailed row lengths
+  // left the slowest warp with far more than the mean work. A row index of n
+  // means none is left (ticket numbers only grow, so every later one is n too).
+  auto take = [&]() -> unsigned {  // raw ticket, valid in lane 0
+    unsigned t = 0;
+    if (lane == 0) t = atomicAdd(ticket, 1u);
+    return t;
+  };
+  const int32_t nr = (int32_t)n;  // row indices are int32
+  const unsigned nw32 = (unsigned)nw;
+  auto row_at = [&](unsigned raw) -> int32_t {
+    const unsigned id = __shfl_sync(0xffffffffu, raw, 0) + nw32;
+    return id < (unsigned)nr ? (int32_t)order[id] : nr;
+  };
+  int32_t row = (int32_t)order[w];
+  int32_t r_nx = row_at(take());
+  int32_t r_nn = row_at(take());
+  unsigned raw_n3 = take();
+  // Prefetch pipeline (as in the forward row kernel): ticket three rows
+  // ahead, its row two ahead, bounds two rows ahead, the next chunk's (index,
+  // value) pairs one chunk ahead, the next row's X_s chunk one row ahead,
+  // each chunk's accumulator values at its start.
   int64_t s_cur = tptr[row], e_cur = tptr[row + 1];
   int64_t s_nx = 0, e_nx = 0;
-  if (row + nw < n) {
-    s_nx = tptr[row + nw];
-    e_nx = tptr[row + nw + 1];
+  if (r_nx < n) {
+    s_nx = tptr[r_nx];
+    e_nx = tptr[r_nx + 1];
   }
   auto fetch = [&](int64_t pos, int64_t end, int32_t& j, T& v, T& v2) {
     j = 0;
@@ -246,20 +268,21 @@ k_adj_quarter(const int64_t* __restrict__ tptr, const int32_t* __restrict__ tidx
   T xi[NCB][VEC], xn[NCB][VEC];
 #pragma unroll
   for (int c = 0; c < NCB; ++c) {
-    load_vec<T, VEC>(Xs + row * F + c * CB + lq * VEC, xi[c]);
+    load_vec<T, VEC>(Xs + (int64_t)row * F + c * CB + lq * VEC, xi[c]);
 #pragma unroll
     for (int i = 0; i < VEC; ++i) xn[c][i] = T(0);
-    if (row + nw < n) load_vec<T, VEC>(Xs + (row + nw) * F + c * CB + lq * VEC, xn[c]);
+    if (r_nx < n) load_vec<T, VEC>(Xs + (int64_t)r_nx * F + c * CB + lq * VEC, xn[c]);
   }
   int32_t j_c;
   T v_c, w_c;
   fetch(s_cur + lane, e_cur, j_c, v_c, w_c);
-  for (; row < n; row += nw) {
-    const int64_t nn = row + 2 * nw;
+  while (row < n) {
+    const int32_t r_n3 = row_at(raw_n3);  // the ticket taken one row ago
+    raw_n3 = take();
     int64_t s_nn = 0, e_nn = 0;
-    if (nn < n) {
-      s_nn = tptr[nn];
-      e_nn = tptr[nn + 1];
+    if (r_nn < n) {
+      s_nn = tptr[r_nn];
+      e_nn = tptr[r_nn + 1];
     }
     T acc[NCB][VEC], accf[NCB][VEC];
 #pragma unroll
@@ -345,14 +368,14 @@ k_adj_quarter(const int64_t* __restrict__ tptr, const int32_t* __restrict__ tidx
         acc[c][i] = acc[c][i] + __shfl_xor_sync(0xffffffffu, acc[c][i], 8);
         acc[c][i] = acc[c][i] + __shfl_xor_sync(0xffffffffu, acc[c][i], 16);
       }
-      if (q == 0) store_vec<T, VEC>(G0 + row * F + c * CB + lq * VEC, acc[c]);
+      if (q == 0) store_vec<T, VEC>(G0 + (int64_t)row * F + c * CB + lq * VEC, acc[c]);
       if constexpr (FUSE) {
 #pragma unroll
         for (int i = 0; i < VEC; ++i) {
           accf[c][i] = accf[c][i] + __shfl_xor_sync(0xffffffffu, accf[c][i], 8);
           accf[c][i] = accf[c][i] + __shfl_xor_sync(0xffffffffu, accf[c][i], 16);
         }
-        if (q == 0) store_vec<T, VEC>(Xnew + row * F + c * CB + lq * VEC, accf[c]);
+        if (q == 0) store_vec<T, VEC>(Xnew + (int64_t)row * F + c * CB + lq * VEC, accf[c]);
       }
     }
     // rotate: next row's X_s chunk is in xn; fetch the one after it
@@ -360,12 +383,15 @@ k_adj_quarter(const int64_t* __restrict__ tptr, const int32_t* __restrict__ tidx
     for (int c = 0; c < NCB; ++c) {
 #pragma unroll
       for (int i = 0; i < VEC; ++i) xi[c][i] = xn[c][i];
-      if (nn < n) load_vec<T, VEC>(Xs + nn * F + c * CB + lq * VEC, xn[c]);
+      if (r_nn < n) load_vec<T, VEC>(Xs + (int64_t)r_nn * F + c * CB + lq * VEC, xn[c]);
     }
     s_cur = s_nx;
     e_cur = e_nx;
     s_nx = s_nn;
     e_nx = e_nn;
+    row = r_nx;
+    r_nx = r_nn;
+    r_nn = r_n3;
   }
 }
 
@@ -376,64 +402,141 @@ __global__ void k_differ(const I* __restrict__ a, const I* __restrict__ b, int64
     if (a[i] != b[i]) flag[0] = 1;
 }
 
+// sort key of a row of P^T: rows longer than thr by decreasing length, then
+// every other row (one key, so a stable sort keeps their index order)
+__global__ void k_order_keys(const int64_t* __restrict__ ptr, int64_t n, int64_t thr, uint64_t* __restrict__ keys,
+                             uint32_t* __restrict__ rows) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t len = ptr[i + 1] - ptr[i];
+    keys[i] = len > thr ? 0xffffffffull - (uint64_t)(len < 0xfffffffell ? len : 0xfffffffell) : 0xffffffffull;
+    rows[i] = (uint32_t)i;
+  }
+}
+
 __global__ void k_invert_map(const int32_t* __restrict__ map, int64_t nnz, int32_t* __restrict__ inv) {
   for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < nnz; q += (int64_t)gridDim.x * blockDim.x)
     inv[map[q]] = (int32_t)q;
 }
 
-// Normalisation backward in one pass over P's rows (warp per row): gP of
-// entry p is read from the CSC-order accumulator through the inverse map, u_i
-// is reduced in FP64, then every entry's dW is written; v (symmetric mode) is
-// the CSC row dot computed beforehand.
-template <class T>
-__global__ void k_norm_bwd_gather(const int64_t* __restrict__ ptr, const int32_t* __restrict__ idx,
-                                  const T* __restrict__ P, const T* __restrict__ gPt, const int32_t* __restrict__ inv,
-                                  const double* __restrict__ deg, const double* __restrict__ v, int64_t n,
-                                  int symmetric, T* __restrict__ dW) {
-  const int64_t row = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
-  const int lane = threadIdx.x & 31;
-  if (row >= n) return;
-  const int64_t s0 = ptr[row], s1 = ptr[row + 1];
-  // The first KEEP entries per lane (rows up to 32*KEEP entries, the common
-  // case) are gathered once, all in flight together, and kept in registers
-  // for the second pass; longer rows gather the rest twice. Each lane still
-  // sums its entries in increasing position order.
-  constexpr int KEEP = 4;
-  double gk[KEEP];
+// Normalisation backward in one pass over P's rows: gP of entry p is read
+// from the CSC-order accumulator through the inverse map, u_i = sum_p gP P is
+// reduced in FP64, then every entry's dW is written; v (symmetric mode) is the
+// CSC row dot computed beforehand. Sixteen lanes per row, two rows per warp:
+// each lane holds up to KEEP entries of its row in registers, and every load
+// a row needs (bounds, degree, v, inverse map, P, the gathers) is issued before
+// the reduction, so the dependent chain per row is bounds -> map -> gather.
+// Rows longer than LPR * KEEP entries gather the rest in batches of TB loads
+// per lane and park gP in dW until u is known.
+template <class T, bool SYM>
+__global__ void __launch_bounds__(256) k_norm_bwd_gather(const int64_t* __restrict__ ptr,
+                                                         const int32_t* __restrict__ idx, const T* __restrict__ P,
+                                                         const T* __restrict__ gPt, const int32_t* __restrict__ inv,
+                                                         const double* __restrict__ deg,
+                                                         const double* __restrict__ v, int64_t n,
+                                                         T* __restrict__ dW) {
+  constexpr int KEEP = 8, LPR = 16, TB = 8;
+  const int64_t row = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) / LPR;
+  const int l = threadIdx.x & (LPR - 1);
+  const bool has_row = row < n;
+  int64_t s0 = 0, s1 = 0;
+  double di = 0.0, vi = 0.0;
+  if (has_row) {
+    s0 = ptr[row];
+    s1 = ptr[row + 1];
+    di = deg[row];
+    if (SYM) vi = v[row];
+  }
+  T gk[KEEP], pk[KEEP];
+  double ak[SYM ? KEEP : 1];
+  int32_t q[KEEP];
+#pragma unroll
+  for (int k = 0; k < KEEP; ++k) {
+    const int64_t p = s0 + l + LPR * k;
+    q[k] = 0;
+    pk[k] = T(0);
+    if (p < s1) {
+      q[k] = inv[p];
+      pk[k] = P[p];
+    }
+  }
+  if (SYM) {
+#pragma unroll
+    for (int k = 0; k < KEEP; ++k) {
+      const int64_t p = s0 + l + LPR * k;
+      ak[k] = 0.0;
+      if (p < s1) ak[k] = deg[idx[p]];
+    }
+  }
+#pragma unroll
+  for (int k = 0; k < KEEP; ++k) {
+    const int64_t p = s0 + l + LPR * k;
+    gk[k] = T(0);
+    if (p < s1) gk[k] = gPt[q[k]];
+  }
   double u = 0.0;
 #pragma unroll
-  for (int k = 0; k < KEEP; ++k) {
-    const int64_t p = s0 + lane + 32 * k;
-    gk[k] = 0.0;
-    if (p < s1) gk[k] = (double)gPt[inv[p]];
+  for (int k = 0; k < KEEP; ++k) u += (double)gk[k] * (double)pk[k];  // zero past the row's end
+  // rest of a long row: gathered once in batches of TB loads per lane; gP is
+  // parked in dW and rewritten with the gradient below
+  for (int64_t base = s0 + l + LPR * KEEP; base < s1; base += LPR * TB) {
+    int32_t qt[TB];
+    T pt[TB];
+#pragma unroll
+    for (int k = 0; k < TB; ++k) {
+      const int64_t p = base + LPR * k;
+      qt[k] = 0;
+      pt[k] = T(0);
+      if (p < s1) {
+        qt[k] = inv[p];
+        pt[k] = P[p];
+      }
+    }
+#pragma unroll
+    for (int k = 0; k < TB; ++k) {
+      const int64_t p = base + LPR * k;
+      if (p < s1) {
+        const T g = gPt[qt[k]];
+        u += (double)g * (double)pt[k];
+        dW[p] = g;
+      }
+    }
   }
 #pragma unroll
-  for (int k = 0; k < KEEP; ++k) {
-    const int64_t p = s0 + lane + 32 * k;
-    if (p < s1) u += gk[k] * (double)P[p];
-  }
-  for (int64_t p = s0 + lane + 32 * KEEP; p < s1; p += 32) u += (double)gPt[inv[p]] * (double)P[p];
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) u += __shfl_xor_sync(0xffffffffu, u, o);
-  const double di = deg[row];
+  for (int o = LPR / 2; o > 0; o >>= 1) u += __shfl_xor_sync(0xffffffffu, u, o);
+  if (!has_row) return;
   const bool live = di > kMinProbB;
   const double ai = live ? 1.0 / sqrt(di) : 0.0;
-  const double shift = live ? (symmetric ? (u + v[row]) / (2.0 * di) : u) : 0.0;
-  auto grad = [&](int64_t p, double gp) -> double {
+  const double rdi = live ? 1.0 / di : 0.0;
+  const double shift = live ? (SYM ? (u + vi) * (0.5 * rdi) : u) : 0.0;
+  auto grad = [&](double gp, double dj) -> double {
     if (!live) return 0.0;
-    if (symmetric) {
-      const double dj = deg[idx[p]];
-      const double aj = dj > kMinProbB ? 1.0 / sqrt(dj) : 0.0;
-      return gp * ai * aj - shift;
-    }
-    return (gp - shift) / di;
+    if (SYM) return gp * ai * (dj > kMinProbB ? 1.0 / sqrt(dj) : 0.0) - shift;
+    return (gp - shift) * rdi;
   };
 #pragma unroll
   for (int k = 0; k < KEEP; ++k) {
-    const int64_t p = s0 + lane + 32 * k;
-    if (p < s1) dW[p] = (T)grad(p, gk[k]);
+    const int64_t p = s0 + l + LPR * k;
+    if (p < s1) dW[p] = (T)grad((double)gk[k], SYM ? ak[k] : 0.0);
   }
-  for (int64_t p = s0 + lane + 32 * KEEP; p < s1; p += 32) dW[p] = (T)grad(p, (double)gPt[inv[p]]);
+  for (int64_t base = s0 + l + LPR * KEEP; base < s1; base += LPR * TB) {
+    T gt[TB];
+    double dj[TB];
+#pragma unroll
+    for (int k = 0; k < TB; ++k) {
+      const int64_t p = base + LPR * k;
+      gt[k] = T(0);
+      dj[k] = 0.0;
+      if (p < s1) {
+        gt[k] = dW[p];
+        if (SYM) dj[k] = deg[idx[p]];
+      }
+    }
+#pragma unroll
+    for (int k = 0; k < TB; ++k) {
+      const int64_t p = base + LPR * k;
+      if (p < s1) dW[p] = (T)grad((double)gt[k], dj[k]);
+    }
+  }
 }
 
 template <class T>
@@ -478,8 +581,9 @@ void launch_adj(const CsrView& t, const T* G1, const T* Xs, T* G0, T* gPt, int g
 }
 
 template <class T, int NCB, int U, bool FUSE = false>
-void launch_adj_quarter(const CsrView& t, const T* G1, const T* Xs, T* G0, T* gPt, int gp_accum, cudaStream_t s,
-                        const T* pval = nullptr, const T* Xprev = nullptr, T* Xnew = nullptr) {
+void launch_adj_quarter(const CsrView& t, const uint32_t* order, unsigned int* ticket, const T* G1, const T* Xs,
+                        T* G0, T* gPt, int gp_accum, cudaStream_t s, const T* pval = nullptr,
+                        const T* Xprev = nullptr, T* Xnew = nullptr) {
   auto kern = k_adj_quarter<T, NCB, U, FUSE>;
   int dev = 0, per_sm = 0;
   SCL_CUDA(cudaGetDevice(&dev));
@@ -487,7 +591,7 @@ void launch_adj_quarter(const CsrView& t, const T* G1, const T* Xs, T* G0, T* gP
   const int64_t need = (t.n_rows * 32 + 255) / 256;
   const int64_t grid = std::max<int64_t>(1, std::min<int64_t>(need, (int64_t)std::max(per_sm, 1) * sm_count(dev)));
   kern<<<(unsigned)grid, 256, 0, s>>>(t.indptr, t.indices, static_cast<const T*>(t.values), G1, Xs, G0, gPt,
-                                      t.n_rows, pval, Xprev, Xnew, gp_accum);
+                                      t.n_rows, pval, Xprev, Xnew, gp_accum, order, ticket);
   SCL_CUDA(cudaGetLastError());
 }
 
@@ -501,20 +605,22 @@ bool adj_fusable(int64_t F, const void* a, const void* b, const void* c, const v
 }
 
 template <class T>
-void adj_step_fused(const CsrView& t, const T* pval, const T* G1, const T* Xs, T* G0, T* gPt, int gp_accum,
-                    const T* Xprev, T* Xnew, cudaStream_t s) {
-  launch_adj_quarter<T, 1, 4, true>(t, G1, Xs, G0, gPt, gp_accum, s, pval, Xprev, Xnew);
+void adj_step_fused(const CsrView& t, const uint32_t* order, unsigned int* ticket, const T* pval, const T* G1,
+                    const T* Xs, T* G0, T* gPt, int gp_accum, const T* Xprev, T* Xnew, cudaStream_t s) {
+  launch_adj_quarter<T, 1, 4, true>(t, order, ticket, G1, Xs, G0, gPt, gp_accum, s, pval, Xprev, Xnew);
 }
 
+// ticket: a zeroed counter of its own for the quarter-warp kernels' row hand-out
 template <class T>
-void adj_step(const CsrView& t, const T* G1, const T* Xs, T* G0, T* gPt, int gp_accum, int64_t F, cudaStream_t s) {
+void adj_step(const CsrView& t, const uint32_t* order, unsigned int* ticket, const T* G1, const T* Xs, T* G0,
+              T* gPt, int gp_accum, int64_t F, cudaStream_t s) {
   constexpr int kV16 = 16 / (int)sizeof(T);
   const auto al = [&](const void* p, int b) { return (reinterpret_cast<uintptr_t>(p) % (uintptr_t)b) == 0; };
   // quarter-warp kernel: rows of 1, 2 or 4 blocks of 8 sixteen-byte chunks
   if (al(G1, 16) && al(Xs, 16) && al(G0, 16)) {
-    if (F == 8 * kV16) return launch_adj_quarter<T, 1, 4>(t, G1, Xs, G0, gPt, gp_accum, s);
-    if (F == 16 * kV16) return launch_adj_quarter<T, 2, 4>(t, G1, Xs, G0, gPt, gp_accum, s);
-    if (F == 32 * kV16) return launch_adj_quarter<T, 4, 4>(t, G1, Xs, G0, gPt, gp_accum, s);
+    if (F == 8 * kV16) return launch_adj_quarter<T, 1, 4>(t, order, ticket, G1, Xs, G0, gPt, gp_accum, s);
+    if (F == 16 * kV16) return launch_adj_quarter<T, 2, 4>(t, order, ticket, G1, Xs, G0, gPt, gp_accum, s);
+    if (F == 32 * kV16) return launch_adj_quarter<T, 4, 4>(t, order, ticket, G1, Xs, G0, gPt, gp_accum, s);
   }
   // one 16-byte chunk per lane when the row fits one column block of the warp
   if (F % kV16 == 0 && F <= 32 * kV16 && F > 16 * kV16 && al(G1, 16) && al(Xs, 16) && al(G0, 16))
@@ -538,6 +644,20 @@ void build_adjoint(const DeviceCSR& g, Adjoint& a, cudaStream_t s) {
     k_invert_map<<<std::min<unsigned>(nblk(g.nnz, 256), 148u * 16u), 256, 0, s>>>(a.tmap.as<int32_t>(), g.nnz,
                                                                                    a.tinv.as<int32_t>());
     SCL_CUDA(cudaGetLastError());
+  }
+  // processing order of P^T's rows: those over twice the mean length first,
+  // longest first, then the rest in index order (a stable sort on the key)
+  const int64_t n = a.t.n_rows;
+  a.order = DevBuf(std::max<int64_t>(n, 1) * 4, s);
+  if (n > 0) {
+    const int64_t thr = std::max<int64_t>(32, 2 * ((g.nnz + n - 1) / n));
+    DevBuf keys(n * 8, s), keys2(n * 8, s), rows(n * 4, s);
+    k_order_keys<<<std::min<unsigned>(nblk(n, 256), 148u * 8u), 256, 0, s>>>(a.t.indptr.as<int64_t>(), n, thr,
+                                                                           keys.as<uint64_t>(),
+                                                                           rows.as<uint32_t>());
+    SCL_CUDA(cudaGetLastError());
+    radix_sort_pairs(keys.as<uint64_t>(), rows.as<uint32_t>(), keys2.as<uint64_t>(), a.order.as<uint32_t>(), n,
+                     32, s);
   }
   // a structurally symmetric P (the kNN union graphs) has P^T's structure:
   // then one pass over it can serve P and P^T together (fused recompute)
@@ -663,6 +783,10 @@ static void backward_typed(const CsrView& g, const Adjoint& adj, const T* X0, co
     return;
   }
   int gp_accum = 0;  // the first backward step writes the accumulator
+  SCL_REQUIRE(adj.order.p != nullptr, kErrInternal, "adjoint row order is missing");
+  const uint32_t* order = adj.order.as<uint32_t>();
+  DevBuf tickets((size_t)steps * sizeof(unsigned int), s);  // one row counter per step
+  SCL_CUDA(cudaMemsetAsync(tickets.p, 0, (size_t)steps * sizeof(unsigned int), s));
   const int64_t seg = std::min<int64_t>(every, steps);
   // recomputed iterates: two buffer sets, the segment being walked and the
   // (earlier) segment being recomputed alongside it
@@ -722,13 +846,13 @@ static void backward_typed(const CsrView& g, const Adjoint& adj, const T* X0, co
       T* Gnext = (st == 0) ? dX0 : ((Gcur == Ga.as<T>()) ? Gb.as<T>() : Ga.as<T>());
       if (fuse && has_next && mn < c) {
         if (!bn[mn - cn].p) bn[mn - cn] = DevBuf(blk, s);
-        adj_step_fused<T>(tv, static_cast<const T*>(g.values), Gcur, X[st - c], Gnext, gPt, gp_accum,
-                          Xn[mn - cn - 1], bn[mn - cn].as<T>(), s);
+        adj_step_fused<T>(tv, order, tickets.as<unsigned int>() + st, static_cast<const T*>(g.values), Gcur,
+                          X[st - c], Gnext, gPt, gp_accum, Xn[mn - cn - 1], bn[mn - cn].as<T>(), s);
         Xn[mn - cn] = bn[mn - cn].as<T>();
         ++mn;
         advance();
       } else {
-        adj_step<T>(tv, Gcur, X[st - c], Gnext, gPt, gp_accum, F, s);
+        adj_step<T>(tv, order, tickets.as<unsigned int>() + st, Gcur, X[st - c], Gnext, gPt, gp_accum, F, s);
       }
       gp_accum = 1;
       Gcur = Gnext;
@@ -766,9 +890,9 @@ static void norm_bwd_typed(const CsrView& P, const Adjoint& adj, const T* gPt, c
   if (symmetric)  // v_i = sum over column i of P of gP * P: a row dot over the CSC view
     k_row_dot<T><<<nblk(n * 32, 256), 256, 0, s>>>(adj.t.indptr.as<int64_t>(), gPt, adj.t.values.as<T>(), n,
                                                    v.as<double>());
-  k_norm_bwd_gather<T><<<nblk(n * 32, 256), 256, 0, s>>>(P.indptr, P.indices, static_cast<const T*>(P.values), gPt,
-                                                         adj.tinv.as<int32_t>(), degrees, v.as<double>(), n,
-                                                         symmetric, dW);
+  auto kern = symmetric ? k_norm_bwd_gather<T, true> : k_norm_bwd_gather<T, false>;
+  kern<<<nblk(n * 16, 256), 256, 0, s>>>(P.indptr, P.indices, static_cast<const T*>(P.values), gPt,
+                                        adj.tinv.as<int32_t>(), degrees, v.as<double>(), n, dW);
   SCL_CUDA(cudaGetLastError());
 }
 

@@ -278,6 +278,8 @@ struct Adjoint {
   DevBuf tinv;    // int32[nnz]: entry p of P is entry tinv[p] of P^T
   bool values_ok = false;
   bool sym_structure = false;  // P^T has P's indptr and indices (P's values need no remap)
+  DevBuf order;   // uint32[n]: rows of P^T in the order the backward steps take them
+                  // (rows over twice the mean length first, longest first; then the rest in index order)
 };
 void build_adjoint(const DeviceCSR& g, Adjoint& a, cudaStream_t s);
 void adjoint_values(const void* vals, DType t, Adjoint& a, cudaStream_t s);

@@ -691,8 +691,12 @@ SCL_EXPORT scl_error_t scl_gpu_graph_autotune(scl_gpu_graph_t graph, int64_t n_f
   const int r = std::max(reps, 1);
   try {
     auto step = [&](const SpmmPlan& p) {
-      if (graph->reo) spmm_reordered(*graph->reo, a, p, s);
-      else spmm_with_plan(a, p, s);
+      if (graph->reo) {
+        attach_schedule(*graph->reo, a, p, s);  // as the diffusion runs it
+        spmm_reordered(*graph->reo, a, p, s);
+      } else {
+        spmm_with_plan(a, p, s);
+      }
     };
     for (const SpmmPlan& p : cands) {
       step(p);  // warm-up (also validates the shape and builds any layout it needs)

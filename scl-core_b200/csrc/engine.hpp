@@ -147,6 +147,10 @@ struct SpmmArgs {
   void* Y;         // n_rows x F, row-major
   DType ytype;
   const int32_t* row_map = nullptr;  // optional: output row r is written to Y[row_map[r]]
+  // optional for plan kind 12: a per-warp list of row groups (warp_schedule),
+  // used when the launch has exactly sched_warps warps
+  const int32_t* sched = nullptr;
+  int64_t sched_warps = 0;
 };
 // Launch shape of the SpMM kernel: `group` lanes own one output row and each
 // lane owns `vec` contiguous columns (16 bytes of X) per pass; vec == 1 is the
@@ -227,7 +231,23 @@ struct Reordered {
   uint64_t values_version = 0;  // bumped whenever `values` is rewritten
   // grouped layouts of the permuted structure for C = 1, 2, 4 rows per warp (built on first use)
   mutable std::unique_ptr<Grouped> grouped[3];
+  // plan kind 12's warp schedules for groups of 1, 2, 4 rows (built on first use) and their warp counts
+  mutable DevBuf sched[3];
+  mutable int64_t sched_warps[3] = {0, 0, 0};
 };
+// Warps of a plan kind 12 launch (multi-row kernel, `stage` gathers per batch)
+// over n_rows rows of F values of type t.
+int64_t rows16_warps(int64_t F, DType t, int stage, int64_t n_rows);
+// Static schedule of the groups of R consecutive rows over nw warps, built on
+// the host from the row lengths: groups whose longest row is over eight times
+// the mean row length are dealt first, longest first, each to the least-loaded
+// warp; then every other group in index order to the least-loaded warp (cost
+// = longest row + 8). Each warp's list starts with its long groups. Layout:
+// int32[nw + 1] list offsets, then int32[groups] group ids.
+DevBuf warp_schedule(const int64_t* indptr, int64_t n, int R, int64_t nw, cudaStream_t s);
+// Sets a.sched / a.sched_warps for a plan kind 12 step on r's structure (the
+// schedule is built on first use and kept in r); clears them for other plans.
+void attach_schedule(const Reordered& r, SpmmArgs& a, const SpmmPlan& plan, cudaStream_t s);
 // The grouped layout for C rows per warp with current values (built or refreshed on demand).
 const Grouped& reordered_grouped(const Reordered& r, int C, cudaStream_t s);
 // One SpMM step on the permuted structure with `plan` (kind 13 runs on the grouped layout).

@@ -17,6 +17,9 @@
 
 #include <algorithm>
 
+#include <queue>
+#include <vector>
+
 #include "engine.hpp"
 
 namespace sclgpu {
@@ -158,6 +161,10 @@ void build_reorder(const CsrView& g, Reordered& r, cudaStream_t s, int mode) {
   r.n = n;
   r.nnz = nnz;
   r.values_ok = false;
+  for (int i = 0; i < 3; ++i) {
+    r.sched[i] = DevBuf();
+    r.sched_warps[i] = 0;
+  }
   DevBuf L(std::max<int64_t>(n, 1) * 4, s), changed(4, s);
   const int max_rounds = 4 * bits_for(std::max<int64_t>(n, 2)) + 16;
   int rounds = 0;
@@ -191,6 +198,70 @@ void build_reorder(const CsrView& g, Reordered& r, cudaStream_t s, int mode) {
                                                        r.iperm.as<int32_t>(), r.indptr.as<int64_t>(), n,
                                                        r.indices.as<int32_t>(), r.emap.as<int32_t>());
   SCL_CUDA(cudaGetLastError());
+}
+
+DevBuf warp_schedule(const int64_t* indptr, int64_t n, int R, int64_t nw, cudaStream_t s) {
+  SCL_REQUIRE(R >= 1 && nw >= 1 && n < (1ll << 31), kErrInvalidArgument, "bad warp schedule request");
+  const int64_t ng = (n + R - 1) / R;
+  std::vector<int64_t> ip(n + 1);
+  SCL_CUDA(cudaMemcpyAsync(ip.data(), indptr, (n + 1) * sizeof(int64_t), cudaMemcpyDeviceToHost, s));
+  SCL_CUDA(cudaStreamSynchronize(s));
+  std::vector<int64_t> len(ng, 0);
+  for (int64_t g = 0; g < ng; ++g)
+    for (int64_t r = g * R; r < std::min<int64_t>(n, g * R + R); ++r) len[g] = std::max(len[g], ip[r + 1] - ip[r]);
+  const int64_t thr = 8 * std::max<int64_t>(1, (ip[n] + n - 1) / std::max<int64_t>(n, 1));
+  std::vector<int32_t> hubs;
+  for (int64_t g = 0; g < ng; ++g)
+    if (len[g] > thr) hubs.push_back((int32_t)g);
+  std::stable_sort(hubs.begin(), hubs.end(), [&](int32_t a, int32_t b) { return len[a] > len[b]; });
+  using Slot = std::pair<int64_t, int64_t>;  // (load, warp)
+  std::priority_queue<Slot, std::vector<Slot>, std::greater<Slot>> heap;
+  for (int64_t w = 0; w < nw; ++w) heap.push({0, w});
+  std::vector<int32_t> owner(ng);
+  auto deal = [&](int64_t g) {
+    Slot t = heap.top();
+    heap.pop();
+    owner[g] = (int32_t)t.second;
+    heap.push({t.first + len[g] + 8, t.second});
+  };
+  std::vector<char> is_hub(ng, 0);
+  for (int32_t g : hubs) {
+    is_hub[g] = 1;
+    deal(g);
+  }
+  for (int64_t g = 0; g < ng; ++g)
+    if (!is_hub[g]) deal(g);
+  // CSR of the lists: a warp's long groups first (in dealing order), then its others by index
+  std::vector<int32_t> out(nw + 1 + ng), cnt(nw + 1, 0);
+  for (int64_t g = 0; g < ng; ++g) ++cnt[owner[g] + 1];
+  for (int64_t w = 0; w < nw; ++w) cnt[w + 1] += cnt[w];
+  for (int64_t w = 0; w <= nw; ++w) out[w] = cnt[w];
+  std::vector<int32_t> fill(cnt.begin(), cnt.end() - 1);
+  for (int32_t g : hubs) out[nw + 1 + fill[owner[g]]++] = g;
+  for (int64_t g = 0; g < ng; ++g)
+    if (!is_hub[g]) out[nw + 1 + fill[owner[g]]++] = (int32_t)g;
+  DevBuf d(out.size() * sizeof(int32_t), s);
+  SCL_CUDA(cudaMemcpyAsync(d.p, out.data(), out.size() * sizeof(int32_t), cudaMemcpyHostToDevice, s));
+  SCL_CUDA(cudaStreamSynchronize(s));  // `out` is released on return
+  return d;
+}
+
+void attach_schedule(const Reordered& r, SpmmArgs& a, const SpmmPlan& plan, cudaStream_t s) {
+  a.sched = nullptr;
+  a.sched_warps = 0;
+  const int64_t rowb = a.F * (int64_t)dtype_size(a.xtype);
+  if (plan.kind != 12 || a.xtype != a.vtype || !(a.xtype == kF32 || a.xtype == kF64) ||
+      !(rowb == 128 || rowb == 256 || rowb == 512))
+    return;
+  const int R = (int)(512 / rowb), slot = R == 1 ? 0 : (R == 2 ? 1 : 2);
+  const int64_t nw = rows16_warps(a.F, a.xtype, plan.stage, r.n);
+  if (nw <= 0) return;
+  if (r.sched_warps[slot] != nw) {
+    r.sched[slot] = warp_schedule(r.indptr.as<int64_t>(), r.n, R, nw, s);
+    r.sched_warps[slot] = nw;
+  }
+  a.sched = r.sched[slot].as<int32_t>();
+  a.sched_warps = nw;
 }
 
 void reorder_values(const void* vals, DType t, Reordered& r, cudaStream_t s) {
@@ -287,6 +358,7 @@ void diffuse_reordered(const Reordered& r, const void* X0, DType xtype, void* Y,
     a.Y = dst;
     a.ytype = ot;
     const SpmmPlan plan = plan_in ? *plan_in : default_spmm_plan(F, mtype, src, dst, ot);
+    attach_schedule(r, a, plan, s);
     spmm_reordered(r, a, plan, s);
     src = dst;
   }

@@ -695,7 +695,8 @@ k_spmm_row(const int64_t* __restrict__ indptr, const int32_t* __restrict__ indic
 template <class T, int ROWB, int U, int MINB>
 __global__ void __launch_bounds__(kSpmmThreads, MINB)
 k_spmm_rows16(const int64_t* __restrict__ indptr, const int32_t* __restrict__ indices, const T* __restrict__ values,
-              const T* __restrict__ X, T* __restrict__ Y, const int32_t* __restrict__ row_map, int64_t n_rows) {
+              const T* __restrict__ X, T* __restrict__ Y, const int32_t* __restrict__ row_map, int64_t n_rows,
+              const int32_t* __restrict__ sched) {
   constexpr int L = ROWB / 16;
   constexpr int R = 32 / L;
   constexpr int VEC = 16 / (int)sizeof(T);
@@ -710,7 +711,29 @@ k_spmm_rows16(const int64_t* __restrict__ indptr, const int32_t* __restrict__ in
   const int lq = lane % L;
   const int64_t n_grp = (n_rows + R - 1) / R;
   const int64_t nw = ((int64_t)gridDim.x * kSpmmThreads) >> 5;
-  int64_t grp = ((int64_t)blockIdx.x * kSpmmThreads + threadIdx.x) >> 5;
+  const int64_t w_id = ((int64_t)blockIdx.x * kSpmmThreads + threadIdx.x) >> 5;
+  // Groups of R rows: without a schedule warp w takes groups w, w + nw, ...
+  // (a static grid stride); with one it takes its list sched[w] ..
+  // sched[w + 1] - 1 of the group ids stored after the nw + 1 offsets. The
+  // lists balance the warps' work (the longest groups first, each on a
+  // lightly loaded warp); on the grid stride the warps that drew the longest
+  // rows finished last. n_grp means no group is left.
+  const int32_t* __restrict__ glist = sched ? sched + nw + 1 : nullptr;
+  int64_t g_seq = w_id, q_next = 0, q_end = 0;
+  auto next_group = [&]() -> int64_t {
+    if (sched == nullptr) {
+      g_seq += nw;
+      return g_seq < n_grp ? g_seq : n_grp;
+    }
+    const int64_t qp = q_next++;
+    return qp < q_end ? (int64_t)glist[qp] : n_grp;
+  };
+  int64_t grp = w_id;
+  if (sched != nullptr) {
+    q_next = sched[w_id];
+    q_end = sched[w_id + 1];
+    grp = q_next < q_end ? (int64_t)glist[q_next++] : n_grp;
+  }
   if (grp >= n_grp) return;
   const char* __restrict__ Xl = reinterpret_cast<const char*>(X) + lq * 16;
   auto gather = [&](int32_t j) -> uint4 {
@@ -744,9 +767,11 @@ k_spmm_rows16(const int64_t* __restrict__ indptr, const int32_t* __restrict__ in
       s_v[w][b][q * 32 + lq + L * k] = v[k];
     }
   };
+  int64_t g_nx = next_group();
+  int64_t g_nn = next_group();
   int64_t s_cur, e_cur, s_nx, e_nx;
   bounds(grp, s_cur, e_cur);
-  bounds(grp + nw, s_nx, e_nx);
+  bounds(g_nx, s_nx, e_nx);
   int buf = 0;
   {
     int32_t j[R];
@@ -755,9 +780,10 @@ k_spmm_rows16(const int64_t* __restrict__ indptr, const int32_t* __restrict__ in
     publish(0, j, v);
     __syncwarp();
   }
-  for (; grp < n_grp; grp += nw) {
+  while (grp < n_grp) {
+    const int64_t g_n3 = next_group();  // its id is read a group ahead of its bounds
     int64_t s_nn, e_nn;
-    bounds(grp + 2 * nw, s_nn, e_nn);
+    bounds(g_nn, s_nn, e_nn);
     const int len = (int)(e_cur - s_cur);
     int maxlen = len, minlen = len;
 #pragma unroll
@@ -843,6 +869,9 @@ k_spmm_rows16(const int64_t* __restrict__ indptr, const int32_t* __restrict__ in
     e_cur = e_nx;
     s_nx = s_nn;
     e_nx = e_nn;
+    grp = g_nx;
+    g_nx = g_nn;
+    g_nn = g_n3;
   }
 }
 
@@ -1755,9 +1784,18 @@ void launch_rows16_u(const SpmmArgs& a, cudaStream_t s) {
   auto kern = k_spmm_rows16<T, ROWB, U, MINB>;
   const int64_t groups = (a.n_rows + R - 1) / R;
   const dim3 grid(persistent_blocks(kern, 0, groups, 32));
+  const int32_t* sched = (a.sched != nullptr && a.sched_warps == (int64_t)grid.x * (kSpmmThreads / 32)) ? a.sched
+                                                                                                        : nullptr;
   kern<<<grid, kSpmmThreads, 0, s>>>(a.indptr, a.indices, static_cast<const T*>(a.values),
-                                     static_cast<const T*>(a.X), static_cast<T*>(a.Y), a.row_map, a.n_rows);
+                                     static_cast<const T*>(a.X), static_cast<T*>(a.Y), a.row_map, a.n_rows, sched);
   SCL_CUDA(cudaGetLastError());
+}
+
+template <class T, int ROWB, int U, int MINB>
+int64_t warps_rows16_u(int64_t n_rows) {
+  constexpr int R = 32 / (ROWB / 16);
+  return (int64_t)persistent_blocks(k_spmm_rows16<T, ROWB, U, MINB>, 0, (n_rows + R - 1) / R, 32) *
+         (kSpmmThreads / 32);
 }
 
 template <class T, int ROWB>
@@ -2179,6 +2217,27 @@ void spmm_with_plan(const SpmmArgs& a, const SpmmPlan& plan, cudaStream_t s) {
   if (v == kF16 && x == kF16 && y == kF16) return launch_typed<__half, __half, __half, float>(a, plan, s);
   if (v == kF16 && x == kF16 && y == kF32) return launch_typed<__half, __half, float, float>(a, plan, s);
   throw Error(kErrTypeMismatch, "unsupported (values, X, Y) dtype combination for SpMM");
+}
+
+int64_t rows16_warps(int64_t F, DType t, int stage, int64_t n_rows) {
+  const int64_t rowb = F * (int64_t)dtype_size(t);
+  auto pick = [&](auto tag) -> int64_t {
+    using T = decltype(tag);
+#define SCL_RW(RB)                                                        \
+  if (rowb == RB) {                                                       \
+    if (stage == 4) return warps_rows16_u<T, RB, 4, 4>(n_rows);           \
+    if (stage == 8) return warps_rows16_u<T, RB, 8, 3>(n_rows);           \
+    if (stage == 16) return warps_rows16_u<T, RB, 16, 2>(n_rows);         \
+  }
+    SCL_RW(128)
+    SCL_RW(256)
+    SCL_RW(512)
+#undef SCL_RW
+    return 0;
+  };
+  if (t == kF32) return pick(float{});
+  if (t == kF64) return pick(double{});
+  return 0;
 }
 
 void spmm(const SpmmArgs& a, cudaStream_t s) {

@@ -692,7 +692,7 @@ SCL_EXPORT scl_error_t scl_gpu_graph_autotune(scl_gpu_graph_t graph, int64_t n_f
   try {
     auto step = [&](const SpmmPlan& p) {
       if (graph->reo) {
-        attach_schedule(*graph->reo, a, p, s);  // as the diffusion runs it
+        a.reo = graph->reo.get();  // with the schedules the diffusion uses
         spmm_reordered(*graph->reo, a, p, s);
       } else {
         spmm_with_plan(a, p, s);

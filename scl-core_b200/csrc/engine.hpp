@@ -135,6 +135,7 @@ void convert_values(const void* src, DType src_t, void* dst, DType dst_t, int64_
 void validate_csr(const DeviceCSR& g, int32_t* status, cudaStream_t s);
 
 // ---- SpMM / power iteration ------------------------------------------------
+struct Reordered;
 struct SpmmArgs {
   const int64_t* indptr;
   const int32_t* indices;
@@ -147,10 +148,10 @@ struct SpmmArgs {
   void* Y;         // n_rows x F, row-major
   DType ytype;
   const int32_t* row_map = nullptr;  // optional: output row r is written to Y[row_map[r]]
-  // optional for plan kind 12: a per-warp list of row groups (warp_schedule),
-  // used when the launch has exactly sched_warps warps
-  const int32_t* sched = nullptr;
-  int64_t sched_warps = 0;
+  // optional: the reordered graph whose structure indptr/indices are; the
+  // kernels that take a per-warp schedule of rows (plan kinds 9, 10, 12, 14)
+  // look theirs up in it (warp_schedule_for)
+  const Reordered* reo = nullptr;
 };
 // Launch shape of the SpMM kernel: `group` lanes own one output row and each
 // lane owns `vec` contiguous columns (16 bytes of X) per pass; vec == 1 is the
@@ -231,13 +232,14 @@ struct Reordered {
   uint64_t values_version = 0;  // bumped whenever `values` is rewritten
   // grouped layouts of the permuted structure for C = 1, 2, 4 rows per warp (built on first use)
   mutable std::unique_ptr<Grouped> grouped[3];
-  // plan kind 12's warp schedules for groups of 1, 2, 4 rows (built on first use) and their warp counts
-  mutable DevBuf sched[3];
-  mutable int64_t sched_warps[3] = {0, 0, 0};
+  // per-warp schedules of groups of R rows over nw warps (built on first use)
+  struct Schedule {
+    int R = 0;
+    int64_t nw = 0;
+    DevBuf list;
+  };
+  mutable std::vector<Schedule> schedules;
 };
-// Warps of a plan kind 12 launch (multi-row kernel, `stage` gathers per batch)
-// over n_rows rows of F values of type t.
-int64_t rows16_warps(int64_t F, DType t, int stage, int64_t n_rows);
 // Static schedule of the groups of R consecutive rows over nw warps, built on
 // the host from the row lengths: groups whose longest row is over eight times
 // the mean row length are dealt first, longest first, each to the least-loaded
@@ -245,9 +247,9 @@ int64_t rows16_warps(int64_t F, DType t, int stage, int64_t n_rows);
 // = longest row + 8). Each warp's list starts with its long groups. Layout:
 // int32[nw + 1] list offsets, then int32[groups] group ids.
 DevBuf warp_schedule(const int64_t* indptr, int64_t n, int R, int64_t nw, cudaStream_t s);
-// Sets a.sched / a.sched_warps for a plan kind 12 step on r's structure (the
-// schedule is built on first use and kept in r); clears them for other plans.
-void attach_schedule(const Reordered& r, SpmmArgs& a, const SpmmPlan& plan, cudaStream_t s);
+// r's schedule for (R, nw), built and kept on first use; nullptr while s is
+// capturing a CUDA graph (the build reads the row lengths on the host).
+const int32_t* warp_schedule_for(const Reordered& r, int R, int64_t nw, cudaStream_t s);
 // The grouped layout for C rows per warp with current values (built or refreshed on demand).
 const Grouped& reordered_grouped(const Reordered& r, int C, cudaStream_t s);
 // One SpMM step on the permuted structure with `plan` (kind 13 runs on the grouped layout).

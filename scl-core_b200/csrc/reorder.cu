@@ -161,10 +161,7 @@ void build_reorder(const CsrView& g, Reordered& r, cudaStream_t s, int mode) {
   r.n = n;
   r.nnz = nnz;
   r.values_ok = false;
-  for (int i = 0; i < 3; ++i) {
-    r.sched[i] = DevBuf();
-    r.sched_warps[i] = 0;
-  }
+  r.schedules.clear();
   DevBuf L(std::max<int64_t>(n, 1) * 4, s), changed(4, s);
   const int max_rounds = 4 * bits_for(std::max<int64_t>(n, 2)) + 16;
   int rounds = 0;
@@ -246,22 +243,18 @@ DevBuf warp_schedule(const int64_t* indptr, int64_t n, int R, int64_t nw, cudaSt
   return d;
 }
 
-void attach_schedule(const Reordered& r, SpmmArgs& a, const SpmmPlan& plan, cudaStream_t s) {
-  a.sched = nullptr;
-  a.sched_warps = 0;
-  const int64_t rowb = a.F * (int64_t)dtype_size(a.xtype);
-  if (plan.kind != 12 || a.xtype != a.vtype || !(a.xtype == kF32 || a.xtype == kF64) ||
-      !(rowb == 128 || rowb == 256 || rowb == 512))
-    return;
-  const int R = (int)(512 / rowb), slot = R == 1 ? 0 : (R == 2 ? 1 : 2);
-  const int64_t nw = rows16_warps(a.F, a.xtype, plan.stage, r.n);
-  if (nw <= 0) return;
-  if (r.sched_warps[slot] != nw) {
-    r.sched[slot] = warp_schedule(r.indptr.as<int64_t>(), r.n, R, nw, s);
-    r.sched_warps[slot] = nw;
-  }
-  a.sched = r.sched[slot].as<int32_t>();
-  a.sched_warps = nw;
+const int32_t* warp_schedule_for(const Reordered& r, int R, int64_t nw, cudaStream_t s) {
+  for (const Reordered::Schedule& e : r.schedules)
+    if (e.R == R && e.nw == nw) return e.list.as<int32_t>();
+  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+  SCL_CUDA(cudaStreamIsCapturing(s, &cs));
+  if (cs != cudaStreamCaptureStatusNone) return nullptr;
+  Reordered::Schedule e;
+  e.R = R;
+  e.nw = nw;
+  e.list = warp_schedule(r.indptr.as<int64_t>(), r.n, R, nw, s);
+  r.schedules.push_back(std::move(e));
+  return r.schedules.back().list.as<int32_t>();
 }
 
 void reorder_values(const void* vals, DType t, Reordered& r, cudaStream_t s) {
@@ -358,7 +351,7 @@ void diffuse_reordered(const Reordered& r, const void* X0, DType xtype, void* Y,
     a.Y = dst;
     a.ytype = ot;
     const SpmmPlan plan = plan_in ? *plan_in : default_spmm_plan(F, mtype, src, dst, ot);
-    attach_schedule(r, a, plan, s);
+    a.reo = &r;
     spmm_reordered(r, a, plan, s);
     src = dst;
   }

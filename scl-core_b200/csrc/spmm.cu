@@ -889,7 +889,7 @@ template <class VT, class YT, int ROWB, int U, int MINB>
 __global__ void __launch_bounds__(kSpmmThreads, MINB)
 k_spmm_rows16_lp(const int64_t* __restrict__ indptr, const int32_t* __restrict__ indices,
                  const VT* __restrict__ values, const VT* __restrict__ X, YT* __restrict__ Y,
-                 const int32_t* __restrict__ row_map, int64_t n_rows) {
+                 const int32_t* __restrict__ row_map, int64_t n_rows, const int32_t* __restrict__ sched) {
   constexpr int L = ROWB / 16;
   constexpr int Q = 32 / L;  // rows per warp = chains per row
   constexpr int VEC = 8;     // 16-bit values per lane
@@ -905,7 +905,25 @@ k_spmm_rows16_lp(const int64_t* __restrict__ indptr, const int32_t* __restrict__
   const int lq = lane % L;
   const int64_t n_grp = (n_rows + Q - 1) / Q;
   const int64_t nw = ((int64_t)gridDim.x * kSpmmThreads) >> 5;
-  int64_t grp = ((int64_t)blockIdx.x * kSpmmThreads + threadIdx.x) >> 5;
+  const int64_t w_id = ((int64_t)blockIdx.x * kSpmmThreads + threadIdx.x) >> 5;
+  // groups of Q rows: a static grid stride, or this warp's list of a
+  // balanced schedule (as in k_spmm_rows16)
+  const int32_t* __restrict__ glist = sched ? sched + nw + 1 : nullptr;
+  int64_t g_seq = w_id, q_next = 0, q_end = 0;
+  auto next_group = [&]() -> int64_t {
+    if (sched == nullptr) {
+      g_seq += nw;
+      return g_seq < n_grp ? g_seq : n_grp;
+    }
+    const int64_t qp = q_next++;
+    return qp < q_end ? (int64_t)glist[qp] : n_grp;
+  };
+  int64_t grp = w_id;
+  if (sched != nullptr) {
+    q_next = sched[w_id];
+    q_end = sched[w_id + 1];
+    grp = q_next < q_end ? (int64_t)glist[q_next++] : n_grp;
+  }
   if (grp >= n_grp) return;
   const char* __restrict__ Xl = reinterpret_cast<const char*>(X) + lq * 16;
   auto gather = [&](int32_t j) -> uint4 {
@@ -938,9 +956,11 @@ k_spmm_rows16_lp(const int64_t* __restrict__ indptr, const int32_t* __restrict__
       s_v[w][b][q * 32 + lq + L * k] = v[k];
     }
   };
+  int64_t g_nx = next_group();
+  int64_t g_nn = next_group();
   int64_t s_cur, e_cur, s_nx, e_nx;
   bounds(grp, s_cur, e_cur);
-  bounds(grp + nw, s_nx, e_nx);
+  bounds(g_nx, s_nx, e_nx);
   int buf = 0;
   {
     int32_t j[Q];
@@ -949,9 +969,10 @@ k_spmm_rows16_lp(const int64_t* __restrict__ indptr, const int32_t* __restrict__
     publish(0, j, v);
     __syncwarp();
   }
-  for (; grp < n_grp; grp += nw) {
+  while (grp < n_grp) {
+    const int64_t g_n3 = next_group();
     int64_t s_nn, e_nn;
-    bounds(grp + 2 * nw, s_nn, e_nn);
+    bounds(g_nn, s_nn, e_nn);
     const int len = (int)(e_cur - s_cur);
     int maxlen = len, minlen = len;
 #pragma unroll
@@ -1064,6 +1085,9 @@ k_spmm_rows16_lp(const int64_t* __restrict__ indptr, const int32_t* __restrict__
     e_cur = e_nx;
     s_nx = s_nn;
     e_nx = e_nn;
+    grp = g_nx;
+    g_nx = g_nn;
+    g_nn = g_n3;
   }
 }
 
@@ -1350,10 +1374,10 @@ template <int ROWB>
 constexpr int split_pipe_smem() { return split_pipe_warps<ROWB>() * 2 * 32 * ROWB; }
 
 template <class VT, class XT, class YT, int ROWB, bool MIXED>
-__global__ void __launch_bounds__(32 * split_pipe_warps<ROWB>())
+__global__ void __launch_bounds__(32 * split_pipe_warps<ROWB>(), ROWB == 128 ? 3 : 1)
 k_spmm_split_pipe(const int64_t* __restrict__ indptr, const int32_t* __restrict__ indices,
                   const VT* __restrict__ values, const XT* __restrict__ X, YT* __restrict__ Y,
-                  const int32_t* __restrict__ row_map, int64_t n_rows) {
+                  const int32_t* __restrict__ row_map, int64_t n_rows, const int32_t* __restrict__ sched) {
   static_assert(sizeof(XT) == 2 && sizeof(VT) == 2, "the split-chain kernel is for 16-bit storage");
   constexpr int L = ROWB / 16;  // lanes per gathered row
   constexpr int Q = 32 / L;     // chains (entries per load instruction)
@@ -1372,7 +1396,7 @@ k_spmm_split_pipe(const int64_t* __restrict__ indptr, const int32_t* __restrict_
   const int64_t row0 = ((int64_t)blockIdx.x * NT + threadIdx.x) >> 5;
   if (row0 >= n_rows) return;
   ChunkCursor cur;
-  cur.init(indptr, row0, n_rows, nw);
+  cur.init(indptr, row0, n_rows, nw, sched);
   Chunk C = cur.next(indptr);  // pairs loading
   int32_t jC = 0;
   unsigned vC = 0;
@@ -1503,10 +1527,10 @@ __device__ __forceinline__ void lean_consume(const uint4* __restrict__ sb, const
 // entries with a few vector loads instead of U shuffles; for 128-byte rows the
 // shuffles were measured faster and are kept.
 template <class VT, class XT, class YT, int ROWB, int MODE>
-__global__ void __launch_bounds__(32 * split_pipe_warps<ROWB>())
+__global__ void __launch_bounds__(32 * split_pipe_warps<ROWB>(), ROWB == 128 ? 3 : 1)
 k_spmm_split_lean(const int64_t* __restrict__ indptr, const int32_t* __restrict__ indices,
                   const VT* __restrict__ values, const XT* __restrict__ X, YT* __restrict__ Y,
-                  const int32_t* __restrict__ row_map, int64_t n_rows) {
+                  const int32_t* __restrict__ row_map, int64_t n_rows, const int32_t* __restrict__ sched) {
   static_assert(sizeof(XT) == 2 && sizeof(VT) == 2, "the split-chain kernel is for 16-bit storage");
   constexpr int L = ROWB / 16;
   constexpr int Q = 32 / L;
@@ -1531,7 +1555,7 @@ k_spmm_split_lean(const int64_t* __restrict__ indptr, const int32_t* __restrict_
   const int64_t row0 = ((int64_t)blockIdx.x * NT + threadIdx.x) >> 5;
   if (row0 >= n_rows) return;
   ChunkCursor cur;
-  cur.init(indptr, row0, n_rows, nw);
+  cur.init(indptr, row0, n_rows, nw, sched);
   Chunk C = cur.next(indptr);
   int32_t jC = 0;
   unsigned short vC = 0;
@@ -1784,18 +1808,10 @@ void launch_rows16_u(const SpmmArgs& a, cudaStream_t s) {
   auto kern = k_spmm_rows16<T, ROWB, U, MINB>;
   const int64_t groups = (a.n_rows + R - 1) / R;
   const dim3 grid(persistent_blocks(kern, 0, groups, 32));
-  const int32_t* sched = (a.sched != nullptr && a.sched_warps == (int64_t)grid.x * (kSpmmThreads / 32)) ? a.sched
-                                                                                                        : nullptr;
+  const int32_t* sched = a.reo ? warp_schedule_for(*a.reo, R, (int64_t)grid.x * (kSpmmThreads / 32), s) : nullptr;
   kern<<<grid, kSpmmThreads, 0, s>>>(a.indptr, a.indices, static_cast<const T*>(a.values),
                                      static_cast<const T*>(a.X), static_cast<T*>(a.Y), a.row_map, a.n_rows, sched);
   SCL_CUDA(cudaGetLastError());
-}
-
-template <class T, int ROWB, int U, int MINB>
-int64_t warps_rows16_u(int64_t n_rows) {
-  constexpr int R = 32 / (ROWB / 16);
-  return (int64_t)persistent_blocks(k_spmm_rows16<T, ROWB, U, MINB>, 0, (n_rows + R - 1) / R, 32) *
-         (kSpmmThreads / 32);
 }
 
 template <class T, int ROWB>
@@ -1862,8 +1878,10 @@ void launch_split_pipe_r(const SpmmArgs& a, cudaStream_t s) {
   SCL_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, nt, smem));
   const int64_t need = (a.n_rows * 32 + nt - 1) / nt;
   const int64_t grid = std::max<int64_t>(1, std::min<int64_t>(need, (int64_t)std::max(per_sm, 1) * sm_count(dev)));
+  const int32_t* sched = a.reo ? warp_schedule_for(*a.reo, 1, grid * (nt / 32), s) : nullptr;
   kern<<<(unsigned)grid, nt, smem, s>>>(a.indptr, a.indices, static_cast<const VT*>(a.values),
-                                        static_cast<const XT*>(a.X), static_cast<YT*>(a.Y), a.row_map, a.n_rows);
+                                        static_cast<const XT*>(a.X), static_cast<YT*>(a.Y), a.row_map, a.n_rows,
+                                        sched);
   SCL_CUDA(cudaGetLastError());
 }
 
@@ -1895,8 +1913,10 @@ void launch_split_lean_r(const SpmmArgs& a, cudaStream_t s) {
   SCL_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, nt, smem));
   const int64_t need = (a.n_rows * 32 + nt - 1) / nt;
   const int64_t grid = std::max<int64_t>(1, std::min<int64_t>(need, (int64_t)std::max(per_sm, 1) * sm_count(dev)));
+  const int32_t* sched = a.reo ? warp_schedule_for(*a.reo, 1, grid * (nt / 32), s) : nullptr;
   kern<<<(unsigned)grid, nt, smem, s>>>(a.indptr, a.indices, static_cast<const VT*>(a.values),
-                                        static_cast<const XT*>(a.X), static_cast<YT*>(a.Y), a.row_map, a.n_rows);
+                                        static_cast<const XT*>(a.X), static_cast<YT*>(a.Y), a.row_map, a.n_rows,
+                                        sched);
   SCL_CUDA(cudaGetLastError());
 }
 
@@ -1928,8 +1948,10 @@ void launch_rows16_lp_u(const SpmmArgs& a, cudaStream_t s) {
   auto kern = k_spmm_rows16_lp<VT, YT, ROWB, U, MINB>;
   const int64_t groups = (a.n_rows + R - 1) / R;
   const dim3 grid(persistent_blocks(kern, 0, groups, 32));
+  const int32_t* sched = a.reo ? warp_schedule_for(*a.reo, R, (int64_t)grid.x * (kSpmmThreads / 32), s) : nullptr;
   kern<<<grid, kSpmmThreads, 0, s>>>(a.indptr, a.indices, static_cast<const VT*>(a.values),
-                                     static_cast<const VT*>(a.X), static_cast<YT*>(a.Y), a.row_map, a.n_rows);
+                                     static_cast<const VT*>(a.X), static_cast<YT*>(a.Y), a.row_map, a.n_rows,
+                                     sched);
   SCL_CUDA(cudaGetLastError());
 }
 
@@ -2217,27 +2239,6 @@ void spmm_with_plan(const SpmmArgs& a, const SpmmPlan& plan, cudaStream_t s) {
   if (v == kF16 && x == kF16 && y == kF16) return launch_typed<__half, __half, __half, float>(a, plan, s);
   if (v == kF16 && x == kF16 && y == kF32) return launch_typed<__half, __half, float, float>(a, plan, s);
   throw Error(kErrTypeMismatch, "unsupported (values, X, Y) dtype combination for SpMM");
-}
-
-int64_t rows16_warps(int64_t F, DType t, int stage, int64_t n_rows) {
-  const int64_t rowb = F * (int64_t)dtype_size(t);
-  auto pick = [&](auto tag) -> int64_t {
-    using T = decltype(tag);
-#define SCL_RW(RB)                                                        \
-  if (rowb == RB) {                                                       \
-    if (stage == 4) return warps_rows16_u<T, RB, 4, 4>(n_rows);           \
-    if (stage == 8) return warps_rows16_u<T, RB, 8, 3>(n_rows);           \
-    if (stage == 16) return warps_rows16_u<T, RB, 16, 2>(n_rows);         \
-  }
-    SCL_RW(128)
-    SCL_RW(256)
-    SCL_RW(512)
-#undef SCL_RW
-    return 0;
-  };
-  if (t == kF32) return pick(float{});
-  if (t == kF64) return pick(double{});
-  return 0;
 }
 
 void spmm(const SpmmArgs& a, cudaStream_t s) {

@@ -270,6 +270,20 @@ SCL_EXPORT scl_error_t scl_gpu_residual_fp64(const void* X, scl_dtype_t x_dtype,
  * The choice is process-wide. previous (may be null) receives the old one. */
 SCL_EXPORT scl_error_t scl_gpu_knn_set_kernel(int kernel, int* previous);
 
+/* The per-warp schedule of row groups that the SpMM plan kinds 9, 10, 12
+ * and 14 follow on a reordered graph (built there once per graph and warp
+ * count). No counterpart in scl-core. Host only: indptr holds the n_rows + 1
+ * row offsets of a CSR structure, groups are rows_per_group (1, 2 or 4)
+ * consecutive rows, and n_warps lists are made. Groups whose longest row is
+ * over eight times the mean row length are dealt first, longest first, each
+ * to the least-loaded warp (ties: the lowest warp); then every other group in
+ * index order, each to the least-loaded warp (cost = longest row + 8). A
+ * warp's list holds its long groups first, then its others by index. out
+ * (out_len = n_warps + 1 + ceil(n_rows / rows_per_group)) receives the
+ * n_warps + 1 list offsets, then the group ids. */
+SCL_EXPORT scl_error_t scl_gpu_warp_schedule(const int64_t* indptr, int64_t n_rows, int rows_per_group,
+                                             int64_t n_warps, int32_t* out, int64_t out_len);
+
 /* Test hook of the tensor-core kNN's bounded waits. No counterpart in
  * scl-core. CTA `cta` of the following tensor-core searches never receives
  * its first accumulator, so its epilogue's wait runs out after 2 s: the

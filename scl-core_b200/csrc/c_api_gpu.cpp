@@ -623,6 +623,26 @@ SCL_EXPORT scl_error_t scl_gpu_knn_set_kernel(int kernel, int* previous) {
   SCL_API_CATCH
 }
 
+SCL_EXPORT scl_error_t scl_gpu_warp_schedule(const int64_t* indptr, int64_t n_rows, int rows_per_group,
+                                             int64_t n_warps, int32_t* out, int64_t out_len) {
+  SCL_API_CHECK_NULL(indptr, "Offset array pointer is null");
+  SCL_API_CHECK_NULL(out, "Output pointer is null");
+  SCL_API_CHECK(n_rows >= 0 && n_rows < (1ll << 31), SCL_ERROR_INVALID_ARGUMENT, "row count out of range");
+  SCL_API_CHECK(rows_per_group == 1 || rows_per_group == 2 || rows_per_group == 4, SCL_ERROR_INVALID_ARGUMENT,
+                "rows per group must be 1, 2 or 4");
+  SCL_API_CHECK(n_warps >= 1 && n_warps < (1ll << 31), SCL_ERROR_INVALID_ARGUMENT, "warp count out of range");
+  const int64_t groups = (n_rows + rows_per_group - 1) / rows_per_group;
+  SCL_API_CHECK(out_len == n_warps + 1 + groups, SCL_ERROR_DIMENSION_MISMATCH,
+                "output length must be n_warps + 1 + ceil(n_rows / rows_per_group)");
+  for (int64_t r = 0; r < n_rows; ++r)
+    SCL_API_CHECK(indptr[r + 1] >= indptr[r], SCL_ERROR_INVALID_ARGUMENT, "row offsets must not decrease");
+  SCL_API_TRY
+  const std::vector<int32_t> lists = warp_schedule_host(indptr, n_rows, rows_per_group, n_warps);
+  std::copy(lists.begin(), lists.end(), out);
+  SCL_API_RETURN_OK;
+  SCL_API_CATCH
+}
+
 SCL_EXPORT scl_error_t scl_gpu_graph_gather_floor(scl_gpu_graph_t graph, int64_t n_features, scl_dtype_t dtype,
                                                   int reps, double* ms, void* stream) {
   SCL_API_CHECK_NULL(graph, "Graph is null");

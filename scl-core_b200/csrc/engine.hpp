@@ -247,6 +247,8 @@ struct Reordered {
 // = longest row + 8). Each warp's list starts with its long groups. Layout:
 // int32[nw + 1] list offsets, then int32[groups] group ids.
 DevBuf warp_schedule(const int64_t* indptr, int64_t n, int R, int64_t nw, cudaStream_t s);
+// The same schedule from host row offsets ip[0..n] (the host part of warp_schedule).
+std::vector<int32_t> warp_schedule_host(const int64_t* ip, int64_t n, int R, int64_t nw);
 // r's schedule for (R, nw), built and kept on first use; nullptr while s is
 // capturing a CUDA graph (the build reads the row lengths on the host).
 const int32_t* warp_schedule_for(const Reordered& r, int R, int64_t nw, cudaStream_t s);

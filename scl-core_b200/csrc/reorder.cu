@@ -197,21 +197,19 @@ void build_reorder(const CsrView& g, Reordered& r, cudaStream_t s, int mode) {
   SCL_CUDA(cudaGetLastError());
 }
 
-DevBuf warp_schedule(const int64_t* indptr, int64_t n, int R, int64_t nw, cudaStream_t s) {
-  SCL_REQUIRE(R >= 1 && nw >= 1 && n < (1ll << 31), kErrInvalidArgument, "bad warp schedule request");
+std::vector<int32_t> warp_schedule_host(const int64_t* ip, int64_t n, int R, int64_t nw) {
+  SCL_REQUIRE(R >= 1 && nw >= 1 && n >= 0 && n < (1ll << 31) && nw < (1ll << 31), kErrInvalidArgument,
+              "bad warp schedule request");
   const int64_t ng = (n + R - 1) / R;
-  std::vector<int64_t> ip(n + 1);
-  SCL_CUDA(cudaMemcpyAsync(ip.data(), indptr, (n + 1) * sizeof(int64_t), cudaMemcpyDeviceToHost, s));
-  SCL_CUDA(cudaStreamSynchronize(s));
   std::vector<int64_t> len(ng, 0);
   for (int64_t g = 0; g < ng; ++g)
     for (int64_t r = g * R; r < std::min<int64_t>(n, g * R + R); ++r) len[g] = std::max(len[g], ip[r + 1] - ip[r]);
-  const int64_t thr = 8 * std::max<int64_t>(1, (ip[n] + n - 1) / std::max<int64_t>(n, 1));
+  const int64_t thr = 8 * std::max<int64_t>(1, (ip[n] - ip[0] + n - 1) / std::max<int64_t>(n, 1));
   std::vector<int32_t> hubs;
   for (int64_t g = 0; g < ng; ++g)
     if (len[g] > thr) hubs.push_back((int32_t)g);
   std::stable_sort(hubs.begin(), hubs.end(), [&](int32_t a, int32_t b) { return len[a] > len[b]; });
-  using Slot = std::pair<int64_t, int64_t>;  // (load, warp)
+  using Slot = std::pair<int64_t, int64_t>;  // (load, warp): ties go to the lower warp
   std::priority_queue<Slot, std::vector<Slot>, std::greater<Slot>> heap;
   for (int64_t w = 0; w < nw; ++w) heap.push({0, w});
   std::vector<int32_t> owner(ng);
@@ -237,6 +235,14 @@ DevBuf warp_schedule(const int64_t* indptr, int64_t n, int R, int64_t nw, cudaSt
   for (int32_t g : hubs) out[nw + 1 + fill[owner[g]]++] = g;
   for (int64_t g = 0; g < ng; ++g)
     if (!is_hub[g]) out[nw + 1 + fill[owner[g]]++] = (int32_t)g;
+  return out;
+}
+
+DevBuf warp_schedule(const int64_t* indptr, int64_t n, int R, int64_t nw, cudaStream_t s) {
+  std::vector<int64_t> ip(n + 1);
+  SCL_CUDA(cudaMemcpyAsync(ip.data(), indptr, (n + 1) * sizeof(int64_t), cudaMemcpyDeviceToHost, s));
+  SCL_CUDA(cudaStreamSynchronize(s));
+  const std::vector<int32_t> out = warp_schedule_host(ip.data(), n, R, nw);
   DevBuf d(out.size() * sizeof(int32_t), s);
   SCL_CUDA(cudaMemcpyAsync(d.p, out.data(), out.size() * sizeof(int32_t), cudaMemcpyHostToDevice, s));
   SCL_CUDA(cudaStreamSynchronize(s));  // `out` is released on return

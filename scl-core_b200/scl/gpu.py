@@ -294,6 +294,21 @@ def residual_fp64(X, X_ref, rel_floor: float = 1e-3, variant: str = "f32_i32", s
     return {"rel_fro": out[0], "max_rel": out[1], "max_abs": out[2], "ref_fro": out[3]}
 
 
+def warp_schedule(indptr, rows_per_group: int, n_warps: int, variant: str = "f32_i32"):
+    """The per-warp schedule of row groups the SpMM plan kinds 9, 10, 12 and 14
+    follow on a reordered graph (scl_gpu_warp_schedule; host only).
+
+    Returns (offsets, groups): warp w's list is groups[offsets[w]:offsets[w + 1]]."""
+    ip = np.ascontiguousarray(indptr, dtype=np.int64)
+    n = ip.size - 1
+    ng = (n + rows_per_group - 1) // rows_per_group
+    out = np.empty(int(n_warps) + 1 + ng, np.int32)
+    lib = get_library(variant)
+    check_error(lib.scl_gpu_warp_schedule(ctypes.c_void_p(ip.ctypes.data), int(n), int(rows_per_group), int(n_warps),
+                                          ctypes.c_void_p(out.ctypes.data), int(out.size)), "warp_schedule", lib)
+    return out[: n_warps + 1].copy(), out[n_warps + 1:].copy()
+
+
 class GpuBatch:
     """Many independent graphs diffused together in one persistent, CUDA-graph
     replayed launch (scl_gpu_batch_*). Blocks are the graphs' n_b x F blocks
